@@ -1,0 +1,166 @@
+/*
+ * bbmg_b200.h -- C ABI of the B200 black-box multigrid pressure solver.
+ *
+ * Drop-in for NGA2's bbmg pressure solve behind its linear-solver interface:
+ *   init    -> bbmg_create   (ils_class.f90:162-226, bbmg_class.f90:185-600)
+ *   setup   -> bbmg_setup    (ils_class.f90:230-256, 373-376; bbmg_class.f90:932-962)
+ *   solve   -> bbmg_solve    (ils_class.f90:674-822;  bbmg_class.f90:604-728)
+ *   destroy -> bbmg_destroy  (ils_class.f90:826-920)
+ * The public linsol fields (linsol_class.f90:16-58) map to arguments: stc and
+ * opr to bbmg_setup; rhs, sol, maxit, rcvg, it and rerr to bbmg_solve.
+ *
+ * Arrays use NGA2's Fortran layout: i fastest, then j, then k, each direction
+ * padded by `ghost` overlap layers (the config's `no`).  The operator is
+ * opr(nst, imino_:imaxo_, jmino_:jmaxo_, kmino_:kmaxo_) with the stencil index
+ * fastest, exactly the caller's psolv%opr.  Only interior entries are read;
+ * the solver copies in and out (ils_class.f90:247-256, 693-700, 782-788), so
+ * caller arrays stay caller-owned.  Pointers may be host or device memory; the
+ * kind is detected per call.
+ *
+ * Every entry point returns a status code and never aborts the host process.
+ * A handle serves one stream and is not thread-safe; separate handles are
+ * independent.  All compute runs on the GPU: there is no CPU fallback.
+ */
+#ifndef BBMG_B200_H
+#define BBMG_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define BBMG_OK          0  /* converged: rerr <= rcvg                          */
+#define BBMG_MAXIT       1  /* stopped at maxit without reaching rcvg          */
+#define BBMG_STAGNATION  2  /* mixed precision: the residual stopped decreasing */
+#define BBMG_NONFINITE   3  /* NaN or Inf appeared in the residual             */
+#define BBMG_BAD_ARGS    4  /* invalid argument (also a stencil outside 3x3x3) */
+#define BBMG_NOT_SETUP   5  /* solve before setup (ils_class.f90:684)          */
+#define BBMG_CUDA        6  /* a CUDA call failed; see bbmg_last_error         */
+#define BBMG_NO_MEMORY   7  /* device allocation failed                        */
+
+/* solution methods, NGA2's ILS ids (ils_class.f90:16-17) */
+#define BBMG_METHOD_BBOX      1  /* stationary V-cycles (mgsolve)              */
+#define BBMG_METHOD_PCG_BBOX  2  /* V-cycle preconditioned CG (cgsolve)        */
+
+/* arithmetic of the solve */
+#define BBMG_PREC_FP64   0  /* every step in FP64, the reference's arithmetic   */
+#define BBMG_PREC_MIXED  1  /* FP32 V-cycle inside an FP64 outer iteration      */
+
+typedef struct bbmg_handle bbmg_handle;
+
+/* Grid: the pgrid sizes and periodicity bbmg reads (bbmg_class.f90:211-253). */
+typedef struct {
+    int nx, ny, nz;        /* interior cells per direction (>= 1)            */
+    int xper, yper, zper;  /* periodicity flags                              */
+    int ghost;             /* overlap layers of the caller's arrays (>= 0)   */
+} bbmg_grid;
+
+/* Solver knobs: the bbmg parameters the ILS sets (ils_class.f90:189-196,
+ * bbmg_class.f90:91-98) plus the arithmetic mode. */
+typedef struct {
+    int method;            /* BBMG_METHOD_BBOX or BBMG_METHOD_PCG_BBOX       */
+    int precision;         /* BBMG_PREC_FP64 or BBMG_PREC_MIXED              */
+    int ncycle;            /* 1 = V-cycle, 2 = W-cycle                       */
+    int relax_pre;         /* pre-smoothing sweeps                           */
+    int relax_post;        /* post-smoothing sweeps                          */
+    int ncell_coarsest;    /* coarsest level size limit                      */
+    int use_direct_solve;  /* LU at the coarsest level (else relaxation)     */
+    int maxit;             /* linsol maxit                                   */
+    double rcvg;           /* linsol rcvg: relative inf-norm residual        */
+    int device;            /* CUDA device ordinal; -1 = the current device   */
+} bbmg_params;
+
+/* Diagnostics of the last setup/solve. */
+typedef struct {
+    int nlvl;              /* levels in use                                  */
+    int level_dims[16][3]; /* interior sizes per level (first nlvl rows)     */
+    int coarse_n;          /* unknowns of the dense coarsest problem         */
+    int coarse_pinned;     /* round-off pivots pinned in its LU (singular)   */
+    int it;                /* iterations of the last solve                   */
+    double rerr;           /* reported relative residual (inf-norm ratio)    */
+    double res0;           /* initial residual inf-norm                      */
+    double true_rerr;      /* FP64 b - A x inf-norm ratio at exit            */
+    double setup_ms;       /* device time of the last setup                  */
+    double solve_ms;       /* device time of the last solve                  */
+    long long device_bytes;/* device memory held by the handle               */
+    int status;            /* status of the last solve                       */
+    long long launches;    /* kernel launches of the last solve              */
+} bbmg_info;
+
+/* Fill `p` with the ILS values: pcg_bbox, FP64, V(2,2), ncell_coarsest 300,
+ * direct coarsest solve, maxit 100, rcvg 1e-10, current device. */
+void bbmg_default_params(bbmg_params *p);
+
+/* init: build the level hierarchy and allocate device storage.
+ * Replaces bbmg_from_pgrid + initialize (bbmg_class.f90:185-600) as called
+ * from ils%init (ils_class.f90:184-198). */
+int bbmg_create(const bbmg_grid *grid, const bbmg_params *params, bbmg_handle **handle);
+
+/* setup: copy the caller's operator and rebuild every level.
+ * stc is int[nst][3] (C order, the Fortran stc(st,1:3) transposed); every
+ * offset must lie in [-1,1]^3.  opr is (nst, nx+2g, ny+2g, nz+2g), Fortran
+ * order.  Replaces the ils scatter (ils_class.f90:244-256) and bbmg%update
+ * (bbmg_class.f90:932-962). */
+int bbmg_setup(bbmg_handle *h, int nst, const int *stc, const double *opr);
+
+/* solve: rhs and sol are (nx+2g, ny+2g, nz+2g) Fortran arrays; sol holds the
+ * initial guess on entry and the solution on exit (interior only; ghosts are
+ * left for the caller's own sync).  it and rerr follow the reference's
+ * definitions (bbmg_class.f90:627-633, 694-697, 721-724): rerr is
+ * max|r|/max|r0| of the iteration's residual.  Either may be NULL.
+ * Replaces ils%solve's bbmg branch (ils_class.f90:674-822). */
+int bbmg_solve(bbmg_handle *h, const double *rhs, double *sol, int *it, double *rerr);
+
+/* Change maxit / rcvg between solves (the linsol fields). */
+int bbmg_set_convergence(bbmg_handle *h, int maxit, double rcvg);
+
+/* Run on the given cudaStream_t (default: a stream the handle creates). */
+int bbmg_set_stream(bbmg_handle *h, void *stream);
+
+int bbmg_get_info(const bbmg_handle *h, bbmg_info *info);
+
+/* destroy: release the handle and its device memory. */
+int bbmg_destroy(bbmg_handle *h);
+
+/* Message of the last failure on this handle ("" if none); h may be NULL
+ * for failures of bbmg_create. */
+const char *bbmg_last_error(const bbmg_handle *h);
+
+/* ------------------------------------------------------------------------
+ * Step-level access, used by the parity tests to compare each stage of the
+ * method with the reference's routine of the same name.  Arrays are exchanged
+ * in the reference's own layout: one overlap layer, cell-major (k, j, i) with
+ * the coefficient index fastest (27 for opr/f2c/oprc2f as opr(-1:1,-1:1,-1:1),
+ * 8 for c2f as c2f(0:1,0:1,0:1)).
+ * ---------------------------------------------------------------------- */
+#define BBMG_ARR_OPR     0
+#define BBMG_ARR_C2F     1
+#define BBMG_ARR_F2C     2
+#define BBMG_ARR_OPRC2F  3
+#define BBMG_ARR_V       4
+#define BBMG_ARR_F       5
+#define BBMG_ARR_R       6
+
+#define BBMG_STEP_RELAX        0  /* arg = +1/-1: relax(v, f, n, dir)      bbmg_class.f90:848-887 */
+#define BBMG_STEP_RESIDUAL     1  /* get_residual(n)                       bbmg_class.f90:831-844 */
+#define BBMG_STEP_RESTRICT     2  /* f2c(r_n -> f_n+1), v_n+1 = 0          bbmg_class.f90:805-827,739 */
+#define BBMG_STEP_PROLONG      3  /* c2f(v_n+1 -> r_n); v_n += r_n         bbmg_class.f90:779-801,770 */
+#define BBMG_STEP_CYCLE        4  /* cycle(n)                              bbmg_class.f90:732-776 */
+#define BBMG_STEP_DIRECT       5  /* direct_solve()                        bbmg_class.f90:891-927 */
+
+/* prec selects the FP64 (0) or FP32 (1) copy of a level's data. */
+long long bbmg_debug_get(bbmg_handle *h, int level, int which, int prec, double *out);
+long long bbmg_debug_put(bbmg_handle *h, int level, int which, int prec, const double *in);
+int bbmg_debug_step(bbmg_handle *h, int step, int level, int arg, int prec);
+/* Device time of one stage, for roofline measurements: the stage runs `reps`
+ * times back to back on the handle's stream between two CUDA events; returns
+ * the average milliseconds per repetition in *ms. */
+int bbmg_profile_step(bbmg_handle *h, int step, int level, int arg, int prec, int reps, double *ms);
+/* dense coarsest matrix (row-major np x np), its LU (row-major, unit lower
+ * below the diagonal) and pivots; any pointer may be NULL. */
+int bbmg_debug_direct(bbmg_handle *h, double *op, double *lu, int *piv, int *np);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BBMG_B200_H */

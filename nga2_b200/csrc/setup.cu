@@ -1,0 +1,497 @@
+// setup.cu -- operator setup of the black-box multigrid on the GPU (FP64).
+//
+// Every kernel restates one routine of src/solver/bbmg_class.f90 for one
+// rank; the loop nests that accumulate into a coefficient keep the
+// reference's order so that the FP64 results match the oracle bit for bit.
+// The grid-wide work is data parallel per cell: each output cell is written
+// by exactly one thread, so no atomics and no ordering between threads are
+// needed.
+#include "setup.cuh"
+
+namespace bbmg {
+
+// ---------------------------------------------------------------------------
+// Level-1 operator: ils scatter of the caller's nst-point stencil into the
+// 27-point layout (ils_class.f90:247-256), identity in the overlap
+// (bbmg_class.f90:937-949).  src is (nst, nx+2g, ny+2g, nz+2g) Fortran order.
+__global__ void k_scatter_operator(Lay L, const double *__restrict__ src, int nst, int g,
+                                   const int *__restrict__ stc, double *__restrict__ opr) {
+    long long total = (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
+    const long long sx = nst, sy = sx * (L.nx + 2 * g), sz = sy * (L.ny + 2 * g);
+    for (long long t = gtid(); t < total; t += gstride()) {
+        int i, j, k;
+        any_cell(L, t, i, j, k);
+        long long id = L.idx(i, j, k);
+        bool interior = i >= 0 && i < L.nx && j >= 0 && j < L.ny && k >= 0 && k < L.nz;
+        double o[27];
+#pragma unroll
+        for (int q = 0; q < 27; q++) o[q] = 0.0;
+        if (interior) {
+            const double *s = src + (long long)(k + g) * sz + (long long)(j + g) * sy + (long long)(i + g) * sx;
+#pragma unroll 1
+            for (int st = 0; st < nst; st++) {
+                int q = q27(stc[3 * st], stc[3 * st + 1], stc[3 * st + 2]);
+                o[q] = __dadd_rn(o[q], s[st]);
+            }
+        } else {
+            o[kCentre27] = 1.0;
+        }
+#pragma unroll
+        for (int q = 0; q < 27; q++) opr[q * L.plane + id] = o[q];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Periodic copy of the overlap for nplanes planes (msync / vsync on one rank,
+// bbmg_class.f90:1388-1724).  The reference copies x, then y, then z over the
+// full extent of the other directions; the result is that every overlap cell
+// with a coordinate outside the interior of a periodic direction holds the
+// value of the cell obtained by wrapping those coordinates.  The sources are
+// never themselves periodic images, so one gather pass reproduces it.
+__global__ void k_wrap(Lay L, double *__restrict__ a, int nplanes) {
+    long long total = (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
+    for (long long t = gtid(); t < total; t += gstride()) {
+        int i, j, k;
+        any_cell(L, t, i, j, k);
+        int si = wrap(L.xper, i, L.nx), sj = wrap(L.yper, j, L.ny), sk = wrap(L.zper, k, L.nz);
+        if (si == i && sj == j && sk == k) continue;
+        long long d = L.idx(i, j, k), s = L.idx(si, sj, sk);
+        for (int q = 0; q < nplanes; q++) a[q * L.plane + d] = a[q * L.plane + s];
+    }
+}
+__global__ void k_wrap_f(Lay L, float *__restrict__ a, int nplanes) {
+    long long total = (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
+    for (long long t = gtid(); t < total; t += gstride()) {
+        int i, j, k;
+        any_cell(L, t, i, j, k);
+        int si = wrap(L.xper, i, L.nx), sj = wrap(L.yper, j, L.ny), sk = wrap(L.zper, k, L.nz);
+        if (si == i && sj == j && sk == k) continue;
+        long long d = L.idx(i, j, k), s = L.idx(si, sj, sk);
+        for (int q = 0; q < nplanes; q++) a[q * L.plane + d] = a[q * L.plane + s];
+    }
+}
+
+__device__ __forceinline__ double sgn_clamp(double a) {
+    // sign(max(abs(a),epsilon(1.0_WP)),a)
+    return copysign(fmax(fabs(a), kEps), a);
+}
+
+// ---------------------------------------------------------------------------
+// Prolongation, sweep 1: identity and 1-D lines with Shapira lumping
+// (bbmg_class.f90:978-1051).  Every cell including the overlap.
+__global__ void k_prolong_sweep1(Lay L, const double *__restrict__ opr, double *__restrict__ c2f) {
+    const double ratio = 10.0;
+    long long total = (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
+    for (long long t = gtid(); t < total; t += gstride()) {
+        int i, j, k;
+        any_cell(L, t, i, j, k);
+        long long id = L.idx(i, j, k);
+        int n1 = pmod(L.xper, i, L.nx), n2 = pmod(L.yper, j, L.ny), n3 = pmod(L.zper, k, L.nz);
+        double c[8];
+#pragma unroll
+        for (int s = 0; s < 8; s++) c[s] = 0.0;
+        int sum = n1 + n2 + n3;
+        if (sum == 0) {
+            c[0] = 1.0;
+        } else if (sum == 1) {
+            double m = 0.0, z = 0.0, p = 0.0;  // opr1d(-1), opr1d(0), opr1d(+1)
+#pragma unroll 1
+            for (int q = 0; q < 27; q++) {
+                int li = q % 3 - 1, lj = (q / 3) % 3 - 1, lk = q / 9 - 1;
+                int l = n1 ? li : (n2 ? lj : lk);
+                int ax = n1 ? q27(li, 0, 0) : (n2 ? q27(0, lj, 0) : q27(0, 0, lk));
+                double a = opr[q * L.plane + id];
+                if (__dmul_rn(ratio, fabs(opr[ax * L.plane + id])) >= fabs(a)) {
+                    if (l < 0) m = __dadd_rn(m, a);
+                    else if (l == 0) z = __dadd_rn(z, a);
+                    else p = __dadd_rn(p, a);
+                } else {
+                    z = __dadd_rn(z, a);
+                }
+            }
+            z = sgn_clamp(z);
+            c[0] = -m / z;
+            c[n1 ? q8(1, 0, 0) : (n2 ? q8(0, 1, 0) : q8(0, 0, 1))] = -p / z;
+        }
+#pragma unroll
+        for (int s = 0; s < 8; s++) c2f[s * L.plane + id] = c[s];
+    }
+}
+
+// Prolongation, sweep 2: 2-D faces (bbmg_class.f90:1052-1160).  Reads the
+// line weights of the in-plane neighbours written by sweep 1.  AXN is the
+// plane normal (0: yz-plane, 1: zx-plane, 2: xy-plane); PA is the in-plane
+// axis of the reference's inner loop, PB that of its outer loop.
+template <int AXN>
+__device__ __forceinline__ void face_weights(const Lay &L, const double *__restrict__ opr, double *__restrict__ c2f,
+                                             int i, int j, int k) {
+    constexpr int PA = AXN == 0 ? 1 : 0;
+    constexpr int PB = AXN == 2 ? 1 : 2;
+    const double ratio = 10.0;
+    const int ia[3] = {i, j, k};
+    const int na[3] = {L.nx, L.ny, L.nz};
+    if (ia[PA] == -1 || ia[PA] == na[PA] || ia[PB] == -1 || ia[PB] == na[PB]) return;
+    const long long id = L.idx(i, j, k);
+    double o2[9];  // opr2d(a,b) at (a+1) + 3(b+1)
+#pragma unroll
+    for (int e = 0; e < 9; e++) o2[e] = 0.0;
+#pragma unroll 1
+    for (int q = 0; q < 27; q++) {
+        int l[3] = {q % 3 - 1, (q / 3) % 3 - 1, q / 9 - 1};
+        int la = l[PA], lb = l[PB];
+        int lr[3] = {l[0], l[1], l[2]};
+        lr[AXN] = 0;
+        double a = opr[q * L.plane + id];
+        int e = __dmul_rn(ratio, fabs(opr[q27(lr[0], lr[1], lr[2]) * L.plane + id])) >= fabs(a) ? (la + 1) + 3 * (lb + 1) : 4;
+        o2[e] = __dadd_rn(o2[e], a);
+    }
+    const double o00 = sgn_clamp(o2[4]);
+    double c[8];
+#pragma unroll
+    for (int t = 0; t < 8; t++) c[t] = c2f[t * L.plane + id];
+#pragma unroll 1
+    for (int lb = -1; lb <= 1; lb++)
+#pragma unroll 1
+        for (int la = -1; la <= 1; la++) {
+            if (la == 0 && lb == 0) continue;
+            int off[3] = {0, 0, 0};
+            off[PA] = la; off[PB] = lb;
+            const long long nid = L.idx(i + off[0], j + off[1], k + off[2]);
+            const double w = o2[(la + 1) + 3 * (lb + 1)] / o00;
+#pragma unroll 1
+            for (int qb = 0; qb <= 1 - abs(lb); qb++)
+#pragma unroll 1
+                for (int qa = 0; qa <= 1 - abs(la); qa++) {
+                    int s3[3] = {0, 0, 0}, p3[3] = {0, 0, 0};
+                    s3[PA] = (la + 1) / 2 + qa; s3[PB] = (lb + 1) / 2 + qb;
+                    p3[PA] = qa; p3[PB] = qb;
+                    const int so = q8(s3[0], s3[1], s3[2]);
+                    const double cn = c2f[q8(p3[0], p3[1], p3[2]) * L.plane + nid];
+                    c[so] = __dsub_rn(c[so], __dmul_rn(w, cn));
+                }
+        }
+#pragma unroll
+    for (int t = 0; t < 8; t++) c2f[t * L.plane + id] = c[t];
+}
+
+__global__ void k_prolong_sweep2(Lay L, const double *__restrict__ opr, double *__restrict__ c2f) {
+    long long total = (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
+    for (long long t = gtid(); t < total; t += gstride()) {
+        int i, j, k;
+        any_cell(L, t, i, j, k);
+        int n1 = pmod(L.xper, i, L.nx), n2 = pmod(L.yper, j, L.ny), n3 = pmod(L.zper, k, L.nz);
+        if (n1 + n2 + n3 != 2) continue;
+        if (n1 == 0) face_weights<0>(L, opr, c2f, i, j, k);
+        else if (n2 == 0) face_weights<1>(L, opr, c2f, i, j, k);
+        else face_weights<2>(L, opr, c2f, i, j, k);
+    }
+}
+
+// Prolongation, sweep 3: cube centres, interior only (bbmg_class.f90:1161-1194).
+__global__ void k_prolong_sweep3(Lay L, const double *__restrict__ opr, double *__restrict__ c2f) {
+    long long total = (long long)L.nx * L.ny * L.nz;
+    for (long long t = gtid(); t < total; t += gstride()) {
+        int i, j, k;
+        interior_cell(L, t, i, j, k);
+        int n1 = pmod(L.xper, i, L.nx), n2 = pmod(L.yper, j, L.ny), n3 = pmod(L.zper, k, L.nz);
+        if (n1 + n2 + n3 != 3) continue;
+        long long id = L.idx(i, j, k);
+        double d = sgn_clamp(opr[kCentre27 * L.plane + id]);
+        double c[8];
+#pragma unroll
+        for (int s = 0; s < 8; s++) c[s] = c2f[s * L.plane + id];
+#pragma unroll 1
+        for (int q = 0; q < 27; q++) {
+            if (q == kCentre27) continue;
+            int li = q % 3 - 1, lj = (q / 3) % 3 - 1, lk = q / 9 - 1;
+            long long nid = L.idx(i + li, j + lj, k + lk);
+            double w = opr[q * L.plane + id] / d;
+            for (int pk = 0; pk <= 1 - abs(lk); pk++)
+                for (int pj = 0; pj <= 1 - abs(lj); pj++)
+                    for (int pi = 0; pi <= 1 - abs(li); pi++) {
+                        int so = q8((li + 1) / 2 + pi, (lj + 1) / 2 + pj, (lk + 1) / 2 + pk);
+                        c[so] = __dsub_rn(c[so], __dmul_rn(w, c2f[q8(pi, pj, pk) * L.plane + nid]));
+                    }
+        }
+#pragma unroll
+        for (int s = 0; s < 8; s++) c2f[s * L.plane + id] = c[s];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Restriction weights f2c(r, c) = c2f((1-r)/2, 2c+r) over the parity ranges
+// (bbmg_class.f90:1201-1231).  F is the fine level, C the coarse one; f2c is
+// zero beforehand.
+__global__ void k_restriction_weights(Lay F, Lay C, const double *__restrict__ c2f, double *__restrict__ f2c) {
+    long long total = (long long)C.nx * C.ny * C.nz;
+    for (long long t = gtid(); t < total; t += gstride()) {
+        int ci, cj, ck;
+        interior_cell(C, t, ci, cj, ck);
+        int fi = 2 * ci, fj = 2 * cj, fk = 2 * ck;
+        long long cid = C.idx(ci, cj, ck);
+        int rk0 = -pmod(F.zper, fk - 1, F.nz), rk1 = pmod(F.zper, fk + 1, F.nz);
+        int rj0 = -pmod(F.yper, fj - 1, F.ny), rj1 = pmod(F.yper, fj + 1, F.ny);
+        int ri0 = -pmod(F.xper, fi - 1, F.nx), ri1 = pmod(F.xper, fi + 1, F.nx);
+        for (int rk = rk0; rk <= rk1; rk++)
+            for (int rj = rj0; rj <= rj1; rj++)
+                for (int ri = ri0; ri <= ri1; ri++) {
+                    int pi = (1 - ri) / 2, pj = (1 - rj) / 2, pk = (1 - rk) / 2;
+                    f2c[q27(ri, rj, rk) * C.plane + cid] =
+                        c2f[q8(pi, pj, pk) * F.plane + F.idx(fi + ri, fj + rj, fk + rk)];
+                }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Galerkin operator, part 1: oprc2f = A P on the fine interior
+// (bbmg_class.f90:1245-1271).
+__global__ void k_rap_ap(Lay F, const double *__restrict__ opr, const double *__restrict__ c2f,
+                         double *__restrict__ oprc2f) {
+    long long total = (long long)F.nx * F.ny * F.nz;
+    for (long long t = gtid(); t < total; t += gstride()) {
+        int fi, fj, fk;
+        interior_cell(F, t, fi, fj, fk);
+        long long id = F.idx(fi, fj, fk);
+        int px0 = pmod(F.xper, fi, F.nx), py0 = pmod(F.yper, fj, F.ny), pz0 = pmod(F.zper, fk, F.nz);
+        double acc[27];
+#pragma unroll
+        for (int q = 0; q < 27; q++) acc[q] = 0.0;
+#pragma unroll 1
+        for (int q = 0; q < 27; q++) {
+            int li = q % 3 - 1, lj = (q / 3) % 3 - 1, lk = q / 9 - 1;
+            int pxl = pmod(F.xper, fi + li, F.nx), pyl = pmod(F.yper, fj + lj, F.ny), pzl = pmod(F.zper, fk + lk, F.nz);
+            double o = opr[q * F.plane + id];
+            long long nid = F.idx(fi + li, fj + lj, fk + lk);
+            for (int pk = 0; pk <= pzl; pk++)
+                for (int pj = 0; pj <= pyl; pj++)
+                    for (int pi = 0; pi <= pxl; pi++) {
+                        int si = pi + (1 - px0) * min(li, 0) + (1 - pxl) * max(li, 0);
+                        int sj = pj + (1 - py0) * min(lj, 0) + (1 - pyl) * max(lj, 0);
+                        int sk = pk + (1 - pz0) * min(lk, 0) + (1 - pzl) * max(lk, 0);
+                        int so = q27(si, sj, sk);
+                        acc[so] = __dadd_rn(acc[so], __dmul_rn(o, c2f[q8(pi, pj, pk) * F.plane + nid]));
+                    }
+        }
+#pragma unroll
+        for (int q = 0; q < 27; q++) oprc2f[q * F.plane + id] = acc[q];
+    }
+}
+
+// Galerkin operator, part 2: A_c = R (A P) on the coarse interior
+// (bbmg_class.f90:1274-1300).  opr_c is zero beforehand.
+__global__ void k_rap_rap(Lay F, Lay C, const double *__restrict__ f2c, const double *__restrict__ oprc2f,
+                          double *__restrict__ oprc) {
+    long long total = (long long)C.nx * C.ny * C.nz;
+    for (long long t = gtid(); t < total; t += gstride()) {
+        int ci, cj, ck;
+        interior_cell(C, t, ci, cj, ck);
+        int fi = 2 * ci, fj = 2 * cj, fk = 2 * ck;
+        long long cid = C.idx(ci, cj, ck);
+        double acc[27];
+#pragma unroll
+        for (int q = 0; q < 27; q++) acc[q] = 0.0;
+        int rk0 = -pmod(F.zper, fk - 1, F.nz), rk1 = pmod(F.zper, fk + 1, F.nz);
+        int rj0 = -pmod(F.yper, fj - 1, F.ny), rj1 = pmod(F.yper, fj + 1, F.ny);
+        int ri0 = -pmod(F.xper, fi - 1, F.nx), ri1 = pmod(F.xper, fi + 1, F.nx);
+#pragma unroll 1
+        for (int rk = rk0; rk <= rk1; rk++)
+#pragma unroll 1
+            for (int rj = rj0; rj <= rj1; rj++)
+#pragma unroll 1
+                for (int ri = ri0; ri <= ri1; ri++) {
+                    double w = f2c[q27(ri, rj, rk) * C.plane + cid];
+                    long long nid = F.idx(fi + ri, fj + rj, fk + rk);
+                    int lk0 = -1 + pmod(F.zper, fk + rk, F.nz);
+                    int lj0 = -1 + pmod(F.yper, fj + rj, F.ny);
+                    int li0 = -1 + pmod(F.xper, fi + ri, F.nx);
+                    for (int lk = lk0; lk <= 1; lk++)
+                        for (int lj = lj0; lj <= 1; lj++)
+                            for (int li = li0; li <= 1; li++) {
+                                // (r-1)/2 truncates toward zero, as Fortran's integer division
+                                int so = q27((ri - 1) / 2 + li, (rj - 1) / 2 + lj, (rk - 1) / 2 + lk);
+                                acc[so] = __dadd_rn(acc[so], __dmul_rn(w, oprc2f[q27(li, lj, lk) * F.plane + nid]));
+                            }
+                }
+#pragma unroll
+        for (int q = 0; q < 27; q++) oprc[q * C.plane + cid] = acc[q];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Dense coarsest matrix (bbmg_class.f90:1307-1385): column-major np x np.
+// Thread `ind1` owns row ind1, so its accumulations keep the loop order.
+__global__ void k_dense_operator(Lay L, const double *__restrict__ opr, double *__restrict__ OP) {
+    int np = L.nx * L.ny * L.nz;
+    for (int ind1 = threadIdx.x + blockIdx.x * blockDim.x; ind1 < np; ind1 += blockDim.x * gridDim.x) {
+        int i1 = ind1 % L.nx, j1 = (ind1 / L.nx) % L.ny, k1 = ind1 / (L.nx * L.ny);
+        long long id = L.idx(i1, j1, k1);
+        for (int c = 0; c < np; c++) OP[(long long)c * np + ind1] = 0.0;
+        for (int sk = -1; sk <= 1; sk++) {
+            int k2 = k1 + sk;
+            if (k2 == L.nz) { if (!L.zper) continue; k2 = 0; }
+            if (k2 == -1) { if (!L.zper) continue; k2 = L.nz - 1; }
+            for (int sj = -1; sj <= 1; sj++) {
+                int j2 = j1 + sj;
+                if (j2 == L.ny) { if (!L.yper) continue; j2 = 0; }
+                if (j2 == -1) { if (!L.yper) continue; j2 = L.ny - 1; }
+                for (int si = -1; si <= 1; si++) {
+                    int i2 = i1 + si;
+                    if (i2 == L.nx) { if (!L.xper) continue; i2 = 0; }
+                    if (i2 == -1) { if (!L.xper) continue; i2 = L.nx - 1; }
+                    int ind2 = i2 + j2 * L.nx + k2 * L.nx * L.ny;
+                    long long e = (long long)ind2 * np + ind1;
+                    OP[e] = __dadd_rn(OP[e], opr[q27(si, sj, sk) * L.plane + id]);
+                }
+            }
+        }
+    }
+}
+
+// Unblocked LU with row partial pivoting on a column-major n x n matrix, one
+// thread block (the DGESV factorisation of bbmg_class.f90:912-913, done once
+// per setup because the reference's per-call factorisation is deterministic).
+// Pivot: the first row holding the largest magnitude.  Then marks the
+// unknowns whose pivot is below n*eps*max|pivot| (a singular coarsest
+// matrix); the solve sets those to zero.
+__global__ void k_lu(double *__restrict__ A, int n, int *__restrict__ piv, int *__restrict__ pinned,
+                     int *__restrict__ info_out) {
+    __shared__ double sval[1024];
+    __shared__ int sidx[1024];
+    __shared__ int s_info;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    if (tid == 0) s_info = 0;
+    __syncthreads();
+    for (int j = 0; j < n; j++) {
+        // argmax |A(i,j)|, i >= j; ties -> smallest index
+        double best = -1.0;
+        int bi = n;
+        for (int i = j + tid; i < n; i += nt) {
+            double a = fabs(A[(long long)j * n + i]);
+            if (a > best || (a == best && i < bi)) { best = a; bi = i; }
+        }
+        sval[tid] = best; sidx[tid] = bi;
+        __syncthreads();
+        for (int s = nt / 2; s > 0; s >>= 1) {
+            if (tid < s) {
+                double a = sval[tid + s]; int ia = sidx[tid + s];
+                if (a > sval[tid] || (a == sval[tid] && ia < sidx[tid])) { sval[tid] = a; sidx[tid] = ia; }
+            }
+            __syncthreads();
+        }
+        int p = sidx[0];
+        if (p >= n) p = j;
+        __syncthreads();
+        double pv = A[(long long)j * n + p];
+        if (tid == 0) piv[j] = p;
+        if (pv != 0.0) {
+            if (p != j)
+                for (int c = tid; c < n; c += nt) {
+                    double x = A[(long long)c * n + j];
+                    A[(long long)c * n + j] = A[(long long)c * n + p];
+                    A[(long long)c * n + p] = x;
+                }
+            __syncthreads();
+            double d = A[(long long)j * n + j];
+            for (int i = j + 1 + tid; i < n; i += nt) A[(long long)j * n + i] = A[(long long)j * n + i] / d;
+        } else if (tid == 0 && s_info == 0) {
+            s_info = j + 1;
+        }
+        __syncthreads();
+        long long m = (long long)(n - j - 1) * (n - j - 1);
+        for (long long e = tid; e < m; e += nt) {
+            int c = j + 1 + (int)(e / (n - j - 1));
+            int i = j + 1 + (int)(e % (n - j - 1));
+            A[(long long)c * n + i] = __dsub_rn(A[(long long)c * n + i], __dmul_rn(A[(long long)j * n + i], A[(long long)c * n + j]));
+        }
+        __syncthreads();
+    }
+    // pin round-off pivots
+    double umax = 0.0;
+    for (int k = tid; k < n; k += nt) umax = fmax(umax, fabs(A[(long long)k * n + k]));
+    sval[tid] = umax;
+    __syncthreads();
+    for (int s = nt / 2; s > 0; s >>= 1) {
+        if (tid < s) sval[tid] = fmax(sval[tid], sval[tid + s]);
+        __syncthreads();
+    }
+    double tol = (double)n * kEps * sval[0];
+    for (int k = tid; k < n; k += nt) pinned[k] = fabs(A[(long long)k * n + k]) <= tol ? 1 : 0;
+    if (tid == 0) *info_out = s_info;
+}
+
+// ---------------------------------------------------------------------------
+// host launchers
+#define BB_LAUNCH_CHECK() do { cudaError_t e_ = cudaGetLastError(); if (e_ != cudaSuccess) return e_; } while (0)
+
+cudaError_t setup_scatter(const Lay &L, const double *src, int nst, int g, const int *stc, double *opr, cudaStream_t s) {
+    long long n = (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
+    k_scatter_operator<<<grid_for(n, 128), 128, 0, s>>>(L, src, nst, g, stc, opr);
+    BB_LAUNCH_CHECK();
+    return cudaSuccess;
+}
+
+cudaError_t wrap_planes(const Lay &L, double *a, int nplanes, cudaStream_t s) {
+    if (!(L.xper || L.yper || L.zper)) return cudaSuccess;
+    long long n = (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
+    k_wrap<<<grid_for(n, 256), 256, 0, s>>>(L, a, nplanes);
+    BB_LAUNCH_CHECK();
+    return cudaSuccess;
+}
+
+cudaError_t wrap_planes(const Lay &L, float *a, int nplanes, cudaStream_t s) {
+    if (!(L.xper || L.yper || L.zper)) return cudaSuccess;
+    long long n = (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
+    k_wrap_f<<<grid_for(n, 256), 256, 0, s>>>(L, a, nplanes);
+    BB_LAUNCH_CHECK();
+    return cudaSuccess;
+}
+
+cudaError_t setup_prolongation(const Lay &L, const double *opr, double *c2f, cudaStream_t s) {
+    long long na = (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
+    long long ni = (long long)L.nx * L.ny * L.nz;
+    k_prolong_sweep1<<<grid_for(na, 128), 128, 0, s>>>(L, opr, c2f);
+    BB_LAUNCH_CHECK();
+    k_prolong_sweep2<<<grid_for(na, 128), 128, 0, s>>>(L, opr, c2f);
+    BB_LAUNCH_CHECK();
+    k_prolong_sweep3<<<grid_for(ni, 128), 128, 0, s>>>(L, opr, c2f);
+    BB_LAUNCH_CHECK();
+    return wrap_planes(L, c2f, 8, s);
+}
+
+cudaError_t setup_restriction(const Lay &F, const Lay &C, const double *c2f, double *f2c, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(f2c, 0, sizeof(double) * 27 * C.plane, s);
+    if (e != cudaSuccess) return e;
+    long long n = (long long)C.nx * C.ny * C.nz;
+    k_restriction_weights<<<grid_for(n, 128), 128, 0, s>>>(F, C, c2f, f2c);
+    BB_LAUNCH_CHECK();
+    return wrap_planes(C, f2c, 27, s);
+}
+
+cudaError_t setup_operator(const Lay &F, const Lay &C, const double *oprF, const double *c2f, const double *f2c,
+                           double *oprc2f, double *oprC, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(oprc2f, 0, sizeof(double) * 27 * F.plane, s);
+    if (e != cudaSuccess) return e;
+    long long nf = (long long)F.nx * F.ny * F.nz;
+    k_rap_ap<<<grid_for(nf, 128), 128, 0, s>>>(F, oprF, c2f, oprc2f);
+    BB_LAUNCH_CHECK();
+    if ((e = wrap_planes(F, oprc2f, 27, s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(oprC, 0, sizeof(double) * 27 * C.plane, s)) != cudaSuccess) return e;
+    long long nc = (long long)C.nx * C.ny * C.nz;
+    k_rap_rap<<<grid_for(nc, 128), 128, 0, s>>>(F, C, f2c, oprc2f, oprC);
+    BB_LAUNCH_CHECK();
+    return wrap_planes(C, oprC, 27, s);
+}
+
+cudaError_t setup_direct(const Lay &L, const double *opr, double *OP, double *LU, int *piv, int *pinned, int *info,
+                         cudaStream_t s) {
+    int np = L.nx * L.ny * L.nz;
+    k_dense_operator<<<(np + 127) / 128, 128, 0, s>>>(L, opr, OP);
+    BB_LAUNCH_CHECK();
+    cudaError_t e = cudaMemcpyAsync(LU, OP, sizeof(double) * (size_t)np * np, cudaMemcpyDeviceToDevice, s);
+    if (e != cudaSuccess) return e;
+    k_lu<<<1, 1024, 0, s>>>(LU, np, piv, pinned, info);
+    BB_LAUNCH_CHECK();
+    return cudaSuccess;
+}
+
+}  // namespace bbmg

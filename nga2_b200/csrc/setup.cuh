@@ -1,0 +1,66 @@
+// setup.cuh -- launchers of the setup and solve kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace bbmg {
+
+// setup.cu (FP64)
+cudaError_t setup_scatter(const Lay &L, const double *src, int nst, int g, const int *stc, double *opr, cudaStream_t s);
+cudaError_t wrap_planes(const Lay &L, double *a, int nplanes, cudaStream_t s);
+cudaError_t wrap_planes(const Lay &L, float *a, int nplanes, cudaStream_t s);
+cudaError_t setup_prolongation(const Lay &L, const double *opr, double *c2f, cudaStream_t s);
+cudaError_t setup_restriction(const Lay &F, const Lay &C, const double *c2f, double *f2c, cudaStream_t s);
+cudaError_t setup_operator(const Lay &F, const Lay &C, const double *oprF, const double *c2f, const double *f2c,
+                           double *oprc2f, double *oprC, cudaStream_t s);
+cudaError_t setup_direct(const Lay &L, const double *opr, double *OP, double *LU, int *piv, int *pinned, int *info,
+                         cudaStream_t s);
+
+// solve.cu
+template <typename T>
+cudaError_t launch_relax(const Lay &L, const NbrOff &nb, int npt, bool fuse, const T *opr, T *v, const T *f, int dir,
+                         cudaStream_t s);
+template <typename T>
+cudaError_t launch_residual(const Lay &L, const NbrOff &nb, int npt, const T *opr, const T *v, const T *f, T *r,
+                            cudaStream_t s);
+template <typename T>
+cudaError_t launch_restrict(const Lay &F, const Lay &C, const T *c2f, const T *rF, T *fC, T *vC, cudaStream_t s);
+template <typename T>
+cudaError_t launch_prolong(const Lay &F, const Lay &C, const T *c2f, const T *vC, T *vF, cudaStream_t s);
+constexpr size_t kCoarseSmem = 200 * 1024;  // factors of up to 158 unknowns stay on chip
+cudaError_t coarse_solve_prepare();  // per device, before the first coarse solve
+template <typename T>
+cudaError_t launch_coarse_solve(const Lay &L, const double *LU, const int *piv, const int *pinned, const T *f, T *v,
+                                cudaStream_t s);
+
+// reductions (deterministic two-pass) into a device double
+constexpr int kRedBlocks = 592;  // 4 per SM on 148 SMs
+template <typename T>
+cudaError_t launch_maxabs(const Lay &L, const T *x, double *part, double *out, cudaStream_t s);
+template <typename T>
+cudaError_t launch_dot(const Lay &L, const T *a, const T *b, double *part, double *out, cudaStream_t s);
+
+// PCG scalars (device resident)
+struct CgScal {
+    double rho1, rho2, pap, alpha, beta;
+    int iter, pad;
+};
+template <typename TZ>
+cudaError_t launch_cg_rho(const Lay &L, const TZ *zz, const double *res, double *part, CgScal *sc, cudaStream_t s);
+template <typename TZ>
+cudaError_t launch_cg_p(const Lay &L, const TZ *zz, double *pp, const CgScal *sc, cudaStream_t s);
+cudaError_t launch_cg_pap(const Lay &L, const double *pp, const double *Ap, double *part, CgScal *sc, cudaStream_t s);
+cudaError_t launch_cg_xr(const Lay &L, double *sol, const double *pp, double *res, const double *Ap, const CgScal *sc,
+                         cudaStream_t s);
+cudaError_t launch_round_f32(const Lay &L, const double *r, float *f, cudaStream_t s);
+cudaError_t launch_add_correction(const Lay &L, double *x, const float *e, cudaStream_t s);
+
+// caller I/O: Fortran arrays with g overlap layers <-> level interior
+template <typename T>
+cudaError_t launch_from_caller(const Lay &L, const double *src, int g, T *dst, cudaStream_t s);
+cudaError_t launch_to_caller(const Lay &L, const double *src, int g, double *dst, cudaStream_t s);
+// FP64 level arrays <-> FP32 copies (planes)
+cudaError_t launch_to_f32(const double *src, float *dst, long long n, cudaStream_t s);
+
+}  // namespace bbmg

@@ -1,0 +1,199 @@
+"""GPU parity: every stage of the CUDA solver against the CPU oracle.
+
+FP64 stages are compared bit for bit (np.array_equal; the kernels keep the
+reference's term order and use no FMA contraction).  The PCG's dot products are
+parallel reductions on the GPU and sequential sums in the oracle, so pcg_bbox is
+compared by iteration count and solution difference; the mixed-precision solver
+by residual (<= 1e-10) and solution difference against the FP64 oracle.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from nga2_b200 import problems as P
+from nga2_b200.bbmg import BBMG, BBOX, FP64, MIXED, PCG_BBOX
+from oracle.oracle import OracleBBMG, fft_solve_periodic
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+CASES = [((8, 8, 8), (True, True, True)), ((12, 10, 9), (True, False, True)), ((9, 7, 5), (False, False, False)),
+         ((17, 17, 17), (True, True, True)), ((32, 32, 1), (True, True, False)), ((10, 6, 12), (False, True, False)),
+         ((13, 8, 11), (True, True, True))]
+IDS = ["x".join(map(str, d)) + "-" + "".join("p" if p else "w" for p in per) for d, per in CASES]
+
+
+def sync_np(a, per):
+    """The reference's overlap copy (vsync on one rank) on a padded numpy array."""
+    a = a.copy()
+    if per[0]:
+        a[:, :, -1] = a[:, :, 1]; a[:, :, 0] = a[:, :, -2]
+    if per[1]:
+        a[:, -1, :] = a[:, 1, :]; a[:, 0, :] = a[:, -2, :]
+    if per[2]:
+        a[-1, :, :] = a[1, :, :]; a[0, :, :] = a[-2, :, :]
+    return a
+
+
+def rand_vec(shape, per, rng):
+    a = np.zeros(shape)
+    a[1:-1, 1:-1, 1:-1] = rng.standard_normal((shape[0] - 2, shape[1] - 2, shape[2] - 2))
+    return sync_np(a, per)
+
+
+def make_pair(dims, per, method=BBOX, seed=7, full27=False, precision=FP64, **kw):
+    stc, opr = P.random_operator(*dims, per, seed=seed, full27=full27)
+    o = OracleBBMG(*dims, *per, method=method, **kw)
+    o.setup(stc, opr)
+    g = BBMG(*dims, *per, method=method, precision=precision, **kw)
+    g.setup(stc, opr)
+    return o, g
+
+
+@pytest.mark.parametrize("full27", [False, True])
+@pytest.mark.parametrize("dims,per", CASES, ids=IDS)
+def test_setup_bitexact(dims, per, full27):
+    """update(): operators, prolongation, restriction, A*P on every level and the
+    dense coarsest matrix with its LU equal the oracle's bit for bit."""
+    o, g = make_pair(dims, per, full27=full27, ncell_coarsest=0 if dims[0] < 12 else 300)
+    assert g.nlvl == o.nlvl
+    for n in range(1, o.nlvl + 1):
+        assert g.level_dims(n) == o.level_dims(n)
+        names = ["opr"] + (["c2f", "oprc2f"] if n < o.nlvl else []) + (["f2c"] if n > 1 else [])
+        for w in names:
+            a, b = g.get(n, w), o.get(n, w)
+            assert np.array_equal(a, b), (n, w, np.abs(a - b).max())
+    op, lu, piv = g.direct()
+    OP, LU, PIV, info = o.direct()
+    assert np.array_equal(op, OP) and np.array_equal(lu, LU) and np.array_equal(piv, PIV)
+
+
+@pytest.mark.parametrize("dims,per", CASES, ids=IDS)
+def test_solve_steps_bitexact(dims, per):
+    """relax(+1/-1), get_residual, f2c, c2f+correction, direct_solve and a full
+    cycle(1) from the same state equal the oracle bit for bit."""
+    o, g = make_pair(dims, per, full27=(dims[2] == 11))
+    rng = np.random.default_rng(1)
+    nl = o.nlvl
+    for n in range(1, nl + 1):
+        nx, ny, nz = o.level_dims(n)
+        shp = (nz + 2, ny + 2, nx + 2)
+        v, f = rand_vec(shp, per, rng), rand_vec(shp, per, rng)
+        for obj in (o, g):
+            obj.put(n, "v", v); obj.put(n, "f", f)
+        for d in (1, -1):
+            o.relax(n, d); g.step("relax", n, d)
+            assert np.array_equal(g.get(n, "v"), o.get(n, "v")), ("relax", n, d)
+        o.residual(n); g.step("residual", n)
+        assert np.array_equal(g.get(n, "r"), o.get(n, "r")), ("residual", n)
+        if n < nl:
+            o.restrict(n); g.step("restrict", n)
+            assert np.array_equal(g.get(n + 1, "f"), o.get(n + 1, "f")), ("restrict", n)
+            nxc, nyc, nzc = o.level_dims(n + 1)
+            vc = rand_vec((nzc + 2, nyc + 2, nxc + 2), per, rng)
+            o.put(n + 1, "v", vc); g.put(n + 1, "v", vc)
+            o.prolong(n + 1)
+            # the reference prolongs into r and then adds r to v (bbmg_class.f90:768-770)
+            vo = o.get(n, "v") + o.get(n, "r")
+            g.step("prolong", n)
+            assert np.array_equal(g.get(n, "v"), vo), ("prolong", n)
+    # coarsest direct solve
+    nx, ny, nz = o.level_dims(nl)
+    f = rand_vec((nz + 2, ny + 2, nx + 2), per, rng)
+    o.put(nl, "f", f); g.put(nl, "f", f)
+    o.direct_solve(); g.step("direct", nl)
+    assert np.array_equal(g.get(nl, "v"), o.get(nl, "v"))
+    # a whole V-cycle from level 1
+    nx, ny, nz = o.level_dims(1)
+    v, f = rand_vec((nz + 2, ny + 2, nx + 2), per, rng), rand_vec((nz + 2, ny + 2, nx + 2), per, rng)
+    for obj in (o, g):
+        obj.put(1, "v", v); obj.put(1, "f", f)
+    o.cycle(1); g.step("cycle", 1)
+    assert np.array_equal(g.get(1, "v"), o.get(1, "v"))
+
+
+@pytest.mark.parametrize("dims,per", CASES, ids=IDS)
+def test_bbox_solve_bitexact(dims, per):
+    """Stationary V-cycles (mgsolve): same it, rerr and solution bits."""
+    stc, opr = P.random_operator(*dims, per, seed=3)
+    rng = np.random.default_rng(3)
+    rhs = rng.standard_normal(dims[::-1])
+    rhs -= rhs.mean()
+    o = OracleBBMG(*dims, *per, method=BBOX, maxit=30, rcvg=1e-10)
+    o.setup(stc, opr)
+    xo, ito, ro = o.solve(rhs)
+    g = BBMG(*dims, *per, method=BBOX, maxit=30, rcvg=1e-10)
+    g.setup(stc, opr)
+    xg, itg, rg, st = g.solve(rhs)
+    assert itg == ito and rg == ro
+    assert np.array_equal(xg, xo)
+
+
+@pytest.mark.parametrize("dims,per", CASES, ids=IDS)
+def test_pcg_solve(dims, per):
+    """V-cycle preconditioned CG (cgsolve): the dot products are reduced in a
+    different order, so iteration counts may differ by one and the solutions by
+    round-off amplified through the iteration."""
+    stc, opr = P.random_operator(*dims, per, seed=4)
+    rng = np.random.default_rng(4)
+    rhs = rng.standard_normal(dims[::-1]); rhs -= rhs.mean()
+    o = OracleBBMG(*dims, *per, method=PCG_BBOX, maxit=50, rcvg=1e-10)
+    o.setup(stc, opr)
+    xo, ito, ro = o.solve(rhs)
+    g = BBMG(*dims, *per, method=PCG_BBOX, maxit=50, rcvg=1e-10)
+    g.setup(stc, opr)
+    xg, itg, rg, st = g.solve(rhs)
+    assert st == 0 and rg <= 1e-10
+    assert abs(itg - ito) <= 1
+    d = np.abs(P.remove_mean(xg) - P.remove_mean(xo)).max() / np.abs(P.remove_mean(xo)).max()
+    assert d < 1e-8, d
+
+
+@pytest.mark.parametrize("name", ["periodic16", "walls16", "drops24"])
+def test_golden_fixtures_gpu(name):
+    """The committed fixtures: bbox reproduces the oracle bits, pcg_bbox to 1e-8."""
+    from tests.golden.make_golden import make_case
+    ref = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    pb, m = make_case(name)
+    g = BBMG(pb.nx, pb.ny, pb.nz, pb.xper, pb.yper, pb.zper, method=m, rcvg=1e-10)
+    g.setup(pb.stc, pb.opr)
+    x, it, rerr, st = g.solve(pb.rhs)
+    if m == BBOX:
+        assert it == int(ref["it"]) and rerr == float(ref["rerr"]) and np.array_equal(x, ref["sol"])
+    else:
+        assert abs(it - int(ref["it"])) <= 1 and rerr <= 1e-10
+        xr = ref["sol"]
+        assert np.abs(P.remove_mean(x) - P.remove_mean(xr)).max() <= 1e-8 * np.abs(xr).max()
+
+
+@pytest.mark.parametrize("method", [BBOX, PCG_BBOX])
+def test_mixed_precision_matches_fp64(method):
+    """FP32 V-cycle inside the FP64 outer iteration reaches rerr <= 1e-10; its
+    solution agrees with the FP64 oracle's after mean removal."""
+    pb = P.drops_poisson(32, seed=5, ndrops=6, rmin=2.0, rmax=5.0)
+    o = OracleBBMG(32, 32, 32, True, False, True, method=PCG_BBOX, rcvg=1e-12)
+    o.setup(pb.stc, pb.opr)
+    xo, _, _ = o.solve(pb.rhs)
+    g = BBMG(32, 32, 32, True, False, True, method=method, precision=MIXED, rcvg=1e-10, maxit=60)
+    g.setup(pb.stc, pb.opr)
+    xg, it, rerr, st = g.solve(pb.rhs)
+    assert st == 0 and rerr <= 1e-10, (st, it, rerr)
+    d = np.abs(P.remove_mean(xg) - P.remove_mean(xo)).max() / np.abs(P.remove_mean(xo)).max()
+    assert d < 1e-7, d
+
+
+@pytest.mark.parametrize("precision", [FP64, MIXED])
+@pytest.mark.parametrize("method", [BBOX, PCG_BBOX])
+def test_periodic_64_known_answer(method, precision):
+    """64^3 triply periodic Laplacian (the CPU-runnable configuration) against its
+    exact FFT solution."""
+    pb = P.periodic_poisson(64, seed=1)
+    exact = fft_solve_periodic(pb.opr, pb.rhs)
+    g = BBMG(64, 64, 64, True, True, True, method=method, precision=precision, rcvg=1e-10)
+    g.setup(pb.stc, pb.opr)
+    x, it, rerr, st = g.solve(pb.rhs)
+    assert st == 0 and rerr <= 1e-10
+    err = np.abs(P.remove_mean(x) - exact).max() / np.abs(exact).max()
+    assert err < 1e-8, err
