@@ -85,6 +85,7 @@ typedef struct {
     long long device_bytes;/* device memory held by the handle               */
     int status;            /* status of the last solve                       */
     long long launches;    /* kernel launches of the last solve              */
+    int level1_stencil;    /* level-1 storage: 27, 7, or 4 (symmetric 7-pt)  */
 } bbmg_info;
 
 /* Fill `p` with the ILS values: pcg_bbox, FP64, V(2,2), ncell_coarsest 300,

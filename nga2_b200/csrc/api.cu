@@ -29,6 +29,7 @@ struct Level {
     // FP64
     double *opr27 = nullptr;   // 27 planes: the reference's operator
     double *oprS = nullptr;    // solve stencil planes (== opr27 when npt == 27)
+    int nS = 0;                // planes allocated in oprS when it is not opr27
     double *c2f = nullptr, *f2c = nullptr, *oprc2f = nullptr;
     double *v = nullptr, *f = nullptr, *r = nullptr;
     // FP32 (mixed precision)
@@ -66,9 +67,10 @@ struct bbmg_handle {
     // coarsest dense problem
     int np = 0, lu_info = 0, npinned = 0;
     double *OP = nullptr, *LU = nullptr;
-    int *piv = nullptr, *pinned = nullptr, *d_info = nullptr;
+    int *piv = nullptr, *pinned = nullptr, *d_info = nullptr, *d_flag = nullptr;
     // Krylov / outer iteration vectors (level-1 layout)
-    double *sol = nullptr, *pp = nullptr, *Ap = nullptr;
+    double *sol = nullptr, *pp = nullptr, *pp2 = nullptr, *Ap = nullptr;  // pp/pp2 alternate per iteration
+    double *x2 = nullptr;  // second solution buffer of the mixed defect correction (alternates with lv[1].v)
     CgScal *sc = nullptr;
     double *part = nullptr, *dscal = nullptr;  // reduction partials; [0]=res0 [1]=res
     double *h_scal = nullptr;                  // pinned host mirror of dscal
@@ -81,8 +83,9 @@ struct bbmg_handle {
     bool setup_done = false;
     int npt1 = 27;
     // graphs of one iteration: [mode] 0 = FP64 MG, 1 = FP64 PCG, 2 = mixed MG, 3 = mixed PCG
-    cudaGraphExec_t gexec[4] = {nullptr, nullptr, nullptr, nullptr};
-    int gkernels[4] = {0, 0, 0, 0};  // kernel nodes per graph
+    // graphs [mode][parity of the iteration] (the CG direction vectors alternate buffers)
+    cudaGraphExec_t gexec[4][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
+    int gkernels[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};  // kernel nodes per graph
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     long long bytes = 0;
     std::string err;
@@ -142,11 +145,12 @@ bool is_device_ptr(const void *p) {
 inline int odiv(int n) { return n / 2 + n % 2; }  // bbmg_class.f90:147-151
 
 void drop_graphs(bbmg_handle *h) {
-    for (auto &g : h->gexec)
-        if (g) {
-            cudaGraphExecDestroy(g);
-            g = nullptr;
-        }
+    for (auto &gm : h->gexec)
+        for (auto &g : gm)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
 }
 
 // ---------------------------------------------------------------------------
@@ -160,20 +164,14 @@ int vcycle(bbmg_handle *h, int n) {
         if (h->prm.use_direct_solve) {
             CU(h, launch_coarse_solve<T>(l.L, h->LU, h->piv, h->pinned, P::f(l), P::v(l), s));
         } else {
-            int dir = 1;
-            for (int i = 0; i < h->prm.relax_pre + h->prm.relax_post; i++) {
-                CU(h, launch_relax<T>(l.L, l.nb, l.npt, l.fuse, P::opr(l), P::v(l), P::f(l), dir, s));
-                dir = -dir;
-            }
+            CU(h, launch_relax_sweeps<T>(l.L, l.nb, l.npt, l.fuse, P::opr(l), P::v(l), P::f(l), 1,
+                                         h->prm.relax_pre + h->prm.relax_post, s));
         }
         return BBMG_OK;
     }
     Level &c = h->lv[n + 1];
-    int dir = 1;
-    for (int i = 0; i < h->prm.relax_pre; i++) {
-        CU(h, launch_relax<T>(l.L, l.nb, l.npt, l.fuse, P::opr(l), P::v(l), P::f(l), dir, s));
-        dir = -dir;
-    }
+    CU(h, launch_relax_sweeps<T>(l.L, l.nb, l.npt, l.fuse, P::opr(l), P::v(l), P::f(l), 1, h->prm.relax_pre, s));
+    const int dir = (h->prm.relax_pre & 1) ? -1 : 1;
     CU(h, launch_residual<T>(l.L, l.nb, l.npt, P::opr(l), P::v(l), P::f(l), P::r(l), s));
     CU(h, launch_restrict<T>(l.L, c.L, P::c2f(l), P::r(l), P::f(c), P::v(c), s));
     for (int i = 0; i < h->prm.ncycle; i++) {
@@ -183,18 +181,17 @@ int vcycle(bbmg_handle *h, int n) {
         if (st) return st;
     }
     CU(h, launch_prolong<T>(l.L, c.L, P::c2f(l), P::v(c), P::v(l), s));
-    for (int i = 0; i < h->prm.relax_post; i++) {
-        CU(h, launch_relax<T>(l.L, l.nb, l.npt, l.fuse, P::opr(l), P::v(l), P::f(l), dir, s));
-        dir = -dir;
-    }
+    CU(h, launch_relax_sweeps<T>(l.L, l.nb, l.npt, l.fuse, P::opr(l), P::v(l), P::f(l), dir, h->prm.relax_post, s));
     return BBMG_OK;
 }
 
-// One iteration of each solver, written once into a graph.
-int record_iteration(bbmg_handle *h, int mode) {
+// One iteration of each solver, written once into a graph.  `par` selects
+// which of the two CG direction buffers is the old one.
+int record_iteration(bbmg_handle *h, int mode, int par) {
     cudaStream_t s = h->stream;
     Level &l1 = h->lv[1];
     const Lay &L = l1.L;
+    double *pp_old = par ? h->pp2 : h->pp, *pp_new = par ? h->pp : h->pp2;
     int st = BBMG_OK;
     switch (mode) {
     case 0:  // FP64 mgsolve: cycle; residual; max|r| (bbmg_class.f90:716-722)
@@ -202,48 +199,38 @@ int record_iteration(bbmg_handle *h, int mode) {
         CU(h, launch_residual<double>(L, l1.nb, l1.npt, l1.oprS, l1.v, l1.f, l1.r, s));
         CU(h, launch_maxabs<double>(L, l1.r, h->part, h->dscal + 1, s));
         break;
-    case 1:  // FP64 cgsolve body; res lives in l1.f (bbmg_class.f90:655-695)
-        CU(h, cudaMemsetAsync(l1.v, 0, sizeof(double) * L.plane, s));
+    case 1:  // FP64 cgsolve body, v zeroed by the previous step; res lives in l1.f
         if ((st = vcycle<double>(h, 1))) return st;
         CU(h, launch_cg_rho<double>(L, l1.v, l1.f, h->part, h->sc, s));
-        CU(h, launch_cg_p<double>(L, l1.v, h->pp, h->sc, s));
-        CU(h, launch_residual<double>(L, l1.nb, l1.npt, l1.oprS, h->pp, nullptr, h->Ap, s));
-        CU(h, launch_cg_pap(L, h->pp, h->Ap, h->part, h->sc, s));
-        CU(h, launch_cg_xr(L, h->sol, h->pp, l1.f, h->Ap, h->sc, s));
-        CU(h, launch_maxabs<double>(L, l1.f, h->part, h->dscal + 1, s));
+        CU(h, launch_cg_pap_fused<double>(L, l1.nb, l1.npt, l1.oprS, l1.v, pp_old, pp_new, h->Ap, h->part, h->sc, s));
+        CU(h, launch_cg_xr_fused<double>(L, h->sol, pp_new, l1.f, h->Ap, h->sc, nullptr, l1.v, h->part, h->dscal + 1, s));
         break;
-    case 2:  // mixed defect correction: e = V32(r); x += e; r = b - A x (FP64)
-        CU(h, launch_round_f32(L, l1.r, l1.f32, s));
-        CU(h, cudaMemsetAsync(l1.v32, 0, sizeof(float) * L.plane, s));
+    case 2: {  // mixed defect correction: e = V32(r); x += e; r = b - A x (FP64); f32/v32 prepared
+        double *x_old = par ? h->x2 : l1.v, *x_new = par ? l1.v : h->x2;
         if ((st = vcycle<float>(h, 1))) return st;
-        CU(h, launch_add_correction(L, l1.v, l1.v32, s));
-        CU(h, launch_residual<double>(L, l1.nb, l1.npt, l1.oprS, l1.v, l1.f, l1.r, s));
-        CU(h, launch_maxabs<double>(L, l1.r, h->part, h->dscal + 1, s));
+        CU(h, launch_defect_fused(L, l1.nb, l1.npt, l1.oprS, x_old, l1.v32, l1.f, x_new, l1.f32, l1.v32, h->part,
+                                  h->dscal + 1, s));
         break;
-    case 3:  // mixed PCG: FP64 Krylov vectors, FP32 V-cycle preconditioner
-        CU(h, launch_round_f32(L, l1.f, l1.f32, s));
-        CU(h, cudaMemsetAsync(l1.v32, 0, sizeof(float) * L.plane, s));
+    }
+    case 3:  // mixed PCG: FP64 Krylov vectors, FP32 V-cycle; f32/v32 prepared by the previous step
         if ((st = vcycle<float>(h, 1))) return st;
         CU(h, launch_cg_rho<float>(L, l1.v32, l1.f, h->part, h->sc, s));
-        CU(h, launch_cg_p<float>(L, l1.v32, h->pp, h->sc, s));
-        CU(h, launch_residual<double>(L, l1.nb, l1.npt, l1.oprS, h->pp, nullptr, h->Ap, s));
-        CU(h, launch_cg_pap(L, h->pp, h->Ap, h->part, h->sc, s));
-        CU(h, launch_cg_xr(L, h->sol, h->pp, l1.f, h->Ap, h->sc, s));
-        CU(h, launch_maxabs<double>(L, l1.f, h->part, h->dscal + 1, s));
+        CU(h, launch_cg_pap_fused<float>(L, l1.nb, l1.npt, l1.oprS, l1.v32, pp_old, pp_new, h->Ap, h->part, h->sc, s));
+        CU(h, launch_cg_xr_fused<float>(L, h->sol, pp_new, l1.f, h->Ap, h->sc, l1.f32, l1.v32, h->part, h->dscal + 1, s));
         break;
     }
     CU(h, cudaMemcpyAsync(h->h_scal + 1, h->dscal + 1, sizeof(double), cudaMemcpyDeviceToHost, s));
     return BBMG_OK;
 }
 
-int get_graph(bbmg_handle *h, int mode, cudaGraphExec_t *out) {
-    if (h->gexec[mode]) {
-        *out = h->gexec[mode];
+int get_graph(bbmg_handle *h, int mode, int par, cudaGraphExec_t *out) {
+    if (h->gexec[mode][par]) {
+        *out = h->gexec[mode][par];
         return BBMG_OK;
     }
     cudaGraph_t g = nullptr;
     CU(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    int st = record_iteration(h, mode);
+    int st = record_iteration(h, mode, par);
     cudaError_t e = cudaStreamEndCapture(h->stream, &g);
     if (st) {
         if (g) cudaGraphDestroy(g);
@@ -259,11 +246,11 @@ int get_graph(bbmg_handle *h, int mode, cudaGraphExec_t *out) {
         cudaGraphNodeType t;
         if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) nk++;
     }
-    h->gkernels[mode] = nk;
-    e = cudaGraphInstantiate(&h->gexec[mode], g, 0);
+    h->gkernels[mode][par] = nk;
+    e = cudaGraphInstantiate(&h->gexec[mode][par], g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return fail(h, BBMG_CUDA, "graph instantiation failed: %s", cudaGetErrorString(e));
-    *out = h->gexec[mode];
+    *out = h->gexec[mode][par];
     return BBMG_OK;
 }
 
@@ -306,8 +293,8 @@ int bbmg_destroy(bbmg_handle *h) {
         dfree(l.v); dfree(l.f); dfree(l.r);
         dfree(l.oprS32); dfree(l.c2f32); dfree(l.v32); dfree(l.f32); dfree(l.r32);
     }
-    dfree(h->OP); dfree(h->LU); dfree(h->piv); dfree(h->pinned); dfree(h->d_info);
-    dfree(h->sol); dfree(h->pp); dfree(h->Ap); dfree(h->sc); dfree(h->part); dfree(h->dscal);
+    dfree(h->OP); dfree(h->LU); dfree(h->piv); dfree(h->pinned); dfree(h->d_info); dfree(h->d_flag);
+    dfree(h->sol); dfree(h->pp); dfree(h->pp2); dfree(h->Ap); dfree(h->x2); dfree(h->sc); dfree(h->part); dfree(h->dscal);
     dfree(h->d_opr_in); dfree(h->d_stc); dfree(h->d_io);
     if (h->h_scal) cudaFreeHost(h->h_scal);
     if (h->ev0) cudaEventDestroy(h->ev0);
@@ -413,12 +400,14 @@ int bbmg_create(const bbmg_grid *grid, const bbmg_params *params, bbmg_handle **
     const Lay &L1 = h->lv[1].L;
     if ((st = dalloc(h, &h->OP, (size_t)h->np * h->np)) || (st = dalloc(h, &h->LU, (size_t)h->np * h->np)) ||
         (st = dalloc(h, &h->piv, (size_t)h->np)) || (st = dalloc(h, &h->pinned, (size_t)h->np)) ||
-        (st = dalloc(h, &h->d_info, 1)) || (st = dalloc(h, &h->part, (size_t)kRedBlocks)) ||
+        (st = dalloc(h, &h->d_info, 1)) || (st = dalloc(h, &h->d_flag, 1)) ||
+        (st = dalloc(h, &h->part, (size_t)kRedBlocks)) ||
         (st = dalloc(h, &h->dscal, 8)) || (st = dalloc(h, &h->sc, 1)))
         return bail(st);
+    if (mixed && prm.method == BBMG_METHOD_BBOX && (st = dalloc(h, &h->x2, (size_t)L1.plane))) return bail(st);
     if (prm.method == BBMG_METHOD_PCG_BBOX) {
         if ((st = dalloc(h, &h->sol, (size_t)L1.plane)) || (st = dalloc(h, &h->pp, (size_t)L1.plane)) ||
-            (st = dalloc(h, &h->Ap, (size_t)L1.plane)))
+            (st = dalloc(h, &h->pp2, (size_t)L1.plane)) || (st = dalloc(h, &h->Ap, (size_t)L1.plane)))
             return bail(st);
     }
     if (cudaMallocHost((void **)&h->h_scal, 8 * sizeof(double)) != cudaSuccess) return bail(fail(h, BBMG_NO_MEMORY, "pinned host"));
@@ -502,9 +491,19 @@ int bbmg_setup(bbmg_handle *h, int nst, const int *stc, const double *opr) {
     }
     // dense coarsest problem (bbmg_class.f90:961, 1307-1385)
     CU(h, setup_direct(h->lv[h->nlvl].L, h->lv[h->nlvl].opr27, h->OP, h->LU, h->piv, h->pinned, h->d_info, s));
-    // solve-phase operator planes
-    const int npt1 = seven ? 7 : 27;
-    if (npt1 != h->npt1 || !l1.oprS) drop_graphs(h);
+    // solve-phase operator planes: a 7-point level-1 operator that is exactly
+    // symmetric is stored as 4 planes (D, E, N, T), otherwise as 7; coarse
+    // levels keep the 27 planes
+    int sym = 0;
+    if (seven) {
+        const int one = 1;
+        CU(h, cudaMemcpyAsync(h->d_flag, &one, sizeof(int), cudaMemcpyHostToDevice, s));
+        CU(h, check_symmetric7(L1, l1.opr27, h->d_flag, s));
+        CU(h, cudaMemcpyAsync(&sym, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CU(h, cudaStreamSynchronize(s));
+    }
+    const int npt1 = seven ? (sym ? 4 : 7) : 27;
+    if (npt1 != h->npt1) drop_graphs(h);
     h->npt1 = npt1;
     const bool mixed = h->prm.precision == BBMG_PREC_MIXED;
     for (int n = 1; n <= h->nlvl; n++) {
@@ -512,17 +511,30 @@ int bbmg_setup(bbmg_handle *h, int nst, const int *stc, const double *opr) {
         size_t P = (size_t)l.L.plane;
         int npt = (n == 1) ? npt1 : 27;
         if (npt == 27) {
-            if (l.oprS && l.oprS != l.opr27) { dfree(l.oprS); h->bytes -= (long long)(7 * P * sizeof(double)); }
+            if (l.oprS && l.oprS != l.opr27) {
+                dfree(l.oprS);
+                h->bytes -= (long long)((size_t)l.nS * P * sizeof(double));
+                l.nS = 0;
+            }
             l.oprS = l.opr27;
         } else {
-            if (!l.oprS || l.oprS == l.opr27) {
+            if (l.oprS == l.opr27) l.oprS = nullptr;
+            if (l.oprS && l.nS != npt) {
+                dfree(l.oprS);
+                h->bytes -= (long long)((size_t)l.nS * P * sizeof(double));
                 l.oprS = nullptr;
-                int st = dalloc(h, &l.oprS, 7 * P);
-                if (st) return st;
             }
-            for (int q = 0; q < 7; q++)
-                CU(h, cudaMemcpyAsync(l.oprS + q * P, l.opr27 + (size_t)k7to27(q) * P, sizeof(double) * P,
+            if (!l.oprS) {
+                int st = dalloc(h, &l.oprS, (size_t)npt * P);
+                if (st) return st;
+                l.nS = npt;
+            }
+            static const int sym4[4] = {13, 14, 16, 22};
+            for (int q = 0; q < npt; q++) {
+                int slot = npt == 4 ? sym4[q] : k7to27(q);
+                CU(h, cudaMemcpyAsync(l.oprS + q * P, l.opr27 + (size_t)slot * P, sizeof(double) * P,
                                       cudaMemcpyDeviceToDevice, s));
+            }
         }
         if (l.npt != npt) { l.npt = npt; drop_graphs(h); }
         if (mixed) {
@@ -556,6 +568,7 @@ int bbmg_setup(bbmg_handle *h, int nst, const int *stc, const double *opr) {
     h->info.setup_ms = ms;
     h->info.coarse_pinned = h->npinned;
     h->info.device_bytes = h->bytes;
+    h->info.level1_stencil = npt1;
     h->setup_done = true;
     return BBMG_OK;
 }
@@ -623,15 +636,33 @@ int bbmg_solve(bbmg_handle *h, const double *rhs, double *sol, int *it_out, doub
             CU(h, cudaMemcpyAsync(l1.f, l1.r, sizeof(double) * L.plane, cudaMemcpyDeviceToDevice, s));
             CU(h, cudaMemcpyAsync(h->sol, l1.v, sizeof(double) * L.plane, cudaMemcpyDeviceToDevice, s));
             CU(h, cudaMemsetAsync(h->sc, 0, sizeof(CgScal), s));
+            CU(h, cudaMemsetAsync(h->pp, 0, sizeof(double) * L.plane, s));
+            CU(h, cudaMemsetAsync(h->pp2, 0, sizeof(double) * L.plane, s));
+            // the first preconditioner call starts from v = 0 (bbmg_class.f90:659)
+            if (mixed) {
+                CU(h, launch_round_f32(L, l1.f, l1.f32, s));
+                CU(h, cudaMemsetAsync(l1.v32, 0, sizeof(float) * L.plane, s));
+            } else {
+                CU(h, cudaMemsetAsync(l1.v, 0, sizeof(double) * L.plane, s));
+            }
+            launches += mixed ? 1 : 0;
             xout = h->sol;
+        } else if (mixed) {
+            CU(h, launch_round_f32(L, l1.r, l1.f32, s));
+            CU(h, cudaMemsetAsync(l1.v32, 0, sizeof(float) * L.plane, s));
+            launches += 1;
         }
-        cudaGraphExec_t ge = nullptr;
-        if ((st = get_graph(h, mode, &ge))) return st;
+        cudaGraphExec_t ge[2] = {nullptr, nullptr};
+        const bool pingpong = krylov || mixed;
+        if ((st = get_graph(h, mode, 0, &ge[0]))) return st;
+        if (pingpong && (st = get_graph(h, mode, 1, &ge[1]))) return st;
         double prev = HUGE_VAL;
         int stall = 0;
         for (int n = 1; n <= h->prm.maxit; n++) {
-            CU(h, cudaGraphLaunch(ge, s));
-            launches += h->gkernels[mode];
+            const int par = pingpong ? ((n - 1) & 1) : 0;
+            if (!krylov && mixed) xout = par ? l1.v : h->x2;  // the buffer this iteration writes
+            CU(h, cudaGraphLaunch(ge[par], s));
+            launches += h->gkernels[mode][par];
             double mr = 0.0;
             if ((st = sync_read(h, &mr, 1))) return st;
             rerr = mr / res0;  // bbmg_class.f90:696,723

@@ -44,6 +44,23 @@ template <> struct Sten<7> {
     BB_HD static int dz(int q) { return s7z(q); }
 };
 
+// Solve-phase stencil layouts.  NPT = 27: the full 3x3x3 operator, 27 planes.
+// NPT = 7: a 7-point operator, 7 planes in the column-major term order.
+// NPT = 4: a symmetric 7-point operator, planes D, E, N, T; the west, south
+// and bottom coefficients of a cell are the east, north and top ones of its
+// neighbour (used only when the operator is exactly symmetric, so the values
+// are bit-identical).  terms() is the number of stencil terms summed.
+template <int NPT> struct Lay7 {
+    static constexpr int terms = NPT == 27 ? 27 : 7;
+    static constexpr int centre = NPT == 27 ? kCentre27 : kCentre7;
+    // 27-slot of term q (for the neighbour offset table)
+    BB_HD static int slot(int q) { return NPT == 27 ? q : k7to27(q); }
+    // coefficient plane of term q
+    BB_HD static int plane(int q) { return NPT == 4 ? (q < 3 ? 3 - q : q - 3) : q; }
+    // true if term q's coefficient is stored at the neighbour cell
+    BB_HD static bool at_nbr(int q) { return NPT == 4 && q < 3; }
+};
+
 // Element offsets of the 27 neighbours of a cell, for a cell of even x
 // (off[0]) or odd x (off[1]).  In the x-split layout the offset of a
 // neighbour only depends on the parity of i.

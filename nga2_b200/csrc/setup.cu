@@ -420,6 +420,25 @@ __global__ void k_lu(double *__restrict__ A, int n, int *__restrict__ piv, int *
 }
 
 // ---------------------------------------------------------------------------
+// Exact symmetry of a 7-point level-1 operator: west(c) == east(c - x) etc.
+// for every interior cell whose neighbour is interior or a periodic image
+// (a coupling to a non-periodic overlap cell multiplies a zero value either
+// way).  Clears *flag on the first mismatch.
+__global__ void k_check_sym7(Lay L, const double *__restrict__ opr, int *flag) {
+    const long long total = (long long)L.nx * L.ny * L.nz;
+    for (long long t = gtid(); t < total; t += gstride()) {
+        int i, j, k;
+        interior_cell(L, t, i, j, k);
+        const long long id = L.idx(i, j, k);
+        bool ok = true;
+        if (i > 0 || L.xper) ok = ok && opr[q27(-1, 0, 0) * L.plane + id] == opr[q27(1, 0, 0) * L.plane + L.idx(i - 1, j, k)];
+        if (j > 0 || L.yper) ok = ok && opr[q27(0, -1, 0) * L.plane + id] == opr[q27(0, 1, 0) * L.plane + L.idx(i, j - 1, k)];
+        if (k > 0 || L.zper) ok = ok && opr[q27(0, 0, -1) * L.plane + id] == opr[q27(0, 0, 1) * L.plane + L.idx(i, j, k - 1)];
+        if (!ok) atomicAnd(flag, 0);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // host launchers
 #define BB_LAUNCH_CHECK() do { cudaError_t e_ = cudaGetLastError(); if (e_ != cudaSuccess) return e_; } while (0)
 
@@ -480,6 +499,13 @@ cudaError_t setup_operator(const Lay &F, const Lay &C, const double *oprF, const
     k_rap_rap<<<grid_for(nc, 128), 128, 0, s>>>(F, C, f2c, oprc2f, oprC);
     BB_LAUNCH_CHECK();
     return wrap_planes(C, oprC, 27, s);
+}
+
+cudaError_t check_symmetric7(const Lay &L, const double *opr, int *flag, cudaStream_t s) {
+    long long n = (long long)L.nx * L.ny * L.nz;
+    k_check_sym7<<<grid_for(n, 256), 256, 0, s>>>(L, opr, flag);
+    BB_LAUNCH_CHECK();
+    return cudaSuccess;
 }
 
 cudaError_t setup_direct(const Lay &L, const double *opr, double *OP, double *LU, int *piv, int *pinned, int *info,

@@ -14,6 +14,7 @@ cudaError_t setup_prolongation(const Lay &L, const double *opr, double *c2f, cud
 cudaError_t setup_restriction(const Lay &F, const Lay &C, const double *c2f, double *f2c, cudaStream_t s);
 cudaError_t setup_operator(const Lay &F, const Lay &C, const double *oprF, const double *c2f, const double *f2c,
                            double *oprc2f, double *oprC, cudaStream_t s);
+cudaError_t check_symmetric7(const Lay &L, const double *opr, int *flag, cudaStream_t s);
 cudaError_t setup_direct(const Lay &L, const double *opr, double *OP, double *LU, int *piv, int *pinned, int *info,
                          cudaStream_t s);
 
@@ -21,6 +22,11 @@ cudaError_t setup_direct(const Lay &L, const double *opr, double *OP, double *LU
 template <typename T>
 cudaError_t launch_relax(const Lay &L, const NbrOff &nb, int npt, bool fuse, const T *opr, T *v, const T *f, int dir,
                          cudaStream_t s);
+// `nsweeps` alternating sweeps starting with `first_dir` (the relax loops of
+// cycle, bbmg_class.f90:754-758 and 772-775)
+template <typename T>
+cudaError_t launch_relax_sweeps(const Lay &L, const NbrOff &nb, int npt, bool fuse, const T *opr, T *v, const T *f,
+                                int first_dir, int nsweeps, cudaStream_t s);
 template <typename T>
 cudaError_t launch_residual(const Lay &L, const NbrOff &nb, int npt, const T *opr, const T *v, const T *f, T *r,
                             cudaStream_t s);
@@ -35,7 +41,7 @@ cudaError_t launch_coarse_solve(const Lay &L, const double *LU, const int *piv, 
                                 cudaStream_t s);
 
 // reductions (deterministic two-pass) into a device double
-constexpr int kRedBlocks = 592;  // 4 per SM on 148 SMs
+constexpr int kRedBlocks = 1184;  // 8 blocks of 256 threads per SM on 148 SMs
 template <typename T>
 cudaError_t launch_maxabs(const Lay &L, const T *x, double *part, double *out, cudaStream_t s);
 template <typename T>
@@ -53,6 +59,16 @@ cudaError_t launch_cg_p(const Lay &L, const TZ *zz, double *pp, const CgScal *sc
 cudaError_t launch_cg_pap(const Lay &L, const double *pp, const double *Ap, double *part, CgScal *sc, cudaStream_t s);
 cudaError_t launch_cg_xr(const Lay &L, double *sol, const double *pp, double *res, const double *Ap, const CgScal *sc,
                          cudaStream_t s);
+template <typename TZ>
+cudaError_t launch_cg_pap_fused(const Lay &L, const NbrOff &nb, int npt, const double *opr, const TZ *zz,
+                                const double *pp_old, double *pp_new, double *Ap, double *part, CgScal *sc,
+                                cudaStream_t s);
+template <typename TV>
+cudaError_t launch_cg_xr_fused(const Lay &L, double *sol, const double *pp, double *res, const double *Ap,
+                               const CgScal *sc, float *f32, TV *vzero, double *part, double *out, cudaStream_t s);
+cudaError_t launch_defect_fused(const Lay &L, const NbrOff &nb, int npt, const double *opr, const double *x_old,
+                                const float *e, const double *b, double *x_new, float *f32, float *v32, double *part,
+                                double *out, cudaStream_t s);
 cudaError_t launch_round_f32(const Lay &L, const double *r, float *f, cudaStream_t s);
 cudaError_t launch_add_correction(const Lay &L, double *x, const float *e, cudaStream_t s);
 

@@ -21,6 +21,32 @@ static Off27 off_for(const NbrOff &nb, int par) {
     return r;
 }
 
+
+// Programmatic dependent launch: every solve-phase kernel lets the next kernel
+// in the stream start launching as soon as all of its own blocks are running,
+// then waits for its predecessor to finish (and its writes to be visible)
+// before touching memory.  Semantics stay those of plain stream order; only
+// the launch latency overlaps the previous kernel's tail.
+__device__ __forceinline__ void pdl_entry() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_k(void (*kern)(KArgs...), int grid, int block, size_t shm, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = shm;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 template <typename T, bool EXACT> struct Ops;
 template <> struct Ops<double, true> {
     __device__ static __forceinline__ double mac(double s, double a, double b) { return __dadd_rn(s, __dmul_rn(a, b)); }
@@ -46,6 +72,7 @@ template <typename T> struct ExactOf { static constexpr bool value = sizeof(T) =
 template <typename T, int NPT>
 __global__ void __launch_bounds__(256) k_relax(Lay L, Off27 off, const T *__restrict__ opr, T *v,
                                                 const T *__restrict__ f, int px, int py, int pz, int fuse) {
+    pdl_entry();
     using O = Ops<T, ExactOf<T>::value>;
     const int na = (L.nx - px + 1) >> 1, nb = (L.ny - py + 1) >> 1, nc = (L.nz - pz + 1) >> 1;
     const long long total = (long long)na * nb * nc;
@@ -57,12 +84,12 @@ __global__ void __launch_bounds__(256) k_relax(Lay L, Off27 off, const T *__rest
         long long id = L.idx(i, j, k);
         T s = T(0);
 #pragma unroll
-        for (int q = 0; q < NPT; q++) {
-            if (q == Sten<NPT>::centre) continue;
-            const int q27i = NPT == 27 ? q : k7to27(q);
-            s = O::mac(s, opr[q * L.plane + id], v[id + off.o[q27i]]);
+        for (int q = 0; q < Lay7<NPT>::terms; q++) {
+            if (q == Lay7<NPT>::centre) continue;
+            const int o = off.o[Lay7<NPT>::slot(q)];
+            s = O::mac(s, opr[Lay7<NPT>::plane(q) * L.plane + id + (Lay7<NPT>::at_nbr(q) ? o : 0)], v[id + o]);
         }
-        T d = opr[Sten<NPT>::centre * L.plane + id];
+        T d = opr[Lay7<NPT>::plane(Lay7<NPT>::centre) * L.plane + id];
         T val = O::div(O::sub(f[id], s), O::add(d, T(kEps)));
         v[id] = val;
         if (fuse && on_periodic_face(L, i, j, k)) write_images(L, v, i, j, k, val);
@@ -76,6 +103,7 @@ template <typename T, int NPT>
 __global__ void __launch_bounds__(256) k_residual(Lay L, NbrOff nb, const T *__restrict__ opr,
                                                    const T *__restrict__ v, const T *__restrict__ f,
                                                    T *__restrict__ r) {
+    pdl_entry();
     using O = Ops<T, ExactOf<T>::value>;
     const long long total = (long long)L.nx * L.ny * L.nz;
     for (long long t = gtid(); t < total; t += gstride()) {
@@ -85,10 +113,10 @@ __global__ void __launch_bounds__(256) k_residual(Lay L, NbrOff nb, const T *__r
         long long id = L.idx(i, j, k);
         T s = T(0);
 #pragma unroll
-        for (int q = 0; q < NPT; q++) {
-            const int q27i = NPT == 27 ? q : k7to27(q);
-            int o = par ? nb.off[1][q27i] : nb.off[0][q27i];
-            s = O::mac(s, opr[q * L.plane + id], v[id + o]);
+        for (int q = 0; q < Lay7<NPT>::terms; q++) {
+            const int q27i = Lay7<NPT>::slot(q);
+            const int o = par ? nb.off[1][q27i] : nb.off[0][q27i];
+            s = O::mac(s, opr[Lay7<NPT>::plane(q) * L.plane + id + (Lay7<NPT>::at_nbr(q) ? o : 0)], v[id + o]);
         }
         T val = f ? O::sub(f[id], s) : s;
         r[id] = val;
@@ -104,6 +132,7 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_restrict(Lay F, Lay C, const T *__restrict__ c2f,
                                                    const T *__restrict__ rF, T *__restrict__ fC,
                                                    T *__restrict__ vC) {
+    pdl_entry();
     using O = Ops<T, ExactOf<T>::value>;
     const long long total = (long long)C.nx * C.ny * C.nz;
     for (long long t = gtid(); t < total; t += gstride()) {
@@ -136,6 +165,7 @@ __global__ void __launch_bounds__(256) k_restrict(Lay F, Lay C, const T *__restr
 template <typename T>
 __global__ void __launch_bounds__(256) k_prolong(Lay F, Lay C, const T *__restrict__ c2f,
                                                   const T *__restrict__ vC, T *__restrict__ vF) {
+    pdl_entry();
     using O = Ops<T, ExactOf<T>::value>;
     const long long total = (long long)F.nx * F.ny * F.nz;
     for (long long t = gtid(); t < total; t += gstride()) {
@@ -163,6 +193,7 @@ template <typename T>
 __global__ void k_coarse_solve(Lay L, const double *__restrict__ LU, const int *__restrict__ piv,
                                const int *__restrict__ pinned, const T *__restrict__ f, T *__restrict__ v,
                                int mat_in_smem) {
+    pdl_entry();
     extern __shared__ double sm[];
     const int np = L.nx * L.ny * L.nz;
     double *x = sm;
@@ -237,6 +268,7 @@ __device__ __forceinline__ double block_reduce(double v, double *sh) {
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_maxabs_part(Lay L, const T *__restrict__ x, double *__restrict__ part) {
+    pdl_entry();
     __shared__ double sh[256];
     const long long total = (long long)L.nx * L.ny * L.nz;
     double m = 0.0;
@@ -253,6 +285,7 @@ __global__ void __launch_bounds__(256) k_maxabs_part(Lay L, const T *__restrict_
 template <typename TA, typename TB>
 __global__ void __launch_bounds__(256) k_dot_part(Lay L, const TA *__restrict__ a, const TB *__restrict__ b,
                                                    double *__restrict__ part) {
+    pdl_entry();
     __shared__ double sh[256];
     const long long total = (long long)L.nx * L.ny * L.nz;
     double s = 0.0;
@@ -268,6 +301,7 @@ __global__ void __launch_bounds__(256) k_dot_part(Lay L, const TA *__restrict__ 
 
 template <int MODE>
 __global__ void __launch_bounds__(256) k_final(const double *__restrict__ part, int n, double *__restrict__ out) {
+    pdl_entry();
     __shared__ double sh[256];
     double v = MODE == 0 ? 0.0 : 0.0;
     for (int t = threadIdx.x; t < n; t += blockDim.x) {
@@ -283,6 +317,7 @@ __global__ void __launch_bounds__(256) k_final(const double *__restrict__ part, 
 // caller arrays (Fortran, g overlap layers) <-> level interior
 template <typename T>
 __global__ void __launch_bounds__(256) k_from_caller(Lay L, const double *__restrict__ src, int g, T *__restrict__ dst) {
+    pdl_entry();
     const long long total = (long long)L.nx * L.ny * L.nz;
     const long long sy = L.nx + 2 * g, sz = sy * (L.ny + 2 * g);
     for (long long t = gtid(); t < total; t += gstride()) {
@@ -295,6 +330,7 @@ __global__ void __launch_bounds__(256) k_from_caller(Lay L, const double *__rest
 }
 
 __global__ void __launch_bounds__(256) k_to_caller(Lay L, const double *__restrict__ src, int g, double *__restrict__ dst) {
+    pdl_entry();
     const long long total = (long long)L.nx * L.ny * L.nz;
     const long long sy = L.nx + 2 * g, sz = sy * (L.ny + 2 * g);
     for (long long t = gtid(); t < total; t += gstride()) {
@@ -305,6 +341,7 @@ __global__ void __launch_bounds__(256) k_to_caller(Lay L, const double *__restri
 }
 
 __global__ void __launch_bounds__(256) k_to_f32(const double *__restrict__ src, float *__restrict__ dst, long long n) {
+    pdl_entry();
     for (long long t = gtid(); t < n; t += gstride()) dst[t] = (float)src[t];
 }
 
@@ -323,8 +360,9 @@ cudaError_t launch_relax(const Lay &L, const NbrOff &nb, int npt, bool fuse, con
         if (n == 0) continue;
         Off27 off = off_for(nb, px);
         int g = grid_for(n, 256);
-        if (npt == 7) k_relax<T, 7><<<g, 256, 0, s>>>(L, off, opr, v, f, px, py, pz, fuse ? 1 : 0);
-        else k_relax<T, 27><<<g, 256, 0, s>>>(L, off, opr, v, f, px, py, pz, fuse ? 1 : 0);
+        if (npt == 4) launch_k(k_relax<T, 4>, g, 256, 0, s, L, off, opr, v, f, px, py, pz, fuse ? 1 : 0);
+        else if (npt == 7) launch_k(k_relax<T, 7>, g, 256, 0, s, L, off, opr, v, f, px, py, pz, fuse ? 1 : 0);
+        else launch_k(k_relax<T, 27>, g, 256, 0, s, L, off, opr, v, f, px, py, pz, fuse ? 1 : 0);
         BB_CHECK_LAUNCH();
         if (per && !fuse) {
             cudaError_t e = wrap_planes(L, v, 1, s);
@@ -339,8 +377,9 @@ cudaError_t launch_residual(const Lay &L, const NbrOff &nb, int npt, const T *op
                             cudaStream_t s) {
     long long n = (long long)L.nx * L.ny * L.nz;
     int g = grid_for(n, 256);
-    if (npt == 7) k_residual<T, 7><<<g, 256, 0, s>>>(L, nb, opr, v, f, r);
-    else k_residual<T, 27><<<g, 256, 0, s>>>(L, nb, opr, v, f, r);
+    if (npt == 4) launch_k(k_residual<T, 4>, g, 256, 0, s, L, nb, opr, v, f, r);
+    else if (npt == 7) launch_k(k_residual<T, 7>, g, 256, 0, s, L, nb, opr, v, f, r);
+    else launch_k(k_residual<T, 27>, g, 256, 0, s, L, nb, opr, v, f, r);
     BB_CHECK_LAUNCH();
     return cudaSuccess;
 }
@@ -348,7 +387,7 @@ cudaError_t launch_residual(const Lay &L, const NbrOff &nb, int npt, const T *op
 template <typename T>
 cudaError_t launch_restrict(const Lay &F, const Lay &C, const T *c2f, const T *rF, T *fC, T *vC, cudaStream_t s) {
     long long n = (long long)C.nx * C.ny * C.nz;
-    k_restrict<T><<<grid_for(n, 256), 256, 0, s>>>(F, C, c2f, rF, fC, vC);
+    launch_k(k_restrict<T>, grid_for(n, 256), 256, 0, s, F, C, c2f, rF, fC, vC);
     BB_CHECK_LAUNCH();
     return cudaSuccess;
 }
@@ -356,7 +395,7 @@ cudaError_t launch_restrict(const Lay &F, const Lay &C, const T *c2f, const T *r
 template <typename T>
 cudaError_t launch_prolong(const Lay &F, const Lay &C, const T *c2f, const T *vC, T *vF, cudaStream_t s) {
     long long n = (long long)F.nx * F.ny * F.nz;
-    k_prolong<T><<<grid_for(n, 256), 256, 0, s>>>(F, C, c2f, vC, vF);
+    launch_k(k_prolong<T>, grid_for(n, 256), 256, 0, s, F, C, c2f, vC, vF);
     BB_CHECK_LAUNCH();
     return cudaSuccess;
 }
@@ -368,7 +407,7 @@ cudaError_t launch_coarse_solve(const Lay &L, const double *LU, const int *piv, 
     size_t mat = (size_t)np * np * sizeof(double), vec = (size_t)np * sizeof(double);
     int in_smem = (mat + vec) <= kCoarseSmem;
     size_t shm = vec + (in_smem ? mat : 0);
-    k_coarse_solve<T><<<1, 256, shm, s>>>(L, LU, piv, pinned, f, v, in_smem);
+    launch_k(k_coarse_solve<T>, 1, 256, shm, s, L, LU, piv, pinned, f, v, in_smem);
     BB_CHECK_LAUNCH();
     return cudaSuccess;
 }
@@ -381,18 +420,18 @@ cudaError_t coarse_solve_prepare() {
 
 template <typename T>
 cudaError_t launch_maxabs(const Lay &L, const T *x, double *part, double *out, cudaStream_t s) {
-    k_maxabs_part<T><<<kRedBlocks, 256, 0, s>>>(L, x, part);
+    launch_k(k_maxabs_part<T>, kRedBlocks, 256, 0, s, L, x, part);
     BB_CHECK_LAUNCH();
-    k_final<0><<<1, 256, 0, s>>>(part, kRedBlocks, out);
+    launch_k(k_final<0>, 1, 256, 0, s, part, kRedBlocks, out);
     BB_CHECK_LAUNCH();
     return cudaSuccess;
 }
 
 template <typename T>
 cudaError_t launch_dot(const Lay &L, const T *a, const T *b, double *part, double *out, cudaStream_t s) {
-    k_dot_part<T, T><<<kRedBlocks, 256, 0, s>>>(L, a, b, part);
+    launch_k(k_dot_part<T, T>, kRedBlocks, 256, 0, s, L, a, b, part);
     BB_CHECK_LAUNCH();
-    k_final<1><<<1, 256, 0, s>>>(part, kRedBlocks, out);
+    launch_k(k_final<1>, 1, 256, 0, s, part, kRedBlocks, out);
     BB_CHECK_LAUNCH();
     return cudaSuccess;
 }
@@ -400,20 +439,20 @@ cudaError_t launch_dot(const Lay &L, const T *a, const T *b, double *part, doubl
 template <typename T>
 cudaError_t launch_from_caller(const Lay &L, const double *src, int g, T *dst, cudaStream_t s) {
     long long n = (long long)L.nx * L.ny * L.nz;
-    k_from_caller<T><<<grid_for(n, 256), 256, 0, s>>>(L, src, g, dst);
+    launch_k(k_from_caller<T>, grid_for(n, 256), 256, 0, s, L, src, g, dst);
     BB_CHECK_LAUNCH();
     return cudaSuccess;
 }
 
 cudaError_t launch_to_caller(const Lay &L, const double *src, int g, double *dst, cudaStream_t s) {
     long long n = (long long)L.nx * L.ny * L.nz;
-    k_to_caller<<<grid_for(n, 256), 256, 0, s>>>(L, src, g, dst);
+    launch_k(k_to_caller, grid_for(n, 256), 256, 0, s, L, src, g, dst);
     BB_CHECK_LAUNCH();
     return cudaSuccess;
 }
 
 cudaError_t launch_to_f32(const double *src, float *dst, long long n, cudaStream_t s) {
-    k_to_f32<<<grid_for(n, 256), 256, 0, s>>>(src, dst, n);
+    launch_k(k_to_f32, grid_for(n, 256), 256, 0, s, src, dst, n);
     BB_CHECK_LAUNCH();
     return cudaSuccess;
 }
@@ -423,6 +462,7 @@ cudaError_t launch_to_f32(const double *src, float *dst, long long n, cudaStream
 // PCG (bbmg_class.f90:643-703).  Scalars live on the device so an iteration
 // needs no host round trip; only the convergence norm is copied back.
 __global__ void k_cg_rho(const double *__restrict__ part, int n, CgScal *sc) {
+    pdl_entry();
     __shared__ double sh[256];
     double v = 0.0;
     for (int t = threadIdx.x; t < n; t += blockDim.x) v = v + part[t];
@@ -435,6 +475,7 @@ __global__ void k_cg_rho(const double *__restrict__ part, int n, CgScal *sc) {
     }
 }
 __global__ void k_cg_pap(const double *__restrict__ part, int n, CgScal *sc) {
+    pdl_entry();
     __shared__ double sh[256];
     double v = 0.0;
     for (int t = threadIdx.x; t < n; t += blockDim.x) v = v + part[t];
@@ -448,6 +489,7 @@ __global__ void k_cg_pap(const double *__restrict__ part, int n, CgScal *sc) {
 template <typename TZ>
 __global__ void __launch_bounds__(256) k_cg_p(Lay L, const TZ *__restrict__ zz, double *__restrict__ pp,
                                                const CgScal *__restrict__ sc) {
+    pdl_entry();
     const double beta = sc->beta;
     const long long total = (long long)L.nx * L.ny * L.nz;
     for (long long t = gtid(); t < total; t += gstride()) {
@@ -463,6 +505,7 @@ __global__ void __launch_bounds__(256) k_cg_p(Lay L, const TZ *__restrict__ zz, 
 __global__ void __launch_bounds__(256) k_cg_xr(Lay L, double *__restrict__ sol, const double *__restrict__ pp,
                                                 double *__restrict__ res, const double *__restrict__ Ap,
                                                 const CgScal *__restrict__ sc) {
+    pdl_entry();
     const double alpha = sc->alpha;
     const long long total = (long long)L.nx * L.ny * L.nz;
     for (long long t = gtid(); t < total; t += gstride()) {
@@ -476,6 +519,7 @@ __global__ void __launch_bounds__(256) k_cg_xr(Lay L, double *__restrict__ sol, 
 
 // mixed precision: FP64 residual -> FP32 right-hand side of the V-cycle
 __global__ void __launch_bounds__(256) k_round_f32(Lay L, const double *__restrict__ r, float *__restrict__ f) {
+    pdl_entry();
     const long long total = (long long)L.nx * L.ny * L.nz;
     for (long long t = gtid(); t < total; t += gstride()) {
         int i, j, k;
@@ -486,6 +530,7 @@ __global__ void __launch_bounds__(256) k_round_f32(Lay L, const double *__restri
 }
 // mixed precision: x += e (FP32 correction accumulated in FP64), images kept
 __global__ void __launch_bounds__(256) k_add_correction(Lay L, double *__restrict__ x, const float *__restrict__ e) {
+    pdl_entry();
     const long long total = (long long)L.nx * L.ny * L.nz;
     for (long long t = gtid(); t < total; t += gstride()) {
         int i, j, k;
@@ -499,42 +544,42 @@ __global__ void __launch_bounds__(256) k_add_correction(Lay L, double *__restric
 
 template <typename TZ>
 cudaError_t launch_cg_rho(const Lay &L, const TZ *zz, const double *res, double *part, CgScal *sc, cudaStream_t s) {
-    k_dot_part<TZ, double><<<kRedBlocks, 256, 0, s>>>(L, zz, res, part);
+    launch_k(k_dot_part<TZ, double>, kRedBlocks, 256, 0, s, L, zz, res, part);
     BB_CHECK_LAUNCH();
-    k_cg_rho<<<1, 256, 0, s>>>(part, kRedBlocks, sc);
+    launch_k(k_cg_rho, 1, 256, 0, s, part, kRedBlocks, sc);
     BB_CHECK_LAUNCH();
     return cudaSuccess;
 }
 template <typename TZ>
 cudaError_t launch_cg_p(const Lay &L, const TZ *zz, double *pp, const CgScal *sc, cudaStream_t s) {
     long long n = (long long)L.nx * L.ny * L.nz;
-    k_cg_p<TZ><<<grid_for(n, 256), 256, 0, s>>>(L, zz, pp, sc);
+    launch_k(k_cg_p<TZ>, grid_for(n, 256), 256, 0, s, L, zz, pp, sc);
     BB_CHECK_LAUNCH();
     return cudaSuccess;
 }
 cudaError_t launch_cg_pap(const Lay &L, const double *pp, const double *Ap, double *part, CgScal *sc, cudaStream_t s) {
-    k_dot_part<double, double><<<kRedBlocks, 256, 0, s>>>(L, pp, Ap, part);
+    launch_k(k_dot_part<double, double>, kRedBlocks, 256, 0, s, L, pp, Ap, part);
     BB_CHECK_LAUNCH();
-    k_cg_pap<<<1, 256, 0, s>>>(part, kRedBlocks, sc);
+    launch_k(k_cg_pap, 1, 256, 0, s, part, kRedBlocks, sc);
     BB_CHECK_LAUNCH();
     return cudaSuccess;
 }
 cudaError_t launch_cg_xr(const Lay &L, double *sol, const double *pp, double *res, const double *Ap, const CgScal *sc,
                          cudaStream_t s) {
     long long n = (long long)L.nx * L.ny * L.nz;
-    k_cg_xr<<<grid_for(n, 256), 256, 0, s>>>(L, sol, pp, res, Ap, sc);
+    launch_k(k_cg_xr, grid_for(n, 256), 256, 0, s, L, sol, pp, res, Ap, sc);
     BB_CHECK_LAUNCH();
     return cudaSuccess;
 }
 cudaError_t launch_round_f32(const Lay &L, const double *r, float *f, cudaStream_t s) {
     long long n = (long long)L.nx * L.ny * L.nz;
-    k_round_f32<<<grid_for(n, 256), 256, 0, s>>>(L, r, f);
+    launch_k(k_round_f32, grid_for(n, 256), 256, 0, s, L, r, f);
     BB_CHECK_LAUNCH();
     return cudaSuccess;
 }
 cudaError_t launch_add_correction(const Lay &L, double *x, const float *e, cudaStream_t s) {
     long long n = (long long)L.nx * L.ny * L.nz;
-    k_add_correction<<<grid_for(n, 256), 256, 0, s>>>(L, x, e);
+    launch_k(k_add_correction, grid_for(n, 256), 256, 0, s, L, x, e);
     BB_CHECK_LAUNCH();
     return cudaSuccess;
 }
@@ -543,6 +588,261 @@ template cudaError_t launch_cg_rho<float>(const Lay &, const float *, const doub
 template cudaError_t launch_cg_p<double>(const Lay &, const double *, double *, const CgScal *, cudaStream_t);
 template cudaError_t launch_cg_p<float>(const Lay &, const float *, double *, const CgScal *, cudaStream_t);
 
+
+// ---------------------------------------------------------------------------
+// Fused CG steps.  pp_new = zz + beta*pp_old on the own cell (with images) and
+// Ap = A pp_new, the neighbours' pp_new formed on the fly from zz and pp_old
+// (bit-identical to the stored value), plus the block partial of pp_new.Ap
+// (bbmg_class.f90:674-687 in one pass).  pp_old and pp_new are distinct
+// buffers.
+template <typename TZ, int NPT>
+__global__ void __launch_bounds__(256) k_cg_pap_fused(Lay L, NbrOff nb, const double *__restrict__ opr,
+                                                       const TZ *__restrict__ zz, const double *__restrict__ pp_old,
+                                                       double *__restrict__ pp_new, double *__restrict__ Ap,
+                                                       const CgScal *__restrict__ sc, double *__restrict__ part) {
+    pdl_entry();
+    __shared__ double sh[256];
+    const double beta = sc->beta;
+    const long long total = (long long)L.nx * L.ny * L.nz;
+    double acc = 0.0;
+    for (long long t = gtid(); t < total; t += gstride()) {
+        int i, j, k;
+        interior_cell(L, t, i, j, k);
+        const int par = i & 1;
+        const long long id = L.idx(i, j, k);
+        double s = 0.0, pc = 0.0;
+#pragma unroll
+        for (int q = 0; q < Lay7<NPT>::terms; q++) {
+            const int q27i = Lay7<NPT>::slot(q);
+            const int o = par ? nb.off[1][q27i] : nb.off[0][q27i];
+            const double pq = __dadd_rn((double)zz[id + o], __dmul_rn(beta, pp_old[id + o]));
+            if (q == Lay7<NPT>::centre) pc = pq;
+            s = __dadd_rn(s, __dmul_rn(opr[Lay7<NPT>::plane(q) * L.plane + id + (Lay7<NPT>::at_nbr(q) ? o : 0)], pq));
+        }
+        pp_new[id] = pc;
+        if (on_periodic_face(L, i, j, k)) write_images(L, pp_new, i, j, k, pc);
+        Ap[id] = s;
+        acc = __dadd_rn(acc, __dmul_rn(pc, s));
+    }
+    acc = block_reduce<1>(acc, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
+// sol += alpha*pp; res -= alpha*Ap; block partial of max|res|
+// (bbmg_class.f90:688-695).  Also prepares the next preconditioner call: the
+// FP32 right-hand side (mixed precision) and a zero correction vector
+// (bbmg_class.f90:657-659), images included.
+template <typename TV>
+__global__ void __launch_bounds__(256) k_cg_xr_fused(Lay L, double *__restrict__ sol, const double *__restrict__ pp,
+                                                      double *__restrict__ res, const double *__restrict__ Ap,
+                                                      const CgScal *__restrict__ sc, float *__restrict__ f32,
+                                                      TV *__restrict__ vzero, double *__restrict__ part) {
+    pdl_entry();
+    __shared__ double sh[256];
+    const double alpha = sc->alpha;
+    const long long total = (long long)L.nx * L.ny * L.nz;
+    double m = 0.0;
+    for (long long t = gtid(); t < total; t += gstride()) {
+        int i, j, k;
+        interior_cell(L, t, i, j, k);
+        const long long id = L.idx(i, j, k);
+        sol[id] = __dadd_rn(sol[id], __dmul_rn(alpha, pp[id]));
+        const double r = __dsub_rn(res[id], __dmul_rn(alpha, Ap[id]));
+        res[id] = r;
+        const double a = fabs(r);
+        m = (a != a || m != m) ? (a + m) : fmax(m, a);
+        if (f32) f32[id] = (float)r;
+        vzero[id] = TV(0);
+        if (on_periodic_face(L, i, j, k)) write_images(L, vzero, i, j, k, TV(0));
+    }
+    m = block_reduce<0>(m, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = m;
+}
+
+template <typename TZ>
+cudaError_t launch_cg_pap_fused(const Lay &L, const NbrOff &nb, int npt, const double *opr, const TZ *zz,
+                                const double *pp_old, double *pp_new, double *Ap, double *part, CgScal *sc,
+                                cudaStream_t s) {
+    if (npt == 4) launch_k(k_cg_pap_fused<TZ, 4>, kRedBlocks, 256, 0, s, L, nb, opr, zz, pp_old, pp_new, Ap, sc, part);
+    else if (npt == 7) launch_k(k_cg_pap_fused<TZ, 7>, kRedBlocks, 256, 0, s, L, nb, opr, zz, pp_old, pp_new, Ap, sc, part);
+    else launch_k(k_cg_pap_fused<TZ, 27>, kRedBlocks, 256, 0, s, L, nb, opr, zz, pp_old, pp_new, Ap, sc, part);
+    BB_CHECK_LAUNCH();
+    launch_k(k_cg_pap, 1, 256, 0, s, part, kRedBlocks, sc);
+    BB_CHECK_LAUNCH();
+    return cudaSuccess;
+}
+
+template <typename TV>
+cudaError_t launch_cg_xr_fused(const Lay &L, double *sol, const double *pp, double *res, const double *Ap,
+                               const CgScal *sc, float *f32, TV *vzero, double *part, double *out, cudaStream_t s) {
+    launch_k(k_cg_xr_fused<TV>, kRedBlocks, 256, 0, s, L, sol, pp, res, Ap, sc, f32, vzero, part);
+    BB_CHECK_LAUNCH();
+    launch_k(k_final<0>, 1, 256, 0, s, part, kRedBlocks, out);
+    BB_CHECK_LAUNCH();
+    return cudaSuccess;
+}
+template cudaError_t launch_cg_pap_fused<double>(const Lay &, const NbrOff &, int, const double *, const double *,
+                                                 const double *, double *, double *, double *, CgScal *, cudaStream_t);
+template cudaError_t launch_cg_pap_fused<float>(const Lay &, const NbrOff &, int, const double *, const float *,
+                                                const double *, double *, double *, double *, CgScal *, cudaStream_t);
+template cudaError_t launch_cg_xr_fused<double>(const Lay &, double *, const double *, double *, const double *,
+                                                const CgScal *, float *, double *, double *, double *, cudaStream_t);
+template cudaError_t launch_cg_xr_fused<float>(const Lay &, double *, const double *, double *, const double *,
+                                               const CgScal *, float *, float *, double *, double *, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// 7-point operators: the colours of one Gauss-Seidel sweep only couple to
+// colours of Hamming weight +-1 (weight = px+py+pz), so the 8-colour sweep in
+// the reference's order equals four phases by weight (0,1,2,3 forward,
+// 3,2,1,0 backward): the colours inside a phase never read each other.  A phase
+// repeated back to back (the last of a forward sweep and the first of the
+// following backward sweep) recomputes identical values and is skipped.  The
+// result is bit-identical to the colour-by-colour sweep; one launch per phase.
+struct PhaseCols {
+    int n;             // colours in the phase (1..3)
+    int col[3];        // colour index px + 2py + 4pz, ascending
+    long long beg[4];  // prefix sums of the colour point counts
+};
+
+template <typename T, int NPT>
+__global__ void __launch_bounds__(256) k_relax_phase7(Lay L, NbrOff nb, const T *__restrict__ opr, T *v,
+                                                       const T *__restrict__ f, PhaseCols pc, int fuse) {
+    pdl_entry();
+    using O = Ops<T, ExactOf<T>::value>;
+    const long long total = pc.beg[pc.n];
+    for (long long t = gtid(); t < total; t += gstride()) {
+        int c = 0;
+        if (pc.n > 1 && t >= pc.beg[1]) c = (pc.n > 2 && t >= pc.beg[2]) ? 2 : 1;
+        const int col = pc.col[c];
+        const int px = col & 1, py = (col >> 1) & 1, pz = (col >> 2) & 1;
+        const int na = (L.nx - px + 1) >> 1, nbb = (L.ny - py + 1) >> 1;
+        const long long u = t - pc.beg[c];
+        const int a = (int)(u % na);
+        const long long rr = u / na;
+        const int b = (int)(rr % nbb), cc = (int)(rr / nbb);
+        const int i = px + 2 * a, j = py + 2 * b, k = pz + 2 * cc;
+        const long long id = L.idx(i, j, k);
+        T s = T(0);
+#pragma unroll
+        for (int q = 0; q < 7; q++) {
+            if (q == kCentre7) continue;
+            const int q27i = k7to27(q);
+            const int o = px ? nb.off[1][q27i] : nb.off[0][q27i];
+            s = O::mac(s, opr[Lay7<NPT>::plane(q) * L.plane + id + (Lay7<NPT>::at_nbr(q) ? o : 0)], v[id + o]);
+        }
+        const T d = opr[Lay7<NPT>::plane(kCentre7) * L.plane + id];
+        const T val = O::div(O::sub(f[id], s), O::add(d, T(kEps)));
+        v[id] = val;
+        if (fuse && on_periodic_face(L, i, j, k)) write_images(L, v, i, j, k, val);
+    }
+}
+
+static PhaseCols phase_cols(const Lay &L, int w) {
+    PhaseCols p{};
+    p.n = 0;
+    p.beg[0] = 0;
+    for (int col = 0; col < 8; col++) {
+        if (__builtin_popcount(col) != w) continue;
+        int px = col & 1, py = (col >> 1) & 1, pz = (col >> 2) & 1;
+        long long cnt = (long long)((L.nx - px + 1) >> 1) * ((L.ny - py + 1) >> 1) * ((L.nz - pz + 1) >> 1);
+        if (cnt == 0) continue;
+        p.col[p.n] = col;
+        p.beg[p.n + 1] = p.beg[p.n] + cnt;
+        p.n++;
+    }
+    return p;
+}
+
+template <typename T>
+cudaError_t launch_relax_sweeps(const Lay &L, const NbrOff &nb, int npt, bool fuse, const T *opr, T *v, const T *f,
+                                int first_dir, int nsweeps, cudaStream_t s) {
+    if (npt == 27 || !fuse) {
+        int dir = first_dir;
+        for (int i = 0; i < nsweeps; i++) {
+            cudaError_t e = launch_relax<T>(L, nb, npt, fuse, opr, v, f, dir, s);
+            if (e != cudaSuccess) return e;
+            dir = -dir;
+        }
+        return cudaSuccess;
+    }
+    int dir = first_dir, last = -1;
+    for (int i = 0; i < nsweeps; i++) {
+        for (int p = 0; p < 4; p++) {
+            int w = dir > 0 ? p : 3 - p;
+            if (w == last) continue;  // identical recomputation
+            last = w;
+            PhaseCols pc = phase_cols(L, w);
+            if (pc.n == 0) continue;
+            if (npt == 4) launch_k(k_relax_phase7<T, 4>, grid_for(pc.beg[pc.n], 256), 256, 0, s, L, nb, opr, v, f, pc, 1);
+            else launch_k(k_relax_phase7<T, 7>, grid_for(pc.beg[pc.n], 256), 256, 0, s, L, nb, opr, v, f, pc, 1);
+            BB_CHECK_LAUNCH();
+        }
+        dir = -dir;
+    }
+    return cudaSuccess;
+}
+template cudaError_t launch_relax_sweeps<double>(const Lay &, const NbrOff &, int, bool, const double *, double *,
+                                                 const double *, int, int, cudaStream_t);
+template cudaError_t launch_relax_sweeps<float>(const Lay &, const NbrOff &, int, bool, const float *, float *,
+                                                const float *, int, int, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Mixed-precision defect correction step (the FP64 half of an mgsolve
+// iteration, bbmg_class.f90:716-722 with the correction of 770): x_new = x + e
+// on the own cell (images written), r = b - A (x + e) with the neighbours'
+// x + e formed on the fly; r becomes the FP32 right-hand side of the next
+// V-cycle, the FP32 correction is zeroed for it, and the block partial of
+// max|r| is written.  x_old and x_new are distinct buffers.
+template <int NPT>
+__global__ void __launch_bounds__(256) k_defect_fused(Lay L, NbrOff nb, const double *__restrict__ opr,
+                                                       const double *__restrict__ x_old, const float *__restrict__ e,
+                                                       const double *__restrict__ b, double *__restrict__ x_new,
+                                                       float *__restrict__ f32, float *__restrict__ v32,
+                                                       double *__restrict__ part) {
+    pdl_entry();
+    __shared__ double sh[256];
+    const long long total = (long long)L.nx * L.ny * L.nz;
+    double m = 0.0;
+    for (long long t = gtid(); t < total; t += gstride()) {
+        int i, j, k;
+        interior_cell(L, t, i, j, k);
+        const int par = i & 1;
+        const long long id = L.idx(i, j, k);
+        double s = 0.0, xc = 0.0;
+#pragma unroll
+        for (int q = 0; q < Lay7<NPT>::terms; q++) {
+            const int q27i = Lay7<NPT>::slot(q);
+            const int o = par ? nb.off[1][q27i] : nb.off[0][q27i];
+            const double xq = x_old[id + o] + (double)e[id + o];
+            if (q == Lay7<NPT>::centre) xc = xq;
+            s = fma(opr[Lay7<NPT>::plane(q) * L.plane + id + (Lay7<NPT>::at_nbr(q) ? o : 0)], xq, s);
+        }
+        const double r = b[id] - s;
+        x_new[id] = xc;
+        f32[id] = (float)r;
+        v32[id] = 0.0f;
+        if (on_periodic_face(L, i, j, k)) {
+            write_images(L, x_new, i, j, k, xc);
+            write_images(L, v32, i, j, k, 0.0f);
+        }
+        const double a = fabs(r);
+        m = (a != a || m != m) ? (a + m) : fmax(m, a);
+    }
+    m = block_reduce<0>(m, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = m;
+}
+
+cudaError_t launch_defect_fused(const Lay &L, const NbrOff &nb, int npt, const double *opr, const double *x_old,
+                                const float *e, const double *b, double *x_new, float *f32, float *v32, double *part,
+                                double *out, cudaStream_t s) {
+    if (npt == 4) launch_k(k_defect_fused<4>, kRedBlocks, 256, 0, s, L, nb, opr, x_old, e, b, x_new, f32, v32, part);
+    else if (npt == 7) launch_k(k_defect_fused<7>, kRedBlocks, 256, 0, s, L, nb, opr, x_old, e, b, x_new, f32, v32, part);
+    else launch_k(k_defect_fused<27>, kRedBlocks, 256, 0, s, L, nb, opr, x_old, e, b, x_new, f32, v32, part);
+    BB_CHECK_LAUNCH();
+    launch_k(k_final<0>, 1, 256, 0, s, part, kRedBlocks, out);
+    BB_CHECK_LAUNCH();
+    return cudaSuccess;
+}
 #define BB_INST(T)                                                                                                   \
     template cudaError_t launch_relax<T>(const Lay &, const NbrOff &, int, bool, const T *, T *, const T *, int,     \
                                          cudaStream_t);                                                              \

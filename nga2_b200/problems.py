@@ -298,17 +298,20 @@ def channel_poisson(nx=512, ny=512, nz=512, seed=0, stretch=2.0, Lx=2.0 * math.p
                     "L": [Lx, Ly, Lz]})
 
 
-def random_operator(nx, ny, nz, per, seed=0, full27=False, diag_boost=0.0):
+def random_operator(nx, ny, nz, per, seed=0, full27=False, diag_boost=0.0, asym=0.0):
     """Random diagonally dominant (or singular with zero row sums when
     ``diag_boost == 0``) operator for property tests: symmetric 7-point from
     random positive face conductances, optionally with random 27-point
-    off-diagonal couplings (non-symmetric)."""
+    off-diagonal couplings (non-symmetric), or with the 7-point off-diagonals
+    scaled by 1 + asym*U(0,1) (non-symmetric 7-point)."""
     rng = np.random.default_rng(seed)
     xn = uniform_nodes(nx); yn = uniform_nodes(ny); zn = uniform_nodes(nz)
     rho = np.exp(rng.uniform(-2.0, 2.0, size=(nz, ny, nx)))
     opr7, vol = assemble_operator(xn, yn, zn, per, rho=rho)
     if diag_boost:
         opr7[..., 0] += diag_boost * np.abs(opr7[..., 0])
+    if asym:
+        opr7[..., 1:] *= 1.0 + asym * rng.uniform(0.0, 1.0, size=opr7[..., 1:].shape)
     if not full27:
         return STC7.copy(), opr7
     stc = np.array([[i, j, k] for k in (-1, 0, 1) for j in (-1, 0, 1) for i in (-1, 0, 1)], dtype=np.int32)

@@ -131,6 +131,38 @@ def test_bbox_solve_bitexact(dims, per):
     assert np.array_equal(xg, xo)
 
 
+@pytest.mark.parametrize("kind", ["asym7", "channel"])
+def test_bbox_solve_bitexact_level1_layouts(kind):
+    """The 7-plane (non-symmetric) level-1 layout; the symmetric 4-plane layout is
+    what the uniform-grid cases above use."""
+    if kind == "asym7":
+        dims, per = (12, 10, 8), (True, False, True)
+        stc, opr = P.random_operator(*dims, per, seed=5, asym=1e-3)
+        rng = np.random.default_rng(5)
+        rhs = rng.standard_normal(dims[::-1]); rhs -= rhs.mean()
+    else:
+        pb = P.channel_poisson(16, 16, 12, seed=5)
+        dims, per, stc, opr, rhs = (16, 16, 12), (True, False, True), pb.stc, pb.opr, pb.rhs
+    o = OracleBBMG(*dims, *per, method=BBOX, maxit=40, rcvg=1e-10)
+    o.setup(stc, opr)
+    xo, ito, ro = o.solve(rhs)
+    g = BBMG(*dims, *per, method=BBOX, maxit=40, rcvg=1e-10)
+    g.setup(stc, opr)
+    assert g.info["level1_stencil"] == 7
+    xg, itg, rg, st = g.solve(rhs)
+    assert itg == ito and rg == ro and np.array_equal(xg, xo)
+
+
+def test_symmetric_layout_selected():
+    stc, opr = P.random_operator(8, 8, 8, (True, True, True), seed=1)
+    g = BBMG(8, 8, 8, True, True, True)
+    g.setup(stc, opr)
+    assert g.info["level1_stencil"] == 4
+    stc27, opr27 = P.random_operator(8, 8, 8, (True, True, True), seed=1, full27=True)
+    g.setup(stc27, opr27)
+    assert g.info["level1_stencil"] == 27
+
+
 @pytest.mark.parametrize("dims,per", CASES, ids=IDS)
 def test_pcg_solve(dims, per):
     """V-cycle preconditioned CG (cgsolve): the dot products are reduced in a
