@@ -161,6 +161,28 @@ int bbmg_profile_step(bbmg_handle *h, int step, int level, int arg, int prec, in
  * below the diagonal) and pivots; any pointer may be NULL. */
 int bbmg_debug_direct(bbmg_handle *h, double *op, double *lu, int *piv, int *np);
 
+/* ------------------------------------------------------------------------
+ * Residual check without device allocation.  No counterpart in the
+ * reference: it serves callers that cannot call cudaMalloc -- a flow solver
+ * whose device memory comes from its own pool allocator, or a time loop that
+ * must not allocate because allocation can synchronise the device.
+ *
+ * Computes, on `stream` (NULL: the default stream), out[0] = max|rhs - A sol|,
+ * out[1] = max|rhs| and out[2] = out[0] / out[1] over the interior of the
+ * caller's system, with A the caller's stencil (stc host array int[nst][3],
+ * opr in bbmg_setup's layout), overlap cells of non-periodic directions taken
+ * as zero and periodic directions wrapped -- the residual bbmg_solve reports.
+ * opr, rhs, sol and out (3 doubles) must be device memory.  Nothing is
+ * allocated: the only scratch is a static device array of 8192 plane slots
+ * that every GPU loading the library holds until exit, so grids with
+ * nz > 8192 are rejected with BBMG_BAD_ARGS.  The first call on a device
+ * looks up that array's device address (make it before any stream capture).
+ * Calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller.  Errors: bbmg_last_error(NULL).
+ * ---------------------------------------------------------------------- */
+int bbmg_residual_norm_noalloc(const bbmg_grid *grid, int nst, const int *stc, const double *opr,
+                               const double *rhs, const double *sol, double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -31,7 +31,8 @@ ARR = {"opr": 0, "c2f": 1, "f2c": 2, "oprc2f": 3, "v": 4, "f": 5, "r": 6}
 STEP = {"relax": 0, "residual": 1, "restrict": 2, "prolong": 3, "cycle": 4, "direct": 5}
 EXPORTS = ["bbmg_default_params", "bbmg_create", "bbmg_setup", "bbmg_solve", "bbmg_set_convergence",
            "bbmg_set_stream", "bbmg_get_info", "bbmg_destroy", "bbmg_last_error", "bbmg_debug_get",
-           "bbmg_debug_put", "bbmg_debug_step", "bbmg_debug_direct", "bbmg_profile_step"]
+           "bbmg_debug_put", "bbmg_debug_step", "bbmg_debug_direct", "bbmg_profile_step",
+           "bbmg_residual_norm_noalloc"]
 
 
 class BBMGError(RuntimeError):

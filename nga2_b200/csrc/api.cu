@@ -94,6 +94,11 @@ struct bbmg_handle {
 
 static thread_local std::string g_create_err;
 
+namespace bbmg {
+// message for bbmg_last_error(NULL) from entry points without a handle
+void set_create_error(const char *msg) { g_create_err = msg; }
+}  // namespace bbmg
+
 namespace {
 
 int fail(bbmg_handle *h, int code, const char *fmt, ...) {
