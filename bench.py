@@ -307,12 +307,14 @@ def main():
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
     reps = 20
-    ms_sweep = gm.profile("relax", 1, 1, prec=1, reps=reps)
+    ms_sweep = gm.profile("relax", 1, 1, prec=1, reps=reps)  # one forward sweep as the V-cycle runs it
+    lvl1 = gm.info["level1_stencil"]
     ncell = n ** 3
     c1, sv = 4, 4  # symmetric 7-point: 4 coefficients per cell; FP32 vectors
-    bytes_launch = ncell / 8 * (c1 * 4 + 3 * sv)
-    t_launch = ms_sweep / 8 / 1e3
-    achieved = bytes_launch / t_launch / 1e9
+    bytes_sweep = ncell * (c1 * 4 + 3 * sv)
+    nlaunch = 4 if lvl1 in (4, 7) else 8  # colour phases by Hamming weight on 7-point levels
+    t_launch = ms_sweep / nlaunch / 1e3
+    achieved = bytes_sweep / (ms_sweep / 1e3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "relax_fp32_traffic.json")
     if os.path.exists(tpath):
@@ -321,14 +323,16 @@ def main():
         except Exception:
             traffic = None
     roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-            "traffic": traffic, "kernel": "k_relax<float,7> (one GS colour, level 1)",
-            "bytes_per_launch": bytes_launch, "ms_per_launch": t_launch * 1e3, "peak_source": peak_src}
+            "traffic": traffic,
+            "kernel": f"k_relax_phase7<float,{lvl1}> (level-1 Gauss-Seidel, one sweep = {nlaunch} launches)",
+            "bytes_per_launch": bytes_sweep / nlaunch, "ms_per_launch": t_launch * 1e3, "ms_per_sweep": ms_sweep,
+            "peak_source": peak_src}
     # other kernels, for the record
     kern = {}
-    for name, lvl, prec, nl in (("relax", 1, 0, 8), ("residual", 1, 1, 1), ("residual", 1, 0, 1),
-                                ("restrict", 1, 1, 1), ("prolong", 1, 1, 1), ("relax", 2, 1, 8)):
+    for name, lvl, prec in (("relax", 1, 0), ("residual", 1, 1), ("residual", 1, 0), ("restrict", 1, 1),
+                            ("prolong", 1, 1), ("relax", 2, 1), ("relax", 3, 1), ("relax", 4, 1)):
         try:
-            kern[f"{name}_L{lvl}_{'fp32' if prec else 'fp64'}_ms_per_launch"] = gm.profile(name, lvl, 1, prec, 10) / nl
+            kern[f"{name}_L{lvl}_{'fp32' if prec else 'fp64'}_ms"] = gm.profile(name, lvl, 1, prec, 10)
         except Exception as e:  # noqa: BLE001
             kern[f"{name}_L{lvl}"] = str(e)
 

@@ -155,7 +155,8 @@ long long bbmg_debug_put(bbmg_handle *h, int level, int which, int prec, const d
 int bbmg_debug_step(bbmg_handle *h, int step, int level, int arg, int prec);
 /* Device time of one stage, for roofline measurements: the stage runs `reps`
  * times back to back on the handle's stream between two CUDA events; returns
- * the average milliseconds per repetition in *ms. */
+ * the average milliseconds per repetition in *ms.  BBMG_STEP_RELAX times one
+ * sweep as the V-cycle runs it (by colour phases on 7-point levels). */
 int bbmg_profile_step(bbmg_handle *h, int step, int level, int arg, int prec, int reps, double *ms);
 /* dense coarsest matrix (row-major np x np), its LU (row-major, unit lower
  * below the diagonal) and pivots; any pointer may be NULL. */

@@ -212,8 +212,9 @@ int record_iteration(bbmg_handle *h, int mode, int par) {
         break;
     case 2: {  // mixed defect correction: e = V32(r); x += e; r = b - A x (FP64); f32/v32 prepared
         double *x_old = par ? h->x2 : l1.v, *x_new = par ? l1.v : h->x2;
+        CU(h, cudaMemsetAsync(l1.v32, 0, sizeof(float) * L.plane, s));
         if ((st = vcycle<float>(h, 1))) return st;
-        CU(h, launch_defect_fused(L, l1.nb, l1.npt, l1.oprS, x_old, l1.v32, l1.f, x_new, l1.f32, l1.v32, h->part,
+        CU(h, launch_defect_fused(L, l1.nb, l1.npt, l1.oprS, x_old, l1.v32, l1.f, x_new, l1.f32, h->part,
                                   h->dscal + 1, s));
         break;
     }
@@ -861,13 +862,13 @@ int bbmg_profile_step(bbmg_handle *h, int step, int n, int arg, int prec, int re
         cudaError_t e = cudaSuccess;
         if (prec == 1) {
             using P = LvlPtr<float>;
-            if (step == BBMG_STEP_RELAX) e = launch_relax<float>(l.L, l.nb, l.npt, l.fuse, P::opr(l), P::v(l), P::f(l), arg >= 0 ? 1 : -1, s);
+            if (step == BBMG_STEP_RELAX) e = launch_relax_sweeps<float>(l.L, l.nb, l.npt, l.fuse, P::opr(l), P::v(l), P::f(l), arg >= 0 ? 1 : -1, 1, s);
             else if (step == BBMG_STEP_RESIDUAL) e = launch_residual<float>(l.L, l.nb, l.npt, P::opr(l), P::v(l), P::f(l), P::r(l), s);
             else if (step == BBMG_STEP_RESTRICT) e = launch_restrict<float>(l.L, h->lv[n + 1].L, P::c2f(l), P::r(l), P::f(h->lv[n + 1]), P::v(h->lv[n + 1]), s);
             else e = launch_prolong<float>(l.L, h->lv[n + 1].L, P::c2f(l), P::v(h->lv[n + 1]), P::v(l), s);
         } else {
             using P = LvlPtr<double>;
-            if (step == BBMG_STEP_RELAX) e = launch_relax<double>(l.L, l.nb, l.npt, l.fuse, P::opr(l), P::v(l), P::f(l), arg >= 0 ? 1 : -1, s);
+            if (step == BBMG_STEP_RELAX) e = launch_relax_sweeps<double>(l.L, l.nb, l.npt, l.fuse, P::opr(l), P::v(l), P::f(l), arg >= 0 ? 1 : -1, 1, s);
             else if (step == BBMG_STEP_RESIDUAL) e = launch_residual<double>(l.L, l.nb, l.npt, P::opr(l), P::v(l), P::f(l), P::r(l), s);
             else if (step == BBMG_STEP_RESTRICT) e = launch_restrict<double>(l.L, h->lv[n + 1].L, P::c2f(l), P::r(l), P::f(h->lv[n + 1]), P::v(h->lv[n + 1]), s);
             else e = launch_prolong<double>(l.L, h->lv[n + 1].L, P::c2f(l), P::v(h->lv[n + 1]), P::v(l), s);

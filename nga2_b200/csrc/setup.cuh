@@ -55,11 +55,6 @@ struct CgScal {
 template <typename TZ>
 cudaError_t launch_cg_rho(const Lay &L, const TZ *zz, const double *res, double *part, CgScal *sc, cudaStream_t s);
 template <typename TZ>
-cudaError_t launch_cg_p(const Lay &L, const TZ *zz, double *pp, const CgScal *sc, cudaStream_t s);
-cudaError_t launch_cg_pap(const Lay &L, const double *pp, const double *Ap, double *part, CgScal *sc, cudaStream_t s);
-cudaError_t launch_cg_xr(const Lay &L, double *sol, const double *pp, double *res, const double *Ap, const CgScal *sc,
-                         cudaStream_t s);
-template <typename TZ>
 cudaError_t launch_cg_pap_fused(const Lay &L, const NbrOff &nb, int npt, const double *opr, const TZ *zz,
                                 const double *pp_old, double *pp_new, double *Ap, double *part, CgScal *sc,
                                 cudaStream_t s);
@@ -67,10 +62,9 @@ template <typename TV>
 cudaError_t launch_cg_xr_fused(const Lay &L, double *sol, const double *pp, double *res, const double *Ap,
                                const CgScal *sc, float *f32, TV *vzero, double *part, double *out, cudaStream_t s);
 cudaError_t launch_defect_fused(const Lay &L, const NbrOff &nb, int npt, const double *opr, const double *x_old,
-                                const float *e, const double *b, double *x_new, float *f32, float *v32, double *part,
+                                const float *e, const double *b, double *x_new, float *f32, double *part,
                                 double *out, cudaStream_t s);
 cudaError_t launch_round_f32(const Lay &L, const double *r, float *f, cudaStream_t s);
-cudaError_t launch_add_correction(const Lay &L, double *x, const float *e, cudaStream_t s);
 
 // caller I/O: Fortran arrays with g overlap layers <-> level interior
 template <typename T>

@@ -1,12 +1,19 @@
 // solve.cu -- V-cycle kernels of the black-box multigrid (FP64 and FP32).
 //
 // Each kernel restates one solve-phase routine of src/solver/bbmg_class.f90.
-// The FP64 instantiation (EXACT) evaluates every sum in the reference's
-// column-major term order without FMA contraction, so it matches the oracle
-// bit for bit; the FP32 instantiation is the fast V-cycle of the mixed
-// precision solver and uses FMA.  Terms whose coefficient is structurally
-// zero (the 20 unused slots of a 7-point operator, prolongation weights of the
-// other parity classes) are skipped: adding +0.0 does not change a sum.
+// The FP64 instantiation evaluates every sum in the reference's column-major
+// term order without FMA contraction, so it matches the oracle bit for bit;
+// the FP32 instantiation is the fast V-cycle of the mixed precision solver and
+// uses FMA.  Terms whose coefficient is structurally zero (the 20 unused slots
+// of a 7-point operator, prolongation weights of the other parity classes) are
+// skipped: adding +0.0 does not change a sum.
+//
+// Work mapping: a 2-D launch whose y dimension walks (j,k) rows and whose x
+// dimension walks positions inside a row, so no thread divides a 64-bit
+// linear index.  The Gauss-Seidel kernels give each thread VW consecutive
+// points of one half-row (16-byte vector loads); neighbour offsets that are
+// not a multiple of VW (the odd x-neighbour) fall back to scalar loads that
+// hit the lines the aligned loads just brought in.
 #include "setup.cuh"
 
 namespace bbmg {
@@ -21,7 +28,6 @@ static Off27 off_for(const NbrOff &nb, int par) {
     return r;
 }
 
-
 // Programmatic dependent launch: every solve-phase kernel lets the next kernel
 // in the stream start launching as soon as all of its own blocks are running,
 // then waits for its predecessor to finish (and its writes to be visible)
@@ -33,10 +39,11 @@ __device__ __forceinline__ void pdl_entry() {
 }
 
 template <typename... KArgs, typename... Args>
-static cudaError_t launch_k(void (*kern)(KArgs...), int grid, int block, size_t shm, cudaStream_t s, Args... args) {
+static cudaError_t launch_k(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t shm, cudaStream_t s,
+                            Args... args) {
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)grid);
-    cfg.blockDim = dim3((unsigned)block);
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
     cfg.dynamicSmemBytes = shm;
     cfg.stream = s;
     cudaLaunchAttribute at[1];
@@ -46,6 +53,14 @@ static cudaError_t launch_k(void (*kern)(KArgs...), int grid, int block, size_t 
     cfg.numAttrs = 1;
     return cudaLaunchKernelEx(&cfg, kern, args...);
 }
+
+#define BB_CHECK_LAUNCH(call)                \
+    do {                                     \
+        cudaError_t e0_ = (call);            \
+        if (e0_ != cudaSuccess) return e0_;  \
+        cudaError_t e_ = cudaGetLastError(); \
+        if (e_ != cudaSuccess) return e_;    \
+    } while (0)
 
 template <typename T, bool EXACT> struct Ops;
 template <> struct Ops<double, true> {
@@ -63,64 +78,192 @@ template <typename T> struct Ops<T, false> {
 template <typename T> struct ExactOf { static constexpr bool value = sizeof(T) == 8; };
 
 // ---------------------------------------------------------------------------
-// One colour of the 8-colour Gauss-Seidel (bbmg_class.f90:872-885):
-// A = (B - sum_{l != 0} opr(l) A(nbr)) / (opr(0) + eps) on the points
-// i = px + 2a, j = py + 2b, k = pz + 2c.  With `fuse` the new value is also
-// written into its periodic images (the vsync after the colour); that is only
-// race-free when every periodic direction has an even size, otherwise the
+// launch geometry: x = chunks of a row, y = rows (grid-stride in both)
+struct Geo {
+    dim3 grid, block;
+};
+static Geo geo_rows(long long nchunks, long long nrows, long long cap_blocks = 148LL * 24) {
+    int bx = 1;
+    while (bx < nchunks && bx < 128) bx <<= 1;
+    int by = 256 / bx;
+    long long gx = (nchunks + bx - 1) / bx;
+    if (gx < 1) gx = 1;
+    long long gy = (nrows + by - 1) / by;
+    long long cy = cap_blocks / gx;
+    if (cy < 1) cy = 1;
+    if (gy > cy) gy = cy;
+    if (gy > 65535) gy = 65535;
+    if (gy < 1) gy = 1;
+    return {dim3((unsigned)gx, (unsigned)gy), dim3((unsigned)bx, (unsigned)by)};
+}
+// fixed geometry of the deterministic reductions on a level
+static Geo geo_red(const Lay &L) { return geo_rows(L.nx, (long long)L.ny * L.nz, kRedBlocks); }
+
+#define FOR_ROWS(nrows) for (int row = blockIdx.y * blockDim.y + threadIdx.y; row < (nrows); row += gridDim.y * blockDim.y)
+#define FOR_CHUNKS(nch) for (int ch = blockIdx.x * blockDim.x + threadIdx.x; ch < (nch); ch += gridDim.x * blockDim.x)
+
+// storage-order position t of a row -> x index (odd x first, then even x)
+__device__ __forceinline__ int x_of(const Lay &L, int t) {
+    const int nodd = L.nx >> 1;
+    return t < nodd ? 2 * t + 1 : 2 * (t - nodd);
+}
+
+// VW consecutive values, one vector load when aligned
+template <int VW, typename T> struct VecT;
+template <> struct VecT<1, float> { using type = float; };
+template <> struct VecT<2, float> { using type = float2; };
+template <> struct VecT<4, float> { using type = float4; };
+template <> struct VecT<1, double> { using type = double; };
+template <> struct VecT<2, double> { using type = double2; };
+
+template <int VW, typename T>
+__device__ __forceinline__ void ldv(const T *p, bool aligned, T (&o)[VW]) {
+    if (VW == 1 || !aligned) {
+#pragma unroll
+        for (int e = 0; e < VW; e++) o[e] = p[e];
+    } else {
+        using V = typename VecT<VW, T>::type;
+        const V w = *reinterpret_cast<const V *>(p);
+        const T *wp = reinterpret_cast<const T *>(&w);
+#pragma unroll
+        for (int e = 0; e < VW; e++) o[e] = wp[e];
+    }
+}
+template <int VW, typename T>
+__device__ __forceinline__ void stv(T *p, const T (&o)[VW]) {
+    if (VW == 1) {
+        p[0] = o[0];
+    } else {
+        using V = typename VecT<VW, T>::type;
+        V w;
+        T *wp = reinterpret_cast<T *>(&w);
+#pragma unroll
+        for (int e = 0; e < VW; e++) wp[e] = o[e];
+        *reinterpret_cast<V *>(p) = w;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Gauss-Seidel update of VW points of colour (px,py,pz) starting at id0
+// (bbmg_class.f90:876-880): A = (B - sum_{l != 0} opr(l) A(nbr)) / (opr(0)+eps).
+template <typename T, int NPT, int VW>
+__device__ __forceinline__ void gs_points(const Lay &L, const Off27 &off, const T *__restrict__ opr, T *v,
+                                          const T *__restrict__ f, long long id0, int px, int j, int k, int a0,
+                                          int fuse) {
+    using O = Ops<T, ExactOf<T>::value>;
+    T s[VW];
+#pragma unroll
+    for (int e = 0; e < VW; e++) s[e] = T(0);
+#pragma unroll
+    for (int q = 0; q < Lay7<NPT>::terms; q++) {
+        if (q == Lay7<NPT>::centre) continue;
+        const int o = off.o[Lay7<NPT>::slot(q)];
+        const bool al = (o % VW) == 0;
+        T cv[VW], vv[VW];
+        ldv<VW>(opr + (long long)Lay7<NPT>::plane(q) * L.plane + id0 + (Lay7<NPT>::at_nbr(q) ? o : 0),
+                Lay7<NPT>::at_nbr(q) ? al : true, cv);
+        ldv<VW>(v + id0 + o, al, vv);
+#pragma unroll
+        for (int e = 0; e < VW; e++) s[e] = O::mac(s[e], cv[e], vv[e]);
+    }
+    T dv[VW], fv[VW], out[VW];
+    ldv<VW>(opr + (long long)Lay7<NPT>::plane(Lay7<NPT>::centre) * L.plane + id0, true, dv);
+    ldv<VW>(f + id0, true, fv);
+#pragma unroll
+    for (int e = 0; e < VW; e++) out[e] = O::div(O::sub(fv[e], s[e]), O::add(dv[e], T(kEps)));
+    stv<VW>(v + id0, out);
+    if (fuse) {
+#pragma unroll
+        for (int e = 0; e < VW; e++) {
+            const int i = px + 2 * (a0 + e);
+            if (on_periodic_face(L, i, j, k)) write_images(L, v, i, j, k, out[e]);
+        }
+    }
+}
+
+// One colour of the 8-colour Gauss-Seidel (bbmg_class.f90:872-885) on the
+// points i = px + 2a, j = py + 2b, k = pz + 2c.  With `fuse` the new value is
+// also written into its periodic images (the vsync after the colour); that is
+// only race-free when every periodic direction has an even size, otherwise the
 // caller runs the overlap copy as a separate pass.
-template <typename T, int NPT>
+template <typename T, int NPT, int VW>
 __global__ void __launch_bounds__(256) k_relax(Lay L, Off27 off, const T *__restrict__ opr, T *v,
                                                 const T *__restrict__ f, int px, int py, int pz, int fuse) {
     pdl_entry();
-    using O = Ops<T, ExactOf<T>::value>;
     const int na = (L.nx - px + 1) >> 1, nb = (L.ny - py + 1) >> 1, nc = (L.nz - pz + 1) >> 1;
-    const long long total = (long long)na * nb * nc;
-    for (long long t = gtid(); t < total; t += gstride()) {
-        int a = (int)(t % na);
-        long long rr = t / na;
-        int b = (int)(rr % nb), c = (int)(rr / nb);
-        int i = px + 2 * a, j = py + 2 * b, k = pz + 2 * c;
-        long long id = L.idx(i, j, k);
-        T s = T(0);
-#pragma unroll
-        for (int q = 0; q < Lay7<NPT>::terms; q++) {
-            if (q == Lay7<NPT>::centre) continue;
-            const int o = off.o[Lay7<NPT>::slot(q)];
-            s = O::mac(s, opr[Lay7<NPT>::plane(q) * L.plane + id + (Lay7<NPT>::at_nbr(q) ? o : 0)], v[id + o]);
+    const int nrows = nb * nc, nch = na / VW;
+    const long long hb = px ? 0 : L.B0;
+    FOR_ROWS(nrows) {
+        const int b = row % nb, c = row / nb;
+        const int j = py + 2 * b, k = pz + 2 * c;
+        const long long base = L.G + L.row(j, k) * L.P + hb;
+        FOR_CHUNKS(nch) {
+            gs_points<T, NPT, VW>(L, off, opr, v, f, base + (long long)ch * VW, px, j, k, ch * VW, fuse);
         }
-        T d = opr[Lay7<NPT>::plane(Lay7<NPT>::centre) * L.plane + id];
-        T val = O::div(O::sub(f[id], s), O::add(d, T(kEps)));
-        v[id] = val;
-        if (fuse && on_periodic_face(L, i, j, k)) write_images(L, v, i, j, k, val);
+    }
+}
+
+// 7-point operators: the colours of one sweep only couple to colours of
+// Hamming weight +-1 (weight = px+py+pz), so the 8-colour sweep in the
+// reference's order equals four phases by weight (0,1,2,3 forward, 3,2,1,0
+// backward): the colours inside a phase never read each other.  A phase
+// repeated back to back (the last of a forward sweep and the first of the
+// following backward sweep) recomputes identical values and is skipped.  The
+// result is bit-identical to the colour-by-colour sweep; one launch per
+// phase, blockIdx.z = colour within the phase.
+struct PhaseCols {
+    int n;         // colours in the phase (1..3)
+    int col[3];    // colour index px + 2py + 4pz, ascending
+    Off27 off[2];  // neighbour offsets for even / odd x
+};
+
+template <typename T, int NPT, int VW>
+__global__ void __launch_bounds__(256) k_relax_phase7(Lay L, const T *__restrict__ opr, T *v,
+                                                       const T *__restrict__ f, PhaseCols pc, int fuse) {
+    pdl_entry();
+    const int col = pc.col[blockIdx.z];
+    const int px = col & 1, py = (col >> 1) & 1, pz = (col >> 2) & 1;
+    const int na = (L.nx - px + 1) >> 1, nb = (L.ny - py + 1) >> 1, nc = (L.nz - pz + 1) >> 1;
+    const int nrows = nb * nc, nch = na / VW;
+    const long long hb = px ? 0 : L.B0;
+    const Off27 &off = pc.off[px];
+    FOR_ROWS(nrows) {
+        const int b = row % nb, c = row / nb;
+        const int j = py + 2 * b, k = pz + 2 * c;
+        const long long base = L.G + L.row(j, k) * L.P + hb;
+        FOR_CHUNKS(nch) {
+            gs_points<T, NPT, VW>(L, off, opr, v, f, base + (long long)ch * VW, px, j, k, ch * VW, fuse);
+        }
     }
 }
 
 // Residual r = f - sum_l opr(l) v(nbr) on the interior, periodic images
 // written (bbmg_class.f90:831-844).  With f == nullptr the kernel returns the
-// operator product itself (the PCG's Ap, bbmg_class.f90:676-683).
+// operator product itself.
 template <typename T, int NPT>
 __global__ void __launch_bounds__(256) k_residual(Lay L, NbrOff nb, const T *__restrict__ opr,
                                                    const T *__restrict__ v, const T *__restrict__ f,
                                                    T *__restrict__ r) {
     pdl_entry();
     using O = Ops<T, ExactOf<T>::value>;
-    const long long total = (long long)L.nx * L.ny * L.nz;
-    for (long long t = gtid(); t < total; t += gstride()) {
-        int i, j, k;
-        interior_cell(L, t, i, j, k);
-        const int par = i & 1;
-        long long id = L.idx(i, j, k);
-        T s = T(0);
+    FOR_ROWS(L.ny * L.nz) {
+        const int j = row % L.ny, k = row / L.ny;
+        FOR_CHUNKS(L.nx) {
+            const int i = x_of(L, ch);
+            const int par = i & 1;
+            const long long id = L.idx(i, j, k);
+            T s = T(0);
 #pragma unroll
-        for (int q = 0; q < Lay7<NPT>::terms; q++) {
-            const int q27i = Lay7<NPT>::slot(q);
-            const int o = par ? nb.off[1][q27i] : nb.off[0][q27i];
-            s = O::mac(s, opr[Lay7<NPT>::plane(q) * L.plane + id + (Lay7<NPT>::at_nbr(q) ? o : 0)], v[id + o]);
+            for (int q = 0; q < Lay7<NPT>::terms; q++) {
+                const int q27i = Lay7<NPT>::slot(q);
+                const int o = par ? nb.off[1][q27i] : nb.off[0][q27i];
+                s = O::mac(s, opr[(long long)Lay7<NPT>::plane(q) * L.plane + id + (Lay7<NPT>::at_nbr(q) ? o : 0)],
+                           v[id + o]);
+            }
+            const T val = f ? O::sub(f[id], s) : s;
+            r[id] = val;
+            if (on_periodic_face(L, i, j, k)) write_images(L, r, i, j, k, val);
         }
-        T val = f ? O::sub(f[id], s) : s;
-        r[id] = val;
-        if (on_periodic_face(L, i, j, k)) write_images(L, r, i, j, k, val);
     }
 }
 
@@ -134,27 +277,30 @@ __global__ void __launch_bounds__(256) k_restrict(Lay F, Lay C, const T *__restr
                                                    T *__restrict__ vC) {
     pdl_entry();
     using O = Ops<T, ExactOf<T>::value>;
-    const long long total = (long long)C.nx * C.ny * C.nz;
-    for (long long t = gtid(); t < total; t += gstride()) {
-        int ci, cj, ck;
-        interior_cell(C, t, ci, cj, ck);
-        int fi = 2 * ci, fj = 2 * cj, fk = 2 * ck;
-        int rk0 = -pmod(F.zper, fk - 1, F.nz), rk1 = pmod(F.zper, fk + 1, F.nz);
-        int rj0 = -pmod(F.yper, fj - 1, F.ny), rj1 = pmod(F.yper, fj + 1, F.ny);
-        int ri0 = -pmod(F.xper, fi - 1, F.nx), ri1 = pmod(F.xper, fi + 1, F.nx);
-        T s = T(0);
-        for (int rk = rk0; rk <= rk1; rk++)
-            for (int rj = rj0; rj <= rj1; rj++)
-                for (int ri = ri0; ri <= ri1; ri++) {
-                    long long fid = F.idx(fi + ri, fj + rj, fk + rk);
-                    s = O::mac(s, c2f[q8((1 - ri) / 2, (1 - rj) / 2, (1 - rk) / 2) * F.plane + fid], rF[fid]);
-                }
-        long long cid = C.idx(ci, cj, ck);
-        fC[cid] = s;
-        vC[cid] = T(0);
-        if (on_periodic_face(C, ci, cj, ck)) {
-            write_images(C, fC, ci, cj, ck, s);
-            write_images(C, vC, ci, cj, ck, T(0));
+    FOR_ROWS(C.ny * C.nz) {
+        const int cj = row % C.ny, ck = row / C.ny;
+        const int fj = 2 * cj, fk = 2 * ck;
+        const int rk0 = -pmod(F.zper, fk - 1, F.nz), rk1 = pmod(F.zper, fk + 1, F.nz);
+        const int rj0 = -pmod(F.yper, fj - 1, F.ny), rj1 = pmod(F.yper, fj + 1, F.ny);
+        FOR_CHUNKS(C.nx) {
+            const int ci = x_of(C, ch);
+            const int fi = 2 * ci;
+            const int ri0 = -pmod(F.xper, fi - 1, F.nx), ri1 = pmod(F.xper, fi + 1, F.nx);
+            T s = T(0);
+            for (int rk = rk0; rk <= rk1; rk++)
+                for (int rj = rj0; rj <= rj1; rj++)
+                    for (int ri = ri0; ri <= ri1; ri++) {
+                        const long long fid = F.idx(fi + ri, fj + rj, fk + rk);
+                        s = O::mac(s, c2f[(long long)q8((1 - ri) / 2, (1 - rj) / 2, (1 - rk) / 2) * F.plane + fid],
+                                   rF[fid]);
+                    }
+            const long long cid = C.idx(ci, cj, ck);
+            fC[cid] = s;
+            vC[cid] = T(0);
+            if (on_periodic_face(C, ci, cj, ck)) {
+                write_images(C, fC, ci, cj, ck, s);
+                write_images(C, vC, ci, cj, ck, T(0));
+            }
         }
     }
 }
@@ -167,21 +313,23 @@ __global__ void __launch_bounds__(256) k_prolong(Lay F, Lay C, const T *__restri
                                                   const T *__restrict__ vC, T *__restrict__ vF) {
     pdl_entry();
     using O = Ops<T, ExactOf<T>::value>;
-    const long long total = (long long)F.nx * F.ny * F.nz;
-    for (long long t = gtid(); t < total; t += gstride()) {
-        int i, j, k;
-        interior_cell(F, t, i, j, k);
-        const int n1 = i & 1, n2 = j & 1, n3 = k & 1;
-        const int ci = i >> 1, cj = j >> 1, ck = k >> 1;
-        long long id = F.idx(i, j, k);
-        T e = T(0);
-        for (int pk = 0; pk <= n3; pk++)
-            for (int pj = 0; pj <= n2; pj++)
-                for (int pi = 0; pi <= n1; pi++)
-                    e = O::mac(e, c2f[q8(pi, pj, pk) * F.plane + id], vC[C.idx(ci + pi, cj + pj, ck + pk)]);
-        T val = O::add(vF[id], e);
-        vF[id] = val;
-        if (on_periodic_face(F, i, j, k)) write_images(F, vF, i, j, k, val);
+    FOR_ROWS(F.ny * F.nz) {
+        const int j = row % F.ny, k = row / F.ny;
+        const int n2 = j & 1, n3 = k & 1, cj = j >> 1, ck = k >> 1;
+        FOR_CHUNKS(F.nx) {
+            const int i = x_of(F, ch);
+            const int n1 = i & 1, ci = i >> 1;
+            const long long id = F.idx(i, j, k);
+            T e = T(0);
+            for (int pk = 0; pk <= n3; pk++)
+                for (int pj = 0; pj <= n2; pj++)
+                    for (int pi = 0; pi <= n1; pi++)
+                        e = O::mac(e, c2f[(long long)q8(pi, pj, pk) * F.plane + id],
+                                   vC[C.idx(ci + pi, cj + pj, ck + pk)]);
+            const T val = O::add(vF[id], e);
+            vF[id] = val;
+            if (on_periodic_face(F, i, j, k)) write_images(F, vF, i, j, k, val);
+        }
     }
 }
 
@@ -247,13 +395,13 @@ __global__ void k_coarse_solve(Lay L, const double *__restrict__ LU, const int *
 }
 
 // ---------------------------------------------------------------------------
-// Deterministic reductions: a fixed grid of kRedBlocks blocks, fixed tree.
+// Deterministic reductions: a fixed grid per level, a fixed tree per block.
 template <int MODE>  // 0 = max with NaN propagation, 1 = sum
 __device__ __forceinline__ double block_reduce(double v, double *sh) {
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y;
     sh[tid] = v;
     __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    for (int s = nt / 2; s > 0; s >>= 1) {
         if (tid < s) {
             double a = sh[tid], b = sh[tid + s];
             if (MODE == 0) sh[tid] = (a != a || b != b) ? (a + b) : fmax(a, b);
@@ -265,21 +413,21 @@ __device__ __forceinline__ double block_reduce(double v, double *sh) {
     __syncthreads();
     return r;
 }
+__device__ __forceinline__ bool block_leader() { return threadIdx.x == 0 && threadIdx.y == 0; }
+__device__ __forceinline__ int block_id() { return blockIdx.y * gridDim.x + blockIdx.x; }
+__device__ __forceinline__ double max_nan(double m, double a) { return (a != a || m != m) ? (a + m) : fmax(m, a); }
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_maxabs_part(Lay L, const T *__restrict__ x, double *__restrict__ part) {
     pdl_entry();
     __shared__ double sh[256];
-    const long long total = (long long)L.nx * L.ny * L.nz;
     double m = 0.0;
-    for (long long t = gtid(); t < total; t += gstride()) {
-        int i, j, k;
-        interior_cell(L, t, i, j, k);
-        double a = fabs((double)x[L.idx(i, j, k)]);
-        m = (a != a || m != m) ? (a + m) : fmax(m, a);
+    FOR_ROWS(L.ny * L.nz) {
+        const int j = row % L.ny, k = row / L.ny;
+        FOR_CHUNKS(L.nx) m = max_nan(m, fabs((double)x[L.idx(x_of(L, ch), j, k)]));
     }
     m = block_reduce<0>(m, sh);
-    if (threadIdx.x == 0) part[blockIdx.x] = m;
+    if (block_leader()) part[block_id()] = m;
 }
 
 template <typename TA, typename TB>
@@ -287,27 +435,26 @@ __global__ void __launch_bounds__(256) k_dot_part(Lay L, const TA *__restrict__ 
                                                    double *__restrict__ part) {
     pdl_entry();
     __shared__ double sh[256];
-    const long long total = (long long)L.nx * L.ny * L.nz;
     double s = 0.0;
-    for (long long t = gtid(); t < total; t += gstride()) {
-        int i, j, k;
-        interior_cell(L, t, i, j, k);
-        long long id = L.idx(i, j, k);
-        s = __dadd_rn(s, __dmul_rn((double)a[id], (double)b[id]));
+    FOR_ROWS(L.ny * L.nz) {
+        const int j = row % L.ny, k = row / L.ny;
+        FOR_CHUNKS(L.nx) {
+            const long long id = L.idx(x_of(L, ch), j, k);
+            s = __dadd_rn(s, __dmul_rn((double)a[id], (double)b[id]));
+        }
     }
     s = block_reduce<1>(s, sh);
-    if (threadIdx.x == 0) part[blockIdx.x] = s;
+    if (block_leader()) part[block_id()] = s;
 }
 
 template <int MODE>
 __global__ void __launch_bounds__(256) k_final(const double *__restrict__ part, int n, double *__restrict__ out) {
     pdl_entry();
     __shared__ double sh[256];
-    double v = MODE == 0 ? 0.0 : 0.0;
+    double v = 0.0;
     for (int t = threadIdx.x; t < n; t += blockDim.x) {
         double a = part[t];
-        if (MODE == 0) v = (a != a || v != v) ? (a + v) : fmax(v, a);
-        else v = v + a;
+        v = MODE == 0 ? max_nan(v, a) : v + a;
     }
     v = block_reduce<MODE>(v, sh);
     if (threadIdx.x == 0) *out = v;
@@ -318,145 +465,35 @@ __global__ void __launch_bounds__(256) k_final(const double *__restrict__ part, 
 template <typename T>
 __global__ void __launch_bounds__(256) k_from_caller(Lay L, const double *__restrict__ src, int g, T *__restrict__ dst) {
     pdl_entry();
-    const long long total = (long long)L.nx * L.ny * L.nz;
     const long long sy = L.nx + 2 * g, sz = sy * (L.ny + 2 * g);
-    for (long long t = gtid(); t < total; t += gstride()) {
-        int i, j, k;
-        interior_cell(L, t, i, j, k);
-        T val = (T)src[(k + g) * sz + (j + g) * sy + (i + g)];
-        dst[L.idx(i, j, k)] = val;
-        if (on_periodic_face(L, i, j, k)) write_images(L, dst, i, j, k, val);
+    FOR_ROWS(L.ny * L.nz) {
+        const int j = row % L.ny, k = row / L.ny;
+        FOR_CHUNKS(L.nx) {
+            const int i = ch;  // natural order: coalesced reads of the caller's row
+            const T val = (T)src[(k + g) * sz + (j + g) * sy + (i + g)];
+            dst[L.idx(i, j, k)] = val;
+            if (on_periodic_face(L, i, j, k)) write_images(L, dst, i, j, k, val);
+        }
     }
 }
 
 __global__ void __launch_bounds__(256) k_to_caller(Lay L, const double *__restrict__ src, int g, double *__restrict__ dst) {
     pdl_entry();
-    const long long total = (long long)L.nx * L.ny * L.nz;
     const long long sy = L.nx + 2 * g, sz = sy * (L.ny + 2 * g);
-    for (long long t = gtid(); t < total; t += gstride()) {
-        int i, j, k;
-        interior_cell(L, t, i, j, k);
-        dst[(k + g) * sz + (j + g) * sy + (i + g)] = src[L.idx(i, j, k)];
+    FOR_ROWS(L.ny * L.nz) {
+        const int j = row % L.ny, k = row / L.ny;
+        FOR_CHUNKS(L.nx) {
+            const int i = ch;
+            dst[(k + g) * sz + (j + g) * sy + (i + g)] = src[L.idx(i, j, k)];
+        }
     }
 }
 
 __global__ void __launch_bounds__(256) k_to_f32(const double *__restrict__ src, float *__restrict__ dst, long long n) {
     pdl_entry();
-    for (long long t = gtid(); t < n; t += gstride()) dst[t] = (float)src[t];
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        dst[t] = (float)src[t];
 }
-
-// ---------------------------------------------------------------------------
-// launchers
-#define BB_CHECK_LAUNCH() do { cudaError_t e_ = cudaGetLastError(); if (e_ != cudaSuccess) return e_; } while (0)
-
-template <typename T>
-cudaError_t launch_relax(const Lay &L, const NbrOff &nb, int npt, bool fuse, const T *opr, T *v, const T *f, int dir,
-                         cudaStream_t s) {
-    const bool per = L.xper || L.yper || L.zper;
-    for (int c = 0; c < 8; c++) {
-        int col = dir > 0 ? c : 7 - c;  // colours 1..8 forward, 8..1 backward
-        int px = col & 1, py = (col >> 1) & 1, pz = (col >> 2) & 1;
-        long long n = (long long)((L.nx - px + 1) >> 1) * ((L.ny - py + 1) >> 1) * ((L.nz - pz + 1) >> 1);
-        if (n == 0) continue;
-        Off27 off = off_for(nb, px);
-        int g = grid_for(n, 256);
-        if (npt == 4) launch_k(k_relax<T, 4>, g, 256, 0, s, L, off, opr, v, f, px, py, pz, fuse ? 1 : 0);
-        else if (npt == 7) launch_k(k_relax<T, 7>, g, 256, 0, s, L, off, opr, v, f, px, py, pz, fuse ? 1 : 0);
-        else launch_k(k_relax<T, 27>, g, 256, 0, s, L, off, opr, v, f, px, py, pz, fuse ? 1 : 0);
-        BB_CHECK_LAUNCH();
-        if (per && !fuse) {
-            cudaError_t e = wrap_planes(L, v, 1, s);
-            if (e != cudaSuccess) return e;
-        }
-    }
-    return cudaSuccess;
-}
-
-template <typename T>
-cudaError_t launch_residual(const Lay &L, const NbrOff &nb, int npt, const T *opr, const T *v, const T *f, T *r,
-                            cudaStream_t s) {
-    long long n = (long long)L.nx * L.ny * L.nz;
-    int g = grid_for(n, 256);
-    if (npt == 4) launch_k(k_residual<T, 4>, g, 256, 0, s, L, nb, opr, v, f, r);
-    else if (npt == 7) launch_k(k_residual<T, 7>, g, 256, 0, s, L, nb, opr, v, f, r);
-    else launch_k(k_residual<T, 27>, g, 256, 0, s, L, nb, opr, v, f, r);
-    BB_CHECK_LAUNCH();
-    return cudaSuccess;
-}
-
-template <typename T>
-cudaError_t launch_restrict(const Lay &F, const Lay &C, const T *c2f, const T *rF, T *fC, T *vC, cudaStream_t s) {
-    long long n = (long long)C.nx * C.ny * C.nz;
-    launch_k(k_restrict<T>, grid_for(n, 256), 256, 0, s, F, C, c2f, rF, fC, vC);
-    BB_CHECK_LAUNCH();
-    return cudaSuccess;
-}
-
-template <typename T>
-cudaError_t launch_prolong(const Lay &F, const Lay &C, const T *c2f, const T *vC, T *vF, cudaStream_t s) {
-    long long n = (long long)F.nx * F.ny * F.nz;
-    launch_k(k_prolong<T>, grid_for(n, 256), 256, 0, s, F, C, c2f, vC, vF);
-    BB_CHECK_LAUNCH();
-    return cudaSuccess;
-}
-
-template <typename T>
-cudaError_t launch_coarse_solve(const Lay &L, const double *LU, const int *piv, const int *pinned, const T *f, T *v,
-                                cudaStream_t s) {
-    int np = L.nx * L.ny * L.nz;
-    size_t mat = (size_t)np * np * sizeof(double), vec = (size_t)np * sizeof(double);
-    int in_smem = (mat + vec) <= kCoarseSmem;
-    size_t shm = vec + (in_smem ? mat : 0);
-    launch_k(k_coarse_solve<T>, 1, 256, shm, s, L, LU, piv, pinned, f, v, in_smem);
-    BB_CHECK_LAUNCH();
-    return cudaSuccess;
-}
-
-cudaError_t coarse_solve_prepare() {
-    cudaError_t e = cudaFuncSetAttribute(k_coarse_solve<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCoarseSmem);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_coarse_solve<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCoarseSmem);
-}
-
-template <typename T>
-cudaError_t launch_maxabs(const Lay &L, const T *x, double *part, double *out, cudaStream_t s) {
-    launch_k(k_maxabs_part<T>, kRedBlocks, 256, 0, s, L, x, part);
-    BB_CHECK_LAUNCH();
-    launch_k(k_final<0>, 1, 256, 0, s, part, kRedBlocks, out);
-    BB_CHECK_LAUNCH();
-    return cudaSuccess;
-}
-
-template <typename T>
-cudaError_t launch_dot(const Lay &L, const T *a, const T *b, double *part, double *out, cudaStream_t s) {
-    launch_k(k_dot_part<T, T>, kRedBlocks, 256, 0, s, L, a, b, part);
-    BB_CHECK_LAUNCH();
-    launch_k(k_final<1>, 1, 256, 0, s, part, kRedBlocks, out);
-    BB_CHECK_LAUNCH();
-    return cudaSuccess;
-}
-
-template <typename T>
-cudaError_t launch_from_caller(const Lay &L, const double *src, int g, T *dst, cudaStream_t s) {
-    long long n = (long long)L.nx * L.ny * L.nz;
-    launch_k(k_from_caller<T>, grid_for(n, 256), 256, 0, s, L, src, g, dst);
-    BB_CHECK_LAUNCH();
-    return cudaSuccess;
-}
-
-cudaError_t launch_to_caller(const Lay &L, const double *src, int g, double *dst, cudaStream_t s) {
-    long long n = (long long)L.nx * L.ny * L.nz;
-    launch_k(k_to_caller, grid_for(n, 256), 256, 0, s, L, src, g, dst);
-    BB_CHECK_LAUNCH();
-    return cudaSuccess;
-}
-
-cudaError_t launch_to_f32(const double *src, float *dst, long long n, cudaStream_t s) {
-    launch_k(k_to_f32, grid_for(n, 256), 256, 0, s, src, dst, n);
-    BB_CHECK_LAUNCH();
-    return cudaSuccess;
-}
-
 
 // ---------------------------------------------------------------------------
 // PCG (bbmg_class.f90:643-703).  Scalars live on the device so an iteration
@@ -485,116 +522,11 @@ __global__ void k_cg_pap(const double *__restrict__ part, int n, CgScal *sc) {
         sc->alpha = __ddiv_rn(sc->rho1, v);
     }
 }
-// pp = zz + beta*pp, then the overlap copy of pp (bbmg_class.f90:674-676)
-template <typename TZ>
-__global__ void __launch_bounds__(256) k_cg_p(Lay L, const TZ *__restrict__ zz, double *__restrict__ pp,
-                                               const CgScal *__restrict__ sc) {
-    pdl_entry();
-    const double beta = sc->beta;
-    const long long total = (long long)L.nx * L.ny * L.nz;
-    for (long long t = gtid(); t < total; t += gstride()) {
-        int i, j, k;
-        interior_cell(L, t, i, j, k);
-        long long id = L.idx(i, j, k);
-        double val = __dadd_rn((double)zz[id], __dmul_rn(beta, pp[id]));
-        pp[id] = val;
-        if (on_periodic_face(L, i, j, k)) write_images(L, pp, i, j, k, val);
-    }
-}
-// sol += alpha*pp; res -= alpha*Ap (bbmg_class.f90:688-692)
-__global__ void __launch_bounds__(256) k_cg_xr(Lay L, double *__restrict__ sol, const double *__restrict__ pp,
-                                                double *__restrict__ res, const double *__restrict__ Ap,
-                                                const CgScal *__restrict__ sc) {
-    pdl_entry();
-    const double alpha = sc->alpha;
-    const long long total = (long long)L.nx * L.ny * L.nz;
-    for (long long t = gtid(); t < total; t += gstride()) {
-        int i, j, k;
-        interior_cell(L, t, i, j, k);
-        long long id = L.idx(i, j, k);
-        sol[id] = __dadd_rn(sol[id], __dmul_rn(alpha, pp[id]));
-        res[id] = __dsub_rn(res[id], __dmul_rn(alpha, Ap[id]));
-    }
-}
 
-// mixed precision: FP64 residual -> FP32 right-hand side of the V-cycle
-__global__ void __launch_bounds__(256) k_round_f32(Lay L, const double *__restrict__ r, float *__restrict__ f) {
-    pdl_entry();
-    const long long total = (long long)L.nx * L.ny * L.nz;
-    for (long long t = gtid(); t < total; t += gstride()) {
-        int i, j, k;
-        interior_cell(L, t, i, j, k);
-        long long id = L.idx(i, j, k);
-        f[id] = (float)r[id];
-    }
-}
-// mixed precision: x += e (FP32 correction accumulated in FP64), images kept
-__global__ void __launch_bounds__(256) k_add_correction(Lay L, double *__restrict__ x, const float *__restrict__ e) {
-    pdl_entry();
-    const long long total = (long long)L.nx * L.ny * L.nz;
-    for (long long t = gtid(); t < total; t += gstride()) {
-        int i, j, k;
-        interior_cell(L, t, i, j, k);
-        long long id = L.idx(i, j, k);
-        double val = x[id] + (double)e[id];
-        x[id] = val;
-        if (on_periodic_face(L, i, j, k)) write_images(L, x, i, j, k, val);
-    }
-}
-
-template <typename TZ>
-cudaError_t launch_cg_rho(const Lay &L, const TZ *zz, const double *res, double *part, CgScal *sc, cudaStream_t s) {
-    launch_k(k_dot_part<TZ, double>, kRedBlocks, 256, 0, s, L, zz, res, part);
-    BB_CHECK_LAUNCH();
-    launch_k(k_cg_rho, 1, 256, 0, s, part, kRedBlocks, sc);
-    BB_CHECK_LAUNCH();
-    return cudaSuccess;
-}
-template <typename TZ>
-cudaError_t launch_cg_p(const Lay &L, const TZ *zz, double *pp, const CgScal *sc, cudaStream_t s) {
-    long long n = (long long)L.nx * L.ny * L.nz;
-    launch_k(k_cg_p<TZ>, grid_for(n, 256), 256, 0, s, L, zz, pp, sc);
-    BB_CHECK_LAUNCH();
-    return cudaSuccess;
-}
-cudaError_t launch_cg_pap(const Lay &L, const double *pp, const double *Ap, double *part, CgScal *sc, cudaStream_t s) {
-    launch_k(k_dot_part<double, double>, kRedBlocks, 256, 0, s, L, pp, Ap, part);
-    BB_CHECK_LAUNCH();
-    launch_k(k_cg_pap, 1, 256, 0, s, part, kRedBlocks, sc);
-    BB_CHECK_LAUNCH();
-    return cudaSuccess;
-}
-cudaError_t launch_cg_xr(const Lay &L, double *sol, const double *pp, double *res, const double *Ap, const CgScal *sc,
-                         cudaStream_t s) {
-    long long n = (long long)L.nx * L.ny * L.nz;
-    launch_k(k_cg_xr, grid_for(n, 256), 256, 0, s, L, sol, pp, res, Ap, sc);
-    BB_CHECK_LAUNCH();
-    return cudaSuccess;
-}
-cudaError_t launch_round_f32(const Lay &L, const double *r, float *f, cudaStream_t s) {
-    long long n = (long long)L.nx * L.ny * L.nz;
-    launch_k(k_round_f32, grid_for(n, 256), 256, 0, s, L, r, f);
-    BB_CHECK_LAUNCH();
-    return cudaSuccess;
-}
-cudaError_t launch_add_correction(const Lay &L, double *x, const float *e, cudaStream_t s) {
-    long long n = (long long)L.nx * L.ny * L.nz;
-    launch_k(k_add_correction, grid_for(n, 256), 256, 0, s, L, x, e);
-    BB_CHECK_LAUNCH();
-    return cudaSuccess;
-}
-template cudaError_t launch_cg_rho<double>(const Lay &, const double *, const double *, double *, CgScal *, cudaStream_t);
-template cudaError_t launch_cg_rho<float>(const Lay &, const float *, const double *, double *, CgScal *, cudaStream_t);
-template cudaError_t launch_cg_p<double>(const Lay &, const double *, double *, const CgScal *, cudaStream_t);
-template cudaError_t launch_cg_p<float>(const Lay &, const float *, double *, const CgScal *, cudaStream_t);
-
-
-// ---------------------------------------------------------------------------
-// Fused CG steps.  pp_new = zz + beta*pp_old on the own cell (with images) and
-// Ap = A pp_new, the neighbours' pp_new formed on the fly from zz and pp_old
-// (bit-identical to the stored value), plus the block partial of pp_new.Ap
-// (bbmg_class.f90:674-687 in one pass).  pp_old and pp_new are distinct
-// buffers.
+// pp_new = zz + beta*pp_old on the own cell (with images) and Ap = A pp_new,
+// the neighbours' pp_new formed on the fly from zz and pp_old (bit-identical
+// to the stored value), plus the block partial of pp_new.Ap
+// (bbmg_class.f90:674-687 in one pass).  pp_old and pp_new are distinct.
 template <typename TZ, int NPT>
 __global__ void __launch_bounds__(256) k_cg_pap_fused(Lay L, NbrOff nb, const double *__restrict__ opr,
                                                        const TZ *__restrict__ zz, const double *__restrict__ pp_old,
@@ -603,29 +535,32 @@ __global__ void __launch_bounds__(256) k_cg_pap_fused(Lay L, NbrOff nb, const do
     pdl_entry();
     __shared__ double sh[256];
     const double beta = sc->beta;
-    const long long total = (long long)L.nx * L.ny * L.nz;
     double acc = 0.0;
-    for (long long t = gtid(); t < total; t += gstride()) {
-        int i, j, k;
-        interior_cell(L, t, i, j, k);
-        const int par = i & 1;
-        const long long id = L.idx(i, j, k);
-        double s = 0.0, pc = 0.0;
+    FOR_ROWS(L.ny * L.nz) {
+        const int j = row % L.ny, k = row / L.ny;
+        FOR_CHUNKS(L.nx) {
+            const int i = x_of(L, ch);
+            const int par = i & 1;
+            const long long id = L.idx(i, j, k);
+            double s = 0.0, pc = 0.0;
 #pragma unroll
-        for (int q = 0; q < Lay7<NPT>::terms; q++) {
-            const int q27i = Lay7<NPT>::slot(q);
-            const int o = par ? nb.off[1][q27i] : nb.off[0][q27i];
-            const double pq = __dadd_rn((double)zz[id + o], __dmul_rn(beta, pp_old[id + o]));
-            if (q == Lay7<NPT>::centre) pc = pq;
-            s = __dadd_rn(s, __dmul_rn(opr[Lay7<NPT>::plane(q) * L.plane + id + (Lay7<NPT>::at_nbr(q) ? o : 0)], pq));
+            for (int q = 0; q < Lay7<NPT>::terms; q++) {
+                const int q27i = Lay7<NPT>::slot(q);
+                const int o = par ? nb.off[1][q27i] : nb.off[0][q27i];
+                const double pq = __dadd_rn((double)zz[id + o], __dmul_rn(beta, pp_old[id + o]));
+                if (q == Lay7<NPT>::centre) pc = pq;
+                s = __dadd_rn(s, __dmul_rn(opr[(long long)Lay7<NPT>::plane(q) * L.plane + id +
+                                               (Lay7<NPT>::at_nbr(q) ? o : 0)],
+                                           pq));
+            }
+            pp_new[id] = pc;
+            if (on_periodic_face(L, i, j, k)) write_images(L, pp_new, i, j, k, pc);
+            Ap[id] = s;
+            acc = __dadd_rn(acc, __dmul_rn(pc, s));
         }
-        pp_new[id] = pc;
-        if (on_periodic_face(L, i, j, k)) write_images(L, pp_new, i, j, k, pc);
-        Ap[id] = s;
-        acc = __dadd_rn(acc, __dmul_rn(pc, s));
     }
     acc = block_reduce<1>(acc, sh);
-    if (threadIdx.x == 0) part[blockIdx.x] = acc;
+    if (block_leader()) part[block_id()] = acc;
 }
 
 // sol += alpha*pp; res -= alpha*Ap; block partial of max|res|
@@ -640,117 +575,160 @@ __global__ void __launch_bounds__(256) k_cg_xr_fused(Lay L, double *__restrict__
     pdl_entry();
     __shared__ double sh[256];
     const double alpha = sc->alpha;
-    const long long total = (long long)L.nx * L.ny * L.nz;
     double m = 0.0;
-    for (long long t = gtid(); t < total; t += gstride()) {
-        int i, j, k;
-        interior_cell(L, t, i, j, k);
-        const long long id = L.idx(i, j, k);
-        sol[id] = __dadd_rn(sol[id], __dmul_rn(alpha, pp[id]));
-        const double r = __dsub_rn(res[id], __dmul_rn(alpha, Ap[id]));
-        res[id] = r;
-        const double a = fabs(r);
-        m = (a != a || m != m) ? (a + m) : fmax(m, a);
-        if (f32) f32[id] = (float)r;
-        vzero[id] = TV(0);
-        if (on_periodic_face(L, i, j, k)) write_images(L, vzero, i, j, k, TV(0));
+    FOR_ROWS(L.ny * L.nz) {
+        const int j = row % L.ny, k = row / L.ny;
+        FOR_CHUNKS(L.nx) {
+            const int i = x_of(L, ch);
+            const long long id = L.idx(i, j, k);
+            sol[id] = __dadd_rn(sol[id], __dmul_rn(alpha, pp[id]));
+            const double r = __dsub_rn(res[id], __dmul_rn(alpha, Ap[id]));
+            res[id] = r;
+            m = max_nan(m, fabs(r));
+            if (f32) f32[id] = (float)r;
+            vzero[id] = TV(0);
+            if (on_periodic_face(L, i, j, k)) write_images(L, vzero, i, j, k, TV(0));
+        }
     }
     m = block_reduce<0>(m, sh);
-    if (threadIdx.x == 0) part[blockIdx.x] = m;
+    if (block_leader()) part[block_id()] = m;
 }
 
-template <typename TZ>
-cudaError_t launch_cg_pap_fused(const Lay &L, const NbrOff &nb, int npt, const double *opr, const TZ *zz,
-                                const double *pp_old, double *pp_new, double *Ap, double *part, CgScal *sc,
-                                cudaStream_t s) {
-    if (npt == 4) launch_k(k_cg_pap_fused<TZ, 4>, kRedBlocks, 256, 0, s, L, nb, opr, zz, pp_old, pp_new, Ap, sc, part);
-    else if (npt == 7) launch_k(k_cg_pap_fused<TZ, 7>, kRedBlocks, 256, 0, s, L, nb, opr, zz, pp_old, pp_new, Ap, sc, part);
-    else launch_k(k_cg_pap_fused<TZ, 27>, kRedBlocks, 256, 0, s, L, nb, opr, zz, pp_old, pp_new, Ap, sc, part);
-    BB_CHECK_LAUNCH();
-    launch_k(k_cg_pap, 1, 256, 0, s, part, kRedBlocks, sc);
-    BB_CHECK_LAUNCH();
-    return cudaSuccess;
-}
-
-template <typename TV>
-cudaError_t launch_cg_xr_fused(const Lay &L, double *sol, const double *pp, double *res, const double *Ap,
-                               const CgScal *sc, float *f32, TV *vzero, double *part, double *out, cudaStream_t s) {
-    launch_k(k_cg_xr_fused<TV>, kRedBlocks, 256, 0, s, L, sol, pp, res, Ap, sc, f32, vzero, part);
-    BB_CHECK_LAUNCH();
-    launch_k(k_final<0>, 1, 256, 0, s, part, kRedBlocks, out);
-    BB_CHECK_LAUNCH();
-    return cudaSuccess;
-}
-template cudaError_t launch_cg_pap_fused<double>(const Lay &, const NbrOff &, int, const double *, const double *,
-                                                 const double *, double *, double *, double *, CgScal *, cudaStream_t);
-template cudaError_t launch_cg_pap_fused<float>(const Lay &, const NbrOff &, int, const double *, const float *,
-                                                const double *, double *, double *, double *, CgScal *, cudaStream_t);
-template cudaError_t launch_cg_xr_fused<double>(const Lay &, double *, const double *, double *, const double *,
-                                                const CgScal *, float *, double *, double *, double *, cudaStream_t);
-template cudaError_t launch_cg_xr_fused<float>(const Lay &, double *, const double *, double *, const double *,
-                                               const CgScal *, float *, float *, double *, double *, cudaStream_t);
-
-// ---------------------------------------------------------------------------
-// 7-point operators: the colours of one Gauss-Seidel sweep only couple to
-// colours of Hamming weight +-1 (weight = px+py+pz), so the 8-colour sweep in
-// the reference's order equals four phases by weight (0,1,2,3 forward,
-// 3,2,1,0 backward): the colours inside a phase never read each other.  A phase
-// repeated back to back (the last of a forward sweep and the first of the
-// following backward sweep) recomputes identical values and is skipped.  The
-// result is bit-identical to the colour-by-colour sweep; one launch per phase.
-struct PhaseCols {
-    int n;             // colours in the phase (1..3)
-    int col[3];        // colour index px + 2py + 4pz, ascending
-    long long beg[4];  // prefix sums of the colour point counts
-};
-
-template <typename T, int NPT>
-__global__ void __launch_bounds__(256) k_relax_phase7(Lay L, NbrOff nb, const T *__restrict__ opr, T *v,
-                                                       const T *__restrict__ f, PhaseCols pc, int fuse) {
+// mixed precision: FP64 residual -> FP32 right-hand side of the V-cycle
+__global__ void __launch_bounds__(256) k_round_f32(Lay L, const double *__restrict__ r, float *__restrict__ f) {
     pdl_entry();
-    using O = Ops<T, ExactOf<T>::value>;
-    const long long total = pc.beg[pc.n];
-    for (long long t = gtid(); t < total; t += gstride()) {
-        int c = 0;
-        if (pc.n > 1 && t >= pc.beg[1]) c = (pc.n > 2 && t >= pc.beg[2]) ? 2 : 1;
-        const int col = pc.col[c];
-        const int px = col & 1, py = (col >> 1) & 1, pz = (col >> 2) & 1;
-        const int na = (L.nx - px + 1) >> 1, nbb = (L.ny - py + 1) >> 1;
-        const long long u = t - pc.beg[c];
-        const int a = (int)(u % na);
-        const long long rr = u / na;
-        const int b = (int)(rr % nbb), cc = (int)(rr / nbb);
-        const int i = px + 2 * a, j = py + 2 * b, k = pz + 2 * cc;
-        const long long id = L.idx(i, j, k);
-        T s = T(0);
-#pragma unroll
-        for (int q = 0; q < 7; q++) {
-            if (q == kCentre7) continue;
-            const int q27i = k7to27(q);
-            const int o = px ? nb.off[1][q27i] : nb.off[0][q27i];
-            s = O::mac(s, opr[Lay7<NPT>::plane(q) * L.plane + id + (Lay7<NPT>::at_nbr(q) ? o : 0)], v[id + o]);
+    FOR_ROWS(L.ny * L.nz) {
+        const int j = row % L.ny, k = row / L.ny;
+        FOR_CHUNKS(L.nx) {
+            const long long id = L.idx(x_of(L, ch), j, k);
+            f[id] = (float)r[id];
         }
-        const T d = opr[Lay7<NPT>::plane(kCentre7) * L.plane + id];
-        const T val = O::div(O::sub(f[id], s), O::add(d, T(kEps)));
-        v[id] = val;
-        if (fuse && on_periodic_face(L, i, j, k)) write_images(L, v, i, j, k, val);
     }
 }
 
-static PhaseCols phase_cols(const Lay &L, int w) {
+// Mixed-precision defect correction step (the FP64 half of an mgsolve
+// iteration, bbmg_class.f90:716-722 with the correction of 770): x_new = x + e
+// on the own cell (images written), r = b - A (x + e) with the neighbours'
+// x + e formed on the fly; r becomes the FP32 right-hand side of the next
+// V-cycle and the block partial of max|r| is written.  x_old and x_new are
+// distinct buffers; e is only read (its neighbours are needed by other
+// threads), so it is zeroed for the next V-cycle by a separate memset.
+template <int NPT>
+__global__ void __launch_bounds__(256) k_defect_fused(Lay L, NbrOff nb, const double *__restrict__ opr,
+                                                       const double *__restrict__ x_old, const float *__restrict__ e,
+                                                       const double *__restrict__ b, double *__restrict__ x_new,
+                                                       float *__restrict__ f32, double *__restrict__ part) {
+    pdl_entry();
+    __shared__ double sh[256];
+    double m = 0.0;
+    FOR_ROWS(L.ny * L.nz) {
+        const int j = row % L.ny, k = row / L.ny;
+        FOR_CHUNKS(L.nx) {
+            const int i = x_of(L, ch);
+            const int par = i & 1;
+            const long long id = L.idx(i, j, k);
+            double s = 0.0, xc = 0.0;
+#pragma unroll
+            for (int q = 0; q < Lay7<NPT>::terms; q++) {
+                const int q27i = Lay7<NPT>::slot(q);
+                const int o = par ? nb.off[1][q27i] : nb.off[0][q27i];
+                const double xq = x_old[id + o] + (double)e[id + o];
+                if (q == Lay7<NPT>::centre) xc = xq;
+                s = fma(opr[(long long)Lay7<NPT>::plane(q) * L.plane + id + (Lay7<NPT>::at_nbr(q) ? o : 0)], xq, s);
+            }
+            const double r = b[id] - s;
+            x_new[id] = xc;
+            f32[id] = (float)r;
+            if (on_periodic_face(L, i, j, k)) write_images(L, x_new, i, j, k, xc);
+            m = max_nan(m, fabs(r));
+        }
+    }
+    m = block_reduce<0>(m, sh);
+    if (block_leader()) part[block_id()] = m;
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+template <typename T> static int vw_for(int n);
+template <> int vw_for<float>(int n) { return (n % 4 == 0) ? 4 : ((n % 2 == 0) ? 2 : 1); }
+template <> int vw_for<double>(int n) { return (n % 2 == 0) ? 2 : 1; }
+template <typename T> struct VwMax { static constexpr int value = sizeof(T) == 4 ? 4 : 2; };
+
+template <typename T, int NPT>
+static cudaError_t launch_colour(const Lay &L, const Off27 &off, const T *opr, T *v, const T *f, int px, int py,
+                                 int pz, int fuse, cudaStream_t s) {
+    const int na = (L.nx - px + 1) >> 1;
+    const long long nrows = (long long)((L.ny - py + 1) >> 1) * ((L.nz - pz + 1) >> 1);
+    const int vw = vw_for<T>(na);
+    const Geo g = geo_rows(na / vw, nrows);
+    if (vw == VwMax<T>::value)
+        BB_CHECK_LAUNCH((launch_k(k_relax<T, NPT, VwMax<T>::value>, g.grid, g.block, 0, s, L, off, opr, v, f, px, py, pz, fuse)));
+    else if (vw == 2)
+        BB_CHECK_LAUNCH((launch_k(k_relax<T, NPT, 2>, g.grid, g.block, 0, s, L, off, opr, v, f, px, py, pz, fuse)));
+    else
+        BB_CHECK_LAUNCH((launch_k(k_relax<T, NPT, 1>, g.grid, g.block, 0, s, L, off, opr, v, f, px, py, pz, fuse)));
+    return cudaSuccess;
+}
+
+template <typename T>
+cudaError_t launch_relax(const Lay &L, const NbrOff &nb, int npt, bool fuse, const T *opr, T *v, const T *f, int dir,
+                         cudaStream_t s) {
+    const bool per = L.xper || L.yper || L.zper;
+    for (int c = 0; c < 8; c++) {
+        int col = dir > 0 ? c : 7 - c;  // colours 1..8 forward, 8..1 backward
+        int px = col & 1, py = (col >> 1) & 1, pz = (col >> 2) & 1;
+        long long n = (long long)((L.nx - px + 1) >> 1) * ((L.ny - py + 1) >> 1) * ((L.nz - pz + 1) >> 1);
+        if (n == 0) continue;
+        Off27 off = off_for(nb, px);
+        cudaError_t e;
+        if (npt == 4) e = launch_colour<T, 4>(L, off, opr, v, f, px, py, pz, fuse ? 1 : 0, s);
+        else if (npt == 7) e = launch_colour<T, 7>(L, off, opr, v, f, px, py, pz, fuse ? 1 : 0, s);
+        else e = launch_colour<T, 27>(L, off, opr, v, f, px, py, pz, fuse ? 1 : 0, s);
+        if (e != cudaSuccess) return e;
+        if (per && !fuse) {
+            e = wrap_planes(L, v, 1, s);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    return cudaSuccess;
+}
+
+static PhaseCols phase_cols(const Lay &L, const NbrOff &nb, int w, int vw_cap, int &vw, long long &rows,
+                            int &chunks) {
     PhaseCols p{};
     p.n = 0;
-    p.beg[0] = 0;
+    p.off[0] = off_for(nb, 0);
+    p.off[1] = off_for(nb, 1);
+    vw = vw_cap;
+    rows = 0;
+    int na_max = 0;
     for (int col = 0; col < 8; col++) {
         if (__builtin_popcount(col) != w) continue;
         int px = col & 1, py = (col >> 1) & 1, pz = (col >> 2) & 1;
-        long long cnt = (long long)((L.nx - px + 1) >> 1) * ((L.ny - py + 1) >> 1) * ((L.nz - pz + 1) >> 1);
-        if (cnt == 0) continue;
-        p.col[p.n] = col;
-        p.beg[p.n + 1] = p.beg[p.n] + cnt;
-        p.n++;
+        int na = (L.nx - px + 1) >> 1;
+        long long nr = (long long)((L.ny - py + 1) >> 1) * ((L.nz - pz + 1) >> 1);
+        if (na == 0 || nr == 0) continue;
+        p.col[p.n++] = col;
+        while (vw > 1 && na % vw) vw >>= 1;
+        if (nr > rows) rows = nr;
+        if (na > na_max) na_max = na;
     }
+    chunks = na_max / vw;
     return p;
+}
+
+template <typename T, int NPT>
+static cudaError_t launch_phase(const Lay &L, const PhaseCols &pc, int vw, long long rows, int chunks, const T *opr,
+                                T *v, const T *f, cudaStream_t s) {
+    Geo g = geo_rows(chunks, rows, 148LL * 24 / (pc.n > 0 ? pc.n : 1));
+    g.grid.z = pc.n;
+    if (vw == VwMax<T>::value)
+        BB_CHECK_LAUNCH((launch_k(k_relax_phase7<T, NPT, VwMax<T>::value>, g.grid, g.block, 0, s, L, opr, v, f, pc, 1)));
+    else if (vw == 2)
+        BB_CHECK_LAUNCH((launch_k(k_relax_phase7<T, NPT, 2>, g.grid, g.block, 0, s, L, opr, v, f, pc, 1)));
+    else
+        BB_CHECK_LAUNCH((launch_k(k_relax_phase7<T, NPT, 1>, g.grid, g.block, 0, s, L, opr, v, f, pc, 1)));
+    return cudaSuccess;
 }
 
 template <typename T>
@@ -771,81 +749,153 @@ cudaError_t launch_relax_sweeps(const Lay &L, const NbrOff &nb, int npt, bool fu
             int w = dir > 0 ? p : 3 - p;
             if (w == last) continue;  // identical recomputation
             last = w;
-            PhaseCols pc = phase_cols(L, w);
+            int vw, chunks;
+            long long rows;
+            PhaseCols pc = phase_cols(L, nb, w, VwMax<T>::value, vw, rows, chunks);
             if (pc.n == 0) continue;
-            if (npt == 4) launch_k(k_relax_phase7<T, 4>, grid_for(pc.beg[pc.n], 256), 256, 0, s, L, nb, opr, v, f, pc, 1);
-            else launch_k(k_relax_phase7<T, 7>, grid_for(pc.beg[pc.n], 256), 256, 0, s, L, nb, opr, v, f, pc, 1);
-            BB_CHECK_LAUNCH();
+            cudaError_t e = npt == 4 ? launch_phase<T, 4>(L, pc, vw, rows, chunks, opr, v, f, s)
+                                     : launch_phase<T, 7>(L, pc, vw, rows, chunks, opr, v, f, s);
+            if (e != cudaSuccess) return e;
         }
         dir = -dir;
     }
     return cudaSuccess;
 }
-template cudaError_t launch_relax_sweeps<double>(const Lay &, const NbrOff &, int, bool, const double *, double *,
-                                                 const double *, int, int, cudaStream_t);
-template cudaError_t launch_relax_sweeps<float>(const Lay &, const NbrOff &, int, bool, const float *, float *,
-                                                const float *, int, int, cudaStream_t);
 
-// ---------------------------------------------------------------------------
-// Mixed-precision defect correction step (the FP64 half of an mgsolve
-// iteration, bbmg_class.f90:716-722 with the correction of 770): x_new = x + e
-// on the own cell (images written), r = b - A (x + e) with the neighbours'
-// x + e formed on the fly; r becomes the FP32 right-hand side of the next
-// V-cycle, the FP32 correction is zeroed for it, and the block partial of
-// max|r| is written.  x_old and x_new are distinct buffers.
-template <int NPT>
-__global__ void __launch_bounds__(256) k_defect_fused(Lay L, NbrOff nb, const double *__restrict__ opr,
-                                                       const double *__restrict__ x_old, const float *__restrict__ e,
-                                                       const double *__restrict__ b, double *__restrict__ x_new,
-                                                       float *__restrict__ f32, float *__restrict__ v32,
-                                                       double *__restrict__ part) {
-    pdl_entry();
-    __shared__ double sh[256];
-    const long long total = (long long)L.nx * L.ny * L.nz;
-    double m = 0.0;
-    for (long long t = gtid(); t < total; t += gstride()) {
-        int i, j, k;
-        interior_cell(L, t, i, j, k);
-        const int par = i & 1;
-        const long long id = L.idx(i, j, k);
-        double s = 0.0, xc = 0.0;
-#pragma unroll
-        for (int q = 0; q < Lay7<NPT>::terms; q++) {
-            const int q27i = Lay7<NPT>::slot(q);
-            const int o = par ? nb.off[1][q27i] : nb.off[0][q27i];
-            const double xq = x_old[id + o] + (double)e[id + o];
-            if (q == Lay7<NPT>::centre) xc = xq;
-            s = fma(opr[Lay7<NPT>::plane(q) * L.plane + id + (Lay7<NPT>::at_nbr(q) ? o : 0)], xq, s);
-        }
-        const double r = b[id] - s;
-        x_new[id] = xc;
-        f32[id] = (float)r;
-        v32[id] = 0.0f;
-        if (on_periodic_face(L, i, j, k)) {
-            write_images(L, x_new, i, j, k, xc);
-            write_images(L, v32, i, j, k, 0.0f);
-        }
-        const double a = fabs(r);
-        m = (a != a || m != m) ? (a + m) : fmax(m, a);
-    }
-    m = block_reduce<0>(m, sh);
-    if (threadIdx.x == 0) part[blockIdx.x] = m;
+template <typename T>
+cudaError_t launch_residual(const Lay &L, const NbrOff &nb, int npt, const T *opr, const T *v, const T *f, T *r,
+                            cudaStream_t s) {
+    const Geo g = geo_rows(L.nx, (long long)L.ny * L.nz);
+    if (npt == 4) BB_CHECK_LAUNCH((launch_k(k_residual<T, 4>, g.grid, g.block, 0, s, L, nb, opr, v, f, r)));
+    else if (npt == 7) BB_CHECK_LAUNCH((launch_k(k_residual<T, 7>, g.grid, g.block, 0, s, L, nb, opr, v, f, r)));
+    else BB_CHECK_LAUNCH((launch_k(k_residual<T, 27>, g.grid, g.block, 0, s, L, nb, opr, v, f, r)));
+    return cudaSuccess;
+}
+
+template <typename T>
+cudaError_t launch_restrict(const Lay &F, const Lay &C, const T *c2f, const T *rF, T *fC, T *vC, cudaStream_t s) {
+    const Geo g = geo_rows(C.nx, (long long)C.ny * C.nz);
+    BB_CHECK_LAUNCH((launch_k(k_restrict<T>, g.grid, g.block, 0, s, F, C, c2f, rF, fC, vC)));
+    return cudaSuccess;
+}
+
+template <typename T>
+cudaError_t launch_prolong(const Lay &F, const Lay &C, const T *c2f, const T *vC, T *vF, cudaStream_t s) {
+    const Geo g = geo_rows(F.nx, (long long)F.ny * F.nz);
+    BB_CHECK_LAUNCH((launch_k(k_prolong<T>, g.grid, g.block, 0, s, F, C, c2f, vC, vF)));
+    return cudaSuccess;
+}
+
+template <typename T>
+cudaError_t launch_coarse_solve(const Lay &L, const double *LU, const int *piv, const int *pinned, const T *f, T *v,
+                                cudaStream_t s) {
+    int np = L.nx * L.ny * L.nz;
+    size_t mat = (size_t)np * np * sizeof(double), vec = (size_t)np * sizeof(double);
+    int in_smem = (mat + vec) <= kCoarseSmem;
+    size_t shm = vec + (in_smem ? mat : 0);
+    BB_CHECK_LAUNCH((launch_k(k_coarse_solve<T>, dim3(1), dim3(256), shm, s, L, LU, piv, pinned, f, v, in_smem)));
+    return cudaSuccess;
+}
+
+cudaError_t coarse_solve_prepare() {
+    cudaError_t e = cudaFuncSetAttribute(k_coarse_solve<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kCoarseSmem);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_coarse_solve<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCoarseSmem);
+}
+
+template <typename T>
+cudaError_t launch_maxabs(const Lay &L, const T *x, double *part, double *out, cudaStream_t s) {
+    const Geo g = geo_red(L);
+    BB_CHECK_LAUNCH((launch_k(k_maxabs_part<T>, g.grid, g.block, 0, s, L, x, part)));
+    BB_CHECK_LAUNCH((launch_k(k_final<0>, dim3(1), dim3(256), 0, s, (const double *)part, (int)(g.grid.x * g.grid.y), out)));
+    return cudaSuccess;
+}
+
+template <typename T>
+cudaError_t launch_dot(const Lay &L, const T *a, const T *b, double *part, double *out, cudaStream_t s) {
+    const Geo g = geo_red(L);
+    BB_CHECK_LAUNCH((launch_k(k_dot_part<T, T>, g.grid, g.block, 0, s, L, a, b, part)));
+    BB_CHECK_LAUNCH((launch_k(k_final<1>, dim3(1), dim3(256), 0, s, (const double *)part, (int)(g.grid.x * g.grid.y), out)));
+    return cudaSuccess;
+}
+
+template <typename T>
+cudaError_t launch_from_caller(const Lay &L, const double *src, int g, T *dst, cudaStream_t s) {
+    const Geo gg = geo_rows(L.nx, (long long)L.ny * L.nz);
+    BB_CHECK_LAUNCH((launch_k(k_from_caller<T>, gg.grid, gg.block, 0, s, L, src, g, dst)));
+    return cudaSuccess;
+}
+
+cudaError_t launch_to_caller(const Lay &L, const double *src, int g, double *dst, cudaStream_t s) {
+    const Geo gg = geo_rows(L.nx, (long long)L.ny * L.nz);
+    BB_CHECK_LAUNCH((launch_k(k_to_caller, gg.grid, gg.block, 0, s, L, src, g, dst)));
+    return cudaSuccess;
+}
+
+cudaError_t launch_to_f32(const double *src, float *dst, long long n, cudaStream_t s) {
+    BB_CHECK_LAUNCH((launch_k(k_to_f32, dim3(grid_for(n, 256)), dim3(256), 0, s, src, dst, n)));
+    return cudaSuccess;
+}
+
+template <typename TZ>
+cudaError_t launch_cg_rho(const Lay &L, const TZ *zz, const double *res, double *part, CgScal *sc, cudaStream_t s) {
+    const Geo g = geo_red(L);
+    BB_CHECK_LAUNCH((launch_k(k_dot_part<TZ, double>, g.grid, g.block, 0, s, L, zz, res, part)));
+    BB_CHECK_LAUNCH((launch_k(k_cg_rho, dim3(1), dim3(256), 0, s, (const double *)part, (int)(g.grid.x * g.grid.y), sc)));
+    return cudaSuccess;
+}
+
+template <typename TZ>
+cudaError_t launch_cg_pap_fused(const Lay &L, const NbrOff &nb, int npt, const double *opr, const TZ *zz,
+                                const double *pp_old, double *pp_new, double *Ap, double *part, CgScal *sc,
+                                cudaStream_t s) {
+    const Geo g = geo_red(L);
+    const CgScal *csc = sc;
+    if (npt == 4)
+        BB_CHECK_LAUNCH((launch_k(k_cg_pap_fused<TZ, 4>, g.grid, g.block, 0, s, L, nb, opr, zz, pp_old, pp_new, Ap, csc, part)));
+    else if (npt == 7)
+        BB_CHECK_LAUNCH((launch_k(k_cg_pap_fused<TZ, 7>, g.grid, g.block, 0, s, L, nb, opr, zz, pp_old, pp_new, Ap, csc, part)));
+    else
+        BB_CHECK_LAUNCH((launch_k(k_cg_pap_fused<TZ, 27>, g.grid, g.block, 0, s, L, nb, opr, zz, pp_old, pp_new, Ap, csc, part)));
+    BB_CHECK_LAUNCH((launch_k(k_cg_pap, dim3(1), dim3(256), 0, s, (const double *)part, (int)(g.grid.x * g.grid.y), sc)));
+    return cudaSuccess;
+}
+
+template <typename TV>
+cudaError_t launch_cg_xr_fused(const Lay &L, double *sol, const double *pp, double *res, const double *Ap,
+                               const CgScal *sc, float *f32, TV *vzero, double *part, double *out, cudaStream_t s) {
+    const Geo g = geo_red(L);
+    BB_CHECK_LAUNCH((launch_k(k_cg_xr_fused<TV>, g.grid, g.block, 0, s, L, sol, pp, res, Ap, sc, f32, vzero, part)));
+    BB_CHECK_LAUNCH((launch_k(k_final<0>, dim3(1), dim3(256), 0, s, (const double *)part, (int)(g.grid.x * g.grid.y), out)));
+    return cudaSuccess;
+}
+
+cudaError_t launch_round_f32(const Lay &L, const double *r, float *f, cudaStream_t s) {
+    const Geo g = geo_rows(L.nx, (long long)L.ny * L.nz);
+    BB_CHECK_LAUNCH((launch_k(k_round_f32, g.grid, g.block, 0, s, L, r, f)));
+    return cudaSuccess;
 }
 
 cudaError_t launch_defect_fused(const Lay &L, const NbrOff &nb, int npt, const double *opr, const double *x_old,
-                                const float *e, const double *b, double *x_new, float *f32, float *v32, double *part,
+                                const float *e, const double *b, double *x_new, float *f32, double *part,
                                 double *out, cudaStream_t s) {
-    if (npt == 4) launch_k(k_defect_fused<4>, kRedBlocks, 256, 0, s, L, nb, opr, x_old, e, b, x_new, f32, v32, part);
-    else if (npt == 7) launch_k(k_defect_fused<7>, kRedBlocks, 256, 0, s, L, nb, opr, x_old, e, b, x_new, f32, v32, part);
-    else launch_k(k_defect_fused<27>, kRedBlocks, 256, 0, s, L, nb, opr, x_old, e, b, x_new, f32, v32, part);
-    BB_CHECK_LAUNCH();
-    launch_k(k_final<0>, 1, 256, 0, s, part, kRedBlocks, out);
-    BB_CHECK_LAUNCH();
+    const Geo g = geo_red(L);
+    if (npt == 4)
+        BB_CHECK_LAUNCH((launch_k(k_defect_fused<4>, g.grid, g.block, 0, s, L, nb, opr, x_old, e, b, x_new, f32, part)));
+    else if (npt == 7)
+        BB_CHECK_LAUNCH((launch_k(k_defect_fused<7>, g.grid, g.block, 0, s, L, nb, opr, x_old, e, b, x_new, f32, part)));
+    else
+        BB_CHECK_LAUNCH((launch_k(k_defect_fused<27>, g.grid, g.block, 0, s, L, nb, opr, x_old, e, b, x_new, f32, part)));
+    BB_CHECK_LAUNCH((launch_k(k_final<0>, dim3(1), dim3(256), 0, s, (const double *)part, (int)(g.grid.x * g.grid.y), out)));
     return cudaSuccess;
 }
+
 #define BB_INST(T)                                                                                                   \
     template cudaError_t launch_relax<T>(const Lay &, const NbrOff &, int, bool, const T *, T *, const T *, int,     \
                                          cudaStream_t);                                                              \
+    template cudaError_t launch_relax_sweeps<T>(const Lay &, const NbrOff &, int, bool, const T *, T *, const T *,   \
+                                                int, int, cudaStream_t);                                             \
     template cudaError_t launch_residual<T>(const Lay &, const NbrOff &, int, const T *, const T *, const T *, T *,  \
                                             cudaStream_t);                                                           \
     template cudaError_t launch_restrict<T>(const Lay &, const Lay &, const T *, const T *, T *, T *, cudaStream_t); \
@@ -854,7 +904,13 @@ cudaError_t launch_defect_fused(const Lay &L, const NbrOff &nb, int npt, const d
                                                 T *, cudaStream_t);                                                  \
     template cudaError_t launch_maxabs<T>(const Lay &, const T *, double *, double *, cudaStream_t);                \
     template cudaError_t launch_dot<T>(const Lay &, const T *, const T *, double *, double *, cudaStream_t);        \
-    template cudaError_t launch_from_caller<T>(const Lay &, const double *, int, T *, cudaStream_t);
+    template cudaError_t launch_from_caller<T>(const Lay &, const double *, int, T *, cudaStream_t);                 \
+    template cudaError_t launch_cg_rho<T>(const Lay &, const T *, const double *, double *, CgScal *, cudaStream_t); \
+    template cudaError_t launch_cg_pap_fused<T>(const Lay &, const NbrOff &, int, const double *, const T *,         \
+                                                const double *, double *, double *, double *, CgScal *,             \
+                                                cudaStream_t);                                                       \
+    template cudaError_t launch_cg_xr_fused<T>(const Lay &, double *, const double *, double *, const double *,      \
+                                               const CgScal *, float *, T *, double *, double *, cudaStream_t);
 BB_INST(double)
 BB_INST(float)
 
