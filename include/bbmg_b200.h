@@ -115,7 +115,21 @@ int bbmg_solve(bbmg_handle *h, const double *rhs, double *sol, int *it, double *
 /* Change maxit / rcvg between solves (the linsol fields). */
 int bbmg_set_convergence(bbmg_handle *h, int maxit, double rcvg);
 
-/* Run on the given cudaStream_t (default: a stream the handle creates). */
+/* Denominator of rerr.  BBMG_NORM_GUESS (default) is the reference's
+ * max|r0| of the given initial guess (bbmg_class.f90:627-628), under which a
+ * better guess cannot save iterations.  BBMG_NORM_RHS uses max|rhs|, the
+ * residual a zero guess starts from: a solve from a predicted or warm-start
+ * guess then stops at the same max|b - A x| as the zero-guess solve NGA2's
+ * callers make (its zero-guess result is identical under both).  With a zero
+ * rhs the solve falls back to max|r0|. */
+#define BBMG_NORM_GUESS 0
+#define BBMG_NORM_RHS   1
+int bbmg_set_residual_norm(bbmg_handle *h, int norm);
+
+/* Run on the given cudaStream_t.  The default is a stream the handle
+ * creates that synchronises with the legacy default stream, so device arrays
+ * written there before a call are complete when the call reads them; with any
+ * other producer stream, pass it here (or synchronise before the call). */
 int bbmg_set_stream(bbmg_handle *h, void *stream);
 
 int bbmg_get_info(const bbmg_handle *h, bbmg_info *info);

@@ -25,11 +25,13 @@ LIB_PATH = os.path.join(HERE, "libbbmg_b200.so")
 
 BBOX, PCG_BBOX = 1, 2
 FP64, MIXED = 0, 1
+NORM_GUESS, NORM_RHS = 0, 1
 STATUS = {0: "OK", 1: "MAXIT", 2: "STAGNATION", 3: "NONFINITE", 4: "BAD_ARGS", 5: "NOT_SETUP",
           6: "CUDA", 7: "NO_MEMORY"}
 ARR = {"opr": 0, "c2f": 1, "f2c": 2, "oprc2f": 3, "v": 4, "f": 5, "r": 6}
 STEP = {"relax": 0, "residual": 1, "restrict": 2, "prolong": 3, "cycle": 4, "direct": 5}
 EXPORTS = ["bbmg_default_params", "bbmg_create", "bbmg_setup", "bbmg_solve", "bbmg_set_convergence",
+           "bbmg_set_residual_norm",
            "bbmg_set_stream", "bbmg_get_info", "bbmg_destroy", "bbmg_last_error", "bbmg_debug_get",
            "bbmg_debug_put", "bbmg_debug_step", "bbmg_debug_direct", "bbmg_profile_step",
            "bbmg_residual_norm_noalloc"]
@@ -78,6 +80,7 @@ def load(path: str = LIB_PATH):
     lib.bbmg_setup.argtypes = [P, I, C.POINTER(C.c_int), P]
     lib.bbmg_solve.argtypes = [P, P, P, C.POINTER(C.c_int), C.POINTER(C.c_double)]
     lib.bbmg_set_convergence.argtypes = [P, I, D]
+    lib.bbmg_set_residual_norm.argtypes = [P, I]
     lib.bbmg_set_stream.argtypes = [P, P]
     lib.bbmg_get_info.argtypes = [P, C.POINTER(Info)]
     lib.bbmg_destroy.argtypes = [P]
@@ -183,6 +186,10 @@ class BBMG:
 
     def set_convergence(self, maxit, rcvg):
         self._check(self.lib.bbmg_set_convergence(self.h, maxit, rcvg))
+
+    def set_residual_norm(self, norm):
+        """NORM_GUESS (the reference's rerr) or NORM_RHS (rerr = max|r| / max|rhs|)."""
+        self._check(self.lib.bbmg_set_residual_norm(self.h, norm))
 
     def set_stream(self, stream_ptr):
         self._check(self.lib.bbmg_set_stream(self.h, C.c_void_p(stream_ptr)))

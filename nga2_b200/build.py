@@ -13,8 +13,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libbbmg_b200.so")
-SOURCES = ["api.cu", "setup.cu", "solve.cu", "noalloc.cu"]
-HEADERS = ["common.cuh", "layout.cuh", "setup.cuh", "../../include/bbmg_b200.h"]
+SOURCES = ["api.cu", "setup.cu", "solve.cu", "noalloc.cu", "unet.cu"]
+HEADERS = ["common.cuh", "layout.cuh", "setup.cuh", "../../include/bbmg_b200.h", "../../include/bbmg_learned.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

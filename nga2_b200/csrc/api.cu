@@ -59,6 +59,7 @@ template <> struct LvlPtr<float> {
 struct bbmg_handle {
     bbmg_grid grid{};
     bbmg_params prm{};
+    int res_norm = BBMG_NORM_GUESS;
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -350,7 +351,10 @@ int bbmg_create(const bbmg_grid *grid, const bbmg_params *params, bbmg_handle **
         bbmg_destroy(h);
         return code;
     };
-    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(fail(h, BBMG_CUDA, "stream"));
+    // a blocking stream: it waits for work the caller queued on the legacy
+    // default stream (and the reverse), so device arrays a caller has just
+    // written there are complete when setup/solve read them
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamDefault) != cudaSuccess) return bail(fail(h, BBMG_CUDA, "stream"));
     h->own_stream = true;
     if (coarse_solve_prepare() != cudaSuccess) return bail(fail(h, BBMG_CUDA, "coarse solve attributes"));
 
@@ -434,6 +438,7 @@ int bbmg_create(const bbmg_grid *grid, const bbmg_params *params, bbmg_handle **
 
 int bbmg_set_stream(bbmg_handle *h, void *stream) {
     if (!h) return BBMG_BAD_ARGS;
+    if (!h->own_stream && h->stream == (cudaStream_t)stream) return BBMG_OK;  // graphs stay valid
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
@@ -447,6 +452,13 @@ int bbmg_set_convergence(bbmg_handle *h, int maxit, double rcvg) {
     if (!h || maxit < 0) return BBMG_BAD_ARGS;
     h->prm.maxit = maxit;
     h->prm.rcvg = rcvg;
+    return BBMG_OK;
+}
+
+int bbmg_set_residual_norm(bbmg_handle *h, int norm) {
+    if (!h) return BBMG_BAD_ARGS;
+    if (norm != BBMG_NORM_GUESS && norm != BBMG_NORM_RHS) return fail(h, BBMG_BAD_ARGS, "unknown norm %d", norm);
+    h->res_norm = norm;
     return BBMG_OK;
 }
 
@@ -621,13 +633,19 @@ int bbmg_solve(bbmg_handle *h, const double *rhs, double *sol, int *it_out, doub
     // initial residual (bbmg_class.f90:626-628)
     CU(h, launch_residual<double>(L, l1.nb, l1.npt, l1.oprS, l1.v, l1.f, l1.r, s));
     CU(h, launch_maxabs<double>(L, l1.r, h->part, h->dscal, s));
-    CU(h, cudaMemcpyAsync(h->h_scal, h->dscal, sizeof(double), cudaMemcpyDeviceToHost, s));
+    const bool by_rhs = h->res_norm == BBMG_NORM_RHS;
+    if (by_rhs) CU(h, launch_maxabs<double>(L, l1.f, h->part, h->dscal + 3, s));
+    CU(h, cudaMemcpyAsync(h->h_scal, h->dscal, sizeof(double) * 4, cudaMemcpyDeviceToHost, s));
     double res0 = 0.0;
     int st = sync_read(h, &res0, 0);
     if (st) return st;
+    // denominator of rerr: the guess's own initial residual (the reference's
+    // definition), or max|rhs|, the residual a zero guess would start from
+    double rnorm = res0;
+    if (by_rhs && h->h_scal[3] > 0.0) rnorm = h->h_scal[3];
     int status = BBMG_OK;
     double *xout = l1.v;
-    long long launches = 4;  // two copies-in, residual, max (two)
+    long long launches = by_rhs ? 6 : 4;  // two copies-in, residual, max (two) [, max of rhs (two)]
     if (res0 == 0.0) {
         it = 0;
         rerr = 0.0;
@@ -671,7 +689,7 @@ int bbmg_solve(bbmg_handle *h, const double *rhs, double *sol, int *it_out, doub
             launches += h->gkernels[mode][par];
             double mr = 0.0;
             if ((st = sync_read(h, &mr, 1))) return st;
-            rerr = mr / res0;  // bbmg_class.f90:696,723
+            rerr = mr / rnorm;  // bbmg_class.f90:696,723 (rnorm = res0 there)
             it = n;
             if (!(rerr == rerr) || std::isinf(rerr)) {
                 status = fail(h, BBMG_NONFINITE, "residual became non-finite at iteration %d", n);

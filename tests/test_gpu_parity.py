@@ -229,3 +229,27 @@ def test_periodic_64_known_answer(method, precision):
     assert st == 0 and rerr <= 1e-10
     err = np.abs(P.remove_mean(x) - exact).max() / np.abs(exact).max()
     assert err < 1e-8, err
+
+
+@pytest.mark.parametrize("precision", [FP64, MIXED])
+@pytest.mark.parametrize("method", [BBOX, PCG_BBOX])
+def test_residual_norm_rhs(method, precision):
+    """NORM_RHS: a zero-guess solve is unchanged (max|r0| = max|b|); a guess
+    near the solution stops as soon as max|r| <= rcvg max|b|, where the
+    reference's rerr (relative to the guess's own residual) keeps iterating."""
+    from nga2_b200.bbmg import NORM_GUESS, NORM_RHS
+    pb = P.drops_poisson(24, seed=2, ndrops=4, rmin=2.0, rmax=4.0)
+    g = BBMG(24, 24, 24, True, False, True, method=method, precision=precision, rcvg=1e-10)
+    g.setup(pb.stc, pb.opr)
+    x0, it0, rerr0, st0 = g.solve(pb.rhs)
+    g.set_residual_norm(NORM_RHS)
+    x1, it1, rerr1, st1 = g.solve(pb.rhs)
+    assert (it1, st1) == (it0, st0) and rerr1 == rerr0 and np.array_equal(x0, x1)
+    # warm start: the zero-guess solution with a 1e-6 relative perturbation
+    rng = np.random.default_rng(0)
+    guess = x0 + 1e-6 * np.abs(x0).max() * rng.standard_normal(x0.shape)
+    _, it_rhs, rerr_rhs, st_rhs = g.solve(pb.rhs, guess.copy())
+    g.set_residual_norm(NORM_GUESS)
+    _, it_ref, rerr_ref, st_ref = g.solve(pb.rhs, guess.copy())
+    assert st_rhs == 0 and st_ref == 0 and rerr_rhs <= 1e-10
+    assert it_rhs < it_ref and it_rhs < it0, (it_rhs, it_ref, it0)
