@@ -61,10 +61,12 @@ int nn_up2(const nn_act *x, const nn_act *y, void *stream);
 int nn_up2_bwd(const nn_act *dy, const nn_act *dx, void *stream);
 
 /* Input embedding: channel i = scales[i] * fields[i] for i < nf, the other
- * channels 0, from nf (<= NN_MAX_FIELDS) FP64 fields of n*d*h*w values (w
- * fastest).  fields and scales are host arrays; the fields are device memory. */
+ * channels 0, from nf (<= NN_MAX_FIELDS) FP64 fields (w fastest).  With
+ * pool = 1 the fields have x's n*d*h*w values; with pool = 2 they live on the
+ * grid twice as fine (n, 2d, 2h, 2w) and are averaged over 2x2x2 children.
+ * fields and scales are host arrays; the fields are device memory. */
 #define NN_MAX_FIELDS 4
-int nn_embed(int nf, const double *const *fields, const double *scales, const nn_act *x, void *stream);
+int nn_embed(int nf, const double *const *fields, const double *scales, int pool, const nn_act *x, void *stream);
 
 /* 1x1x1 head: out[v] = b + sum_c x(v,c) w[c] (FP32 out).  Backward: dx(v,c) =
  * dout[v] w[c] (BF16), dw[c] += sum_v dout[v] x(v,c), db += sum_v dout[v]. */

@@ -67,6 +67,14 @@ struct bbmg_handle {
     std::vector<Level> lv;  // 1-based: lv[0] unused
     // coarsest dense problem
     int np = 0, lu_info = 0, npinned = 0;
+    // coarse tail of the V-cycle in one cooperative launch from level tail_n0
+    // (0: every level runs pass by pass)
+    int tail_n0 = 0;
+    bool tail_off = false;        // cooperative capture unavailable: pass by pass
+    TailBar *tbar = nullptr;
+    int tail_blocks[2] = {0, 0};  // grid per precision (0 = not sized yet)
+    size_t tail_smem_b = 0;
+    int tail_mat_in_smem = 0;
     double *OP = nullptr, *LU = nullptr;
     int *piv = nullptr, *pinned = nullptr, *d_info = nullptr, *d_flag = nullptr;
     // Krylov / outer iteration vectors (level-1 layout)
@@ -161,10 +169,53 @@ void drop_graphs(bbmg_handle *h) {
 
 // ---------------------------------------------------------------------------
 // V-cycle (bbmg_class.f90:732-776), recursive over levels
+template <typename T> struct PrecIdx { static constexpr int value = sizeof(T) == 8 ? 0 : 1; };
+
+// cycle(n) for n >= tail_n0 as one cooperative launch; returns BBMG_NOT_SETUP
+// (nothing launched) when the levels do not qualify
+template <typename T>
+int vcycle_tail(bbmg_handle *h, int n) {
+    using P = LvlPtr<T>;
+    TailArgs<T> A{};
+    A.n = h->nlvl - n + 1;
+    if (A.n > kTailMax || A.n < 2) return BBMG_NOT_SETUP;
+    for (int m = n; m <= h->nlvl; m++) {
+        Level &l = h->lv[m];
+        if (l.npt != 27 || !l.fuse) return BBMG_NOT_SETUP;
+        TailLvl<T> &t = A.lv[m - n];
+        t.L = l.L;
+        for (int q = 0; q < 27; q++) {
+            t.off[0].o[q] = l.nb.off[0][q];
+            t.off[1].o[q] = l.nb.off[1][q];
+        }
+        t.opr = P::opr(l);
+        t.v = P::v(l);
+        t.f = P::f(l);
+        t.r = P::r(l);
+        t.c2f = m < h->nlvl ? P::c2f(l) : nullptr;
+        t.bar = h->tbar;
+    }
+    A.pre = h->prm.relax_pre;
+    A.post = h->prm.relax_post;
+    A.direct = h->prm.use_direct_solve;
+    A.mat_in_smem = h->tail_mat_in_smem;
+    A.LU = h->LU;
+    A.piv = h->piv;
+    A.pinned = h->pinned;
+    int &blocks = h->tail_blocks[PrecIdx<T>::value];
+    if (!blocks) CU(h, tail_grid<T>(h->tail_smem_b, &blocks));
+    CU(h, launch_vtail<T>(A, blocks, h->tail_smem_b, h->stream));
+    return BBMG_OK;
+}
+
 template <typename T>
 int vcycle(bbmg_handle *h, int n) {
     using P = LvlPtr<T>;
     cudaStream_t s = h->stream;
+    if (n == h->tail_n0 && !h->tail_off && h->prm.ncycle == 1) {
+        int st = vcycle_tail<T>(h, n);
+        if (st != BBMG_NOT_SETUP) return st;
+    }
     Level &l = h->lv[n];
     if (n == h->nlvl) {
         if (h->prm.use_direct_solve) {
@@ -239,6 +290,18 @@ int get_graph(bbmg_handle *h, int mode, int par, cudaGraphExec_t *out) {
     CU(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     int st = record_iteration(h, mode, par);
     cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    if ((st || e != cudaSuccess) && h->tail_n0 && !h->tail_off) {
+        // a cooperative launch that cannot be captured here: record the
+        // coarse levels pass by pass instead
+        if (g) cudaGraphDestroy(g);
+        g = nullptr;
+        cudaGetLastError();
+        h->tail_off = true;
+        drop_graphs(h);
+        CU(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        st = record_iteration(h, mode, par);
+        e = cudaStreamEndCapture(h->stream, &g);
+    }
     if (st) {
         if (g) cudaGraphDestroy(g);
         return st;
@@ -302,6 +365,7 @@ int bbmg_destroy(bbmg_handle *h) {
     }
     dfree(h->OP); dfree(h->LU); dfree(h->piv); dfree(h->pinned); dfree(h->d_info); dfree(h->d_flag);
     dfree(h->sol); dfree(h->pp); dfree(h->pp2); dfree(h->Ap); dfree(h->x2); dfree(h->sc); dfree(h->part); dfree(h->dscal);
+    dfree(h->tbar);
     dfree(h->d_opr_in); dfree(h->d_stc); dfree(h->d_io);
     if (h->h_scal) cudaFreeHost(h->h_scal);
     if (h->ev0) cudaEventDestroy(h->ev0);
@@ -419,6 +483,25 @@ int bbmg_create(const bbmg_grid *grid, const bbmg_params *params, bbmg_handle **
         if ((st = dalloc(h, &h->sol, (size_t)L1.plane)) || (st = dalloc(h, &h->pp, (size_t)L1.plane)) ||
             (st = dalloc(h, &h->pp2, (size_t)L1.plane)) || (st = dalloc(h, &h->Ap, (size_t)L1.plane)))
             return bail(st);
+    }
+    {
+        // the coarse tail: the first level >= 2 at or below tail_cells cells
+        // from which every level can be fused (27-point, periodic sizes even)
+        long long tail_cells = 1LL << 21;
+        if (const char *env = getenv("BBMG_TAIL_CELLS")) tail_cells = atoll(env);
+        for (int n = 2; prm.ncycle == 1 && tail_cells > 0 && n < h->nlvl; n++) {
+            const Lay &L = h->lv[n].L;
+            if ((long long)L.nx * L.ny * L.nz > tail_cells || h->nlvl - n + 1 > kTailMax) continue;
+            bool ok = true;
+            for (int m = n; m <= h->nlvl; m++) ok = ok && h->lv[m].fuse;
+            if (ok) { h->tail_n0 = n; break; }
+        }
+        if (h->tail_n0) {
+            unsigned *tb = nullptr;
+            if ((st = dalloc(h, &tb, 4))) return bail(st);
+            h->tbar = reinterpret_cast<TailBar *>(tb);
+            h->tail_smem_b = tail_smem(h->np, &h->tail_mat_in_smem);
+        }
     }
     if (cudaMallocHost((void **)&h->h_scal, 8 * sizeof(double)) != cudaSuccess) return bail(fail(h, BBMG_NO_MEMORY, "pinned host"));
     if (cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess)
@@ -614,6 +697,7 @@ int bbmg_solve(bbmg_handle *h, const double *rhs, double *sol, int *it_out, doub
     int it = -1;
     double rerr = HUGE_VAL;
     CU(h, cudaEventRecord(h->ev0, s));
+    if (h->tbar) CU(h, cudaMemsetAsync(&h->tbar->err, 0, sizeof(unsigned), s));
     // rhs/initial guess into the level-1 arrays; overlap zero, then periodic
     // images (bbmg_class.f90:611-624; ils_class.f90:693-700)
     CU(h, cudaMemsetAsync(l1.f, 0, sizeof(double) * L.plane, s));
@@ -709,6 +793,13 @@ int bbmg_solve(bbmg_handle *h, const double *rhs, double *sol, int *it_out, doub
             prev = rerr;
         }
         if (status == BBMG_OK && rerr > h->prm.rcvg) status = BBMG_MAXIT;
+        if (h->tbar) {
+            unsigned terr = 0;
+            CU(h, cudaMemcpyAsync(h->h_scal + 5, &h->tbar->err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+            CU(h, cudaStreamSynchronize(s));
+            memcpy(&terr, h->h_scal + 5, sizeof(unsigned));
+            if (terr) status = fail(h, BBMG_CUDA, "a grid barrier of the coarse-level kernel timed out");
+        }
     }
     // solution out (ils_class.f90:782-788)
     if (sol_dev) {

@@ -40,6 +40,42 @@ template <typename T>
 cudaError_t launch_coarse_solve(const Lay &L, const double *LU, const int *piv, const int *pinned, const T *f, T *v,
                                 cudaStream_t s);
 
+// the coarse tail of the V-cycle in one cooperative launch (levels n0..nlvl,
+// 27-point operators, V-cycle only)
+struct Off27 {
+    int o[27];
+};
+struct TailBar {
+    unsigned count, gen;  // grid barrier state, zeroed before every launch
+    unsigned err;         // set when a barrier wait runs out; cleared by the host
+};
+template <typename T>
+struct TailLvl {
+    Lay L;
+    Off27 off[2];          // neighbour offsets for even / odd x
+    const T *opr;          // 27 coefficient planes
+    T *v, *f, *r;
+    const T *c2f;          // prolongation weights of this level (to the next coarser one)
+    TailBar *bar;
+};
+constexpr int kTailMax = 8;            // levels in one launch (kernel parameters stay under 4 KB)
+constexpr int kTailThreads = 512;
+constexpr int kTailBlocksPerSm = 1;
+constexpr unsigned kTailSpinLimit = 1u << 24;  // polls of 64 ns naps: about a second
+constexpr size_t kTailSmemMax = 100 * 1024;
+template <typename T>
+struct TailArgs {
+    TailLvl<T> lv[kTailMax];
+    int n;                 // levels in lv; lv[n-1] is the coarsest
+    int pre, post, direct, mat_in_smem;
+    const double *LU;
+    const int *piv, *pinned;
+};
+size_t tail_smem(int np, int *mat_in_smem);
+template <typename T>
+cudaError_t tail_grid(size_t smem, int *blocks);
+template <typename T>
+cudaError_t launch_vtail(const TailArgs<T> &A, int blocks, size_t smem, cudaStream_t s);
 // reductions (deterministic two-pass) into a device double
 constexpr int kRedBlocks = 1184;  // 8 blocks of 256 threads per SM on 148 SMs
 template <typename T>

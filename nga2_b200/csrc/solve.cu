@@ -18,10 +18,6 @@
 
 namespace bbmg {
 
-struct Off27 {
-    int o[27];
-};
-
 static Off27 off_for(const NbrOff &nb, int par) {
     Off27 r;
     for (int q = 0; q < 27; q++) r.o[q] = nb.off[par][q];
@@ -241,29 +237,33 @@ __global__ void __launch_bounds__(256) k_relax_phase7(Lay L, const T *__restrict
 // written (bbmg_class.f90:831-844).  With f == nullptr the kernel returns the
 // operator product itself.
 template <typename T, int NPT>
+__device__ __forceinline__ void residual_point(const Lay &L, const int *__restrict__ off0,
+                                               const int *__restrict__ off1, const T *__restrict__ opr,
+                                               const T *__restrict__ v, const T *__restrict__ f,
+                                               T *__restrict__ r, int i, int j, int k) {
+    using O = Ops<T, ExactOf<T>::value>;
+    const int par = i & 1;
+    const long long id = L.idx(i, j, k);
+    T s = T(0);
+#pragma unroll
+    for (int q = 0; q < Lay7<NPT>::terms; q++) {
+        const int q27i = Lay7<NPT>::slot(q);
+        const int o = par ? off1[q27i] : off0[q27i];
+        s = O::mac(s, opr[(long long)Lay7<NPT>::plane(q) * L.plane + id + (Lay7<NPT>::at_nbr(q) ? o : 0)], v[id + o]);
+    }
+    const T val = f ? O::sub(f[id], s) : s;
+    r[id] = val;
+    if (on_periodic_face(L, i, j, k)) write_images(L, r, i, j, k, val);
+}
+
+template <typename T, int NPT>
 __global__ void __launch_bounds__(256) k_residual(Lay L, NbrOff nb, const T *__restrict__ opr,
                                                    const T *__restrict__ v, const T *__restrict__ f,
                                                    T *__restrict__ r) {
     pdl_entry();
-    using O = Ops<T, ExactOf<T>::value>;
     FOR_ROWS(L.ny * L.nz) {
         const int j = row % L.ny, k = row / L.ny;
-        FOR_CHUNKS(L.nx) {
-            const int i = x_of(L, ch);
-            const int par = i & 1;
-            const long long id = L.idx(i, j, k);
-            T s = T(0);
-#pragma unroll
-            for (int q = 0; q < Lay7<NPT>::terms; q++) {
-                const int q27i = Lay7<NPT>::slot(q);
-                const int o = par ? nb.off[1][q27i] : nb.off[0][q27i];
-                s = O::mac(s, opr[(long long)Lay7<NPT>::plane(q) * L.plane + id + (Lay7<NPT>::at_nbr(q) ? o : 0)],
-                           v[id + o]);
-            }
-            const T val = f ? O::sub(f[id], s) : s;
-            r[id] = val;
-            if (on_periodic_face(L, i, j, k)) write_images(L, r, i, j, k, val);
-        }
+        FOR_CHUNKS(L.nx) residual_point<T, NPT>(L, nb.off[0], nb.off[1], opr, v, f, r, x_of(L, ch), j, k);
     }
 }
 
@@ -272,36 +272,38 @@ __global__ void __launch_bounds__(256) k_residual(Lay L, NbrOff nb, const T *__r
 // fine prolongation weights.  Also zeroes the coarse correction v_c, the first
 // statement of cycle(n+1) (bbmg_class.f90:739).
 template <typename T>
+__device__ __forceinline__ void restrict_point(const Lay &F, const Lay &C, const T *__restrict__ c2f,
+                                               const T *__restrict__ rF, T *__restrict__ fC, T *__restrict__ vC,
+                                               int ci, int cj, int ck) {
+    using O = Ops<T, ExactOf<T>::value>;
+    const int fi = 2 * ci, fj = 2 * cj, fk = 2 * ck;
+    const int rk0 = -pmod(F.zper, fk - 1, F.nz), rk1 = pmod(F.zper, fk + 1, F.nz);
+    const int rj0 = -pmod(F.yper, fj - 1, F.ny), rj1 = pmod(F.yper, fj + 1, F.ny);
+    const int ri0 = -pmod(F.xper, fi - 1, F.nx), ri1 = pmod(F.xper, fi + 1, F.nx);
+    T s = T(0);
+    for (int rk = rk0; rk <= rk1; rk++)
+        for (int rj = rj0; rj <= rj1; rj++)
+            for (int ri = ri0; ri <= ri1; ri++) {
+                const long long fid = F.idx(fi + ri, fj + rj, fk + rk);
+                s = O::mac(s, c2f[(long long)q8((1 - ri) / 2, (1 - rj) / 2, (1 - rk) / 2) * F.plane + fid], rF[fid]);
+            }
+    const long long cid = C.idx(ci, cj, ck);
+    fC[cid] = s;
+    vC[cid] = T(0);
+    if (on_periodic_face(C, ci, cj, ck)) {
+        write_images(C, fC, ci, cj, ck, s);
+        write_images(C, vC, ci, cj, ck, T(0));
+    }
+}
+
+template <typename T>
 __global__ void __launch_bounds__(256) k_restrict(Lay F, Lay C, const T *__restrict__ c2f,
                                                    const T *__restrict__ rF, T *__restrict__ fC,
                                                    T *__restrict__ vC) {
     pdl_entry();
-    using O = Ops<T, ExactOf<T>::value>;
     FOR_ROWS(C.ny * C.nz) {
         const int cj = row % C.ny, ck = row / C.ny;
-        const int fj = 2 * cj, fk = 2 * ck;
-        const int rk0 = -pmod(F.zper, fk - 1, F.nz), rk1 = pmod(F.zper, fk + 1, F.nz);
-        const int rj0 = -pmod(F.yper, fj - 1, F.ny), rj1 = pmod(F.yper, fj + 1, F.ny);
-        FOR_CHUNKS(C.nx) {
-            const int ci = x_of(C, ch);
-            const int fi = 2 * ci;
-            const int ri0 = -pmod(F.xper, fi - 1, F.nx), ri1 = pmod(F.xper, fi + 1, F.nx);
-            T s = T(0);
-            for (int rk = rk0; rk <= rk1; rk++)
-                for (int rj = rj0; rj <= rj1; rj++)
-                    for (int ri = ri0; ri <= ri1; ri++) {
-                        const long long fid = F.idx(fi + ri, fj + rj, fk + rk);
-                        s = O::mac(s, c2f[(long long)q8((1 - ri) / 2, (1 - rj) / 2, (1 - rk) / 2) * F.plane + fid],
-                                   rF[fid]);
-                    }
-            const long long cid = C.idx(ci, cj, ck);
-            fC[cid] = s;
-            vC[cid] = T(0);
-            if (on_periodic_face(C, ci, cj, ck)) {
-                write_images(C, fC, ci, cj, ck, s);
-                write_images(C, vC, ci, cj, ck, T(0));
-            }
-        }
+        FOR_CHUNKS(C.nx) restrict_point<T>(F, C, c2f, rF, fC, vC, x_of(C, ch), cj, ck);
     }
 }
 
@@ -309,27 +311,28 @@ __global__ void __launch_bounds__(256) k_restrict(Lay F, Lay C, const T *__restr
 // (bbmg_class.f90:779-801 then 770).  A fine point of parity class
 // (n1,n2,n3) only carries weights p_d <= n_d.
 template <typename T>
+__device__ __forceinline__ void prolong_point(const Lay &F, const Lay &C, const T *__restrict__ c2f,
+                                              const T *__restrict__ vC, T *__restrict__ vF, int i, int j, int k) {
+    using O = Ops<T, ExactOf<T>::value>;
+    const int n1 = i & 1, n2 = j & 1, n3 = k & 1, ci = i >> 1, cj = j >> 1, ck = k >> 1;
+    const long long id = F.idx(i, j, k);
+    T e = T(0);
+    for (int pk = 0; pk <= n3; pk++)
+        for (int pj = 0; pj <= n2; pj++)
+            for (int pi = 0; pi <= n1; pi++)
+                e = O::mac(e, c2f[(long long)q8(pi, pj, pk) * F.plane + id], vC[C.idx(ci + pi, cj + pj, ck + pk)]);
+    const T val = O::add(vF[id], e);
+    vF[id] = val;
+    if (on_periodic_face(F, i, j, k)) write_images(F, vF, i, j, k, val);
+}
+
+template <typename T>
 __global__ void __launch_bounds__(256) k_prolong(Lay F, Lay C, const T *__restrict__ c2f,
                                                   const T *__restrict__ vC, T *__restrict__ vF) {
     pdl_entry();
-    using O = Ops<T, ExactOf<T>::value>;
     FOR_ROWS(F.ny * F.nz) {
         const int j = row % F.ny, k = row / F.ny;
-        const int n2 = j & 1, n3 = k & 1, cj = j >> 1, ck = k >> 1;
-        FOR_CHUNKS(F.nx) {
-            const int i = x_of(F, ch);
-            const int n1 = i & 1, ci = i >> 1;
-            const long long id = F.idx(i, j, k);
-            T e = T(0);
-            for (int pk = 0; pk <= n3; pk++)
-                for (int pj = 0; pj <= n2; pj++)
-                    for (int pi = 0; pi <= n1; pi++)
-                        e = O::mac(e, c2f[(long long)q8(pi, pj, pk) * F.plane + id],
-                                   vC[C.idx(ci + pi, cj + pj, ck + pk)]);
-            const T val = O::add(vF[id], e);
-            vF[id] = val;
-            if (on_periodic_face(F, i, j, k)) write_images(F, vF, i, j, k, val);
-        }
+        FOR_CHUNKS(F.nx) prolong_point<T>(F, C, c2f, vC, vF, x_of(F, ch), j, k);
     }
 }
 
@@ -338,11 +341,10 @@ __global__ void __launch_bounds__(256) k_prolong(Lay F, Lay C, const T *__restri
 // triangular solves run on one warp with the factors in shared memory when
 // they fit.
 template <typename T>
-__global__ void k_coarse_solve(Lay L, const double *__restrict__ LU, const int *__restrict__ piv,
-                               const int *__restrict__ pinned, const T *__restrict__ f, T *__restrict__ v,
-                               int mat_in_smem) {
-    pdl_entry();
-    extern __shared__ double sm[];
+__device__ __forceinline__ void coarse_solve_block(const Lay &L, const double *__restrict__ LU,
+                                                   const int *__restrict__ piv, const int *__restrict__ pinned,
+                                                   const T *__restrict__ f, T *__restrict__ v, int mat_in_smem,
+                                                   double *sm) {
     const int np = L.nx * L.ny * L.nz;
     double *x = sm;
     const double *A = mat_in_smem ? sm + np : LU;
@@ -392,6 +394,15 @@ __global__ void k_coarse_solve(Lay L, const double *__restrict__ LU, const int *
         v[L.idx(i, j, k)] = val;
         if (on_periodic_face(L, i, j, k)) write_images(L, v, i, j, k, val);
     }
+}
+
+template <typename T>
+__global__ void k_coarse_solve(Lay L, const double *__restrict__ LU, const int *__restrict__ piv,
+                               const int *__restrict__ pinned, const T *__restrict__ f, T *__restrict__ v,
+                               int mat_in_smem) {
+    pdl_entry();
+    extern __shared__ double sm[];
+    coarse_solve_block<T>(L, LU, piv, pinned, f, v, mat_in_smem, sm);
 }
 
 // ---------------------------------------------------------------------------
@@ -890,6 +901,176 @@ cudaError_t launch_defect_fused(const Lay &L, const NbrOff &nb, int npt, const d
     BB_CHECK_LAUNCH((launch_k(k_final<0>, dim3(1), dim3(256), 0, s, (const double *)part, (int)(g.grid.x * g.grid.y), out)));
     return cudaSuccess;
 }
+
+// ---------------------------------------------------------------------------
+// The coarse tail of the V-cycle in one launch.  Below a few million cells a
+// level's colour passes, residual, restriction and prolongation each take a
+// few microseconds of work but a full kernel launch; this persistent kernel
+// runs cycle(n0) (bbmg_class.f90:732-776) for every level n0..nlvl with one
+// grid barrier between dependent passes instead.  Each pass calls the same
+// per-point functions as the single-pass kernels, so the FP64 result is
+// bit-identical.  The launch is cooperative (every block resident), and every
+// barrier wait is bounded: a wait that runs out sets the error flag and the
+// kernel returns, so a fault can never hang the GPU.
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned *p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned atom_add_acq_rel_u32(unsigned *p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
+// Sense-free generation barrier over all blocks of the grid.  Returns false
+// (and raises bar->err) if a wait exceeded kTailSpinLimit polls (about a
+// second); callers then return without touching memory again.
+__device__ bool tail_sync(TailBar *bar) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        if (ld_acquire_u32(&bar->err)) {
+            ok = 0;
+        } else {
+            const unsigned g = ld_acquire_u32(&bar->gen);
+            if (atom_add_acq_rel_u32(&bar->count, 1u) == gridDim.x - 1) {
+                bar->count = 0;  // ordered before the release of the next generation
+                st_release_u32(&bar->gen, g + 1u);
+            } else {
+                unsigned spins = 0;
+                while (ld_acquire_u32(&bar->gen) == g) {
+                    if (++spins > kTailSpinLimit) {
+                        atomicExch(&bar->err, 1u);
+                        ok = 0;
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+template <typename T>
+__device__ bool tail_relax(const TailLvl<T> &l, int dir, bool &go) {
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    for (int c = 0; c < 8; c++) {
+        const int col = dir > 0 ? c : 7 - c;  // colours 1..8 forward, 8..1 backward
+        const int px = col & 1, py = (col >> 1) & 1, pz = (col >> 2) & 1;
+        const Lay &L = l.L;
+        const int na = (L.nx - px + 1) >> 1, nb = (L.ny - py + 1) >> 1, nc = (L.nz - pz + 1) >> 1;
+        const int n = na * nb * nc;
+        if (n == 0) continue;
+        const long long hb = px ? 0 : L.B0;
+        for (int it = tid; it < n; it += nth) {
+            const int a = it % na, row = it / na;
+            const int j = py + 2 * (row % nb), k = pz + 2 * (row / nb);
+            gs_points<T, 27, 1>(L, l.off[px], l.opr, l.v, l.f, L.G + L.row(j, k) * L.P + hb + a, px, j, k, a, 1);
+        }
+        if (!(go = tail_sync(l.bar))) return false;
+    }
+    return true;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kTailThreads) k_vtail(const __grid_constant__ TailArgs<T> A) {
+    extern __shared__ double sm[];
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    bool go = true;
+    // down: pre-smoothing, residual, restriction (bbmg_class.f90:750-763)
+    for (int n = 0; n + 1 < A.n; n++) {
+        const TailLvl<T> &l = A.lv[n], &c = A.lv[n + 1];
+        int dir = 1;
+        for (int i = 0; i < A.pre; i++, dir = -dir)
+            if (!tail_relax(l, dir, go)) return;
+        const Lay &L = l.L;
+        for (int it = tid; it < L.nx * L.ny * L.nz; it += nth) {
+            const int i = it % L.nx, row = it / L.nx;
+            residual_point<T, 27>(L, l.off[0].o, l.off[1].o, l.opr, l.v, l.f, l.r, i, row % L.ny, row / L.ny);
+        }
+        if (!tail_sync(l.bar)) return;
+        const Lay &C = c.L;
+        for (int it = tid; it < C.nx * C.ny * C.nz; it += nth) {
+            const int i = it % C.nx, row = it / C.nx;
+            restrict_point<T>(L, C, l.c2f, l.r, c.f, c.v, i, row % C.ny, row / C.ny);
+        }
+        if (!tail_sync(l.bar)) return;
+    }
+    // coarsest level (bbmg_class.f90:741-748)
+    const TailLvl<T> &lc = A.lv[A.n - 1];
+    if (A.direct) {
+        if (blockIdx.x == 0) coarse_solve_block<T>(lc.L, A.LU, A.piv, A.pinned, lc.f, lc.v, A.mat_in_smem, sm);
+        if (!tail_sync(lc.bar)) return;
+    } else {
+        int dir = 1;
+        for (int i = 0; i < A.pre + A.post; i++, dir = -dir)
+            if (!tail_relax(lc, dir, go)) return;
+    }
+    // up: prolongation + correction, post-smoothing (bbmg_class.f90:766-775)
+    for (int n = A.n - 2; n >= 0; n--) {
+        const TailLvl<T> &l = A.lv[n], &c = A.lv[n + 1];
+        const Lay &F = l.L;
+        for (int it = tid; it < F.nx * F.ny * F.nz; it += nth) {
+            const int i = it % F.nx, row = it / F.nx;
+            prolong_point<T>(F, c.L, l.c2f, c.v, l.v, i, row % F.ny, row / F.ny);
+        }
+        if (!tail_sync(l.bar)) return;
+        int dir = (A.pre & 1) ? -1 : 1;
+        for (int i = 0; i < A.post; i++, dir = -dir)
+            if (!tail_relax(l, dir, go)) return;
+    }
+}
+
+size_t tail_smem(int np, int *mat_in_smem) {
+    const size_t full = sizeof(double) * ((size_t)np + (size_t)np * np);
+    *mat_in_smem = full <= kTailSmemMax ? 1 : 0;
+    return *mat_in_smem ? full : sizeof(double) * (size_t)np;
+}
+
+template <typename T>
+cudaError_t tail_grid(size_t smem, int *blocks) {
+    int dev = 0, nsm = 0, occ = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess && smem > 48 * 1024)
+        e = cudaFuncSetAttribute(k_vtail<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_vtail<T>, kTailThreads, smem);
+    if (e != cudaSuccess) return e;
+    if (occ < 1) return cudaErrorLaunchOutOfResources;
+    *blocks = nsm * (occ < kTailBlocksPerSm ? occ : kTailBlocksPerSm);
+    return cudaSuccess;
+}
+
+template <typename T>
+cudaError_t launch_vtail(const TailArgs<T> &A, int blocks, size_t smem, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(A.lv[0].bar, 0, 2 * sizeof(unsigned), s);  // count, gen; err persists
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(kTailThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    BB_CHECK_LAUNCH(cudaLaunchKernelEx(&cfg, k_vtail<T>, A));
+    return cudaSuccess;
+}
+
+template cudaError_t tail_grid<double>(size_t, int *);
+template cudaError_t tail_grid<float>(size_t, int *);
+template cudaError_t launch_vtail<double>(const TailArgs<double> &, int, size_t, cudaStream_t);
+template cudaError_t launch_vtail<float>(const TailArgs<float> &, int, size_t, cudaStream_t);
 
 #define BB_INST(T)                                                                                                   \
     template cudaError_t launch_relax<T>(const Lay &, const NbrOff &, int, bool, const T *, T *, const T *, int,     \

@@ -267,12 +267,28 @@ struct Fields {
     int nf;
 };
 
-__global__ void k_embed(Fields fs, Act x) {
+// pool = 1: the fields are on x's grid.  pool = 2: they are on the grid twice
+// as fine and each voxel gets the mean of its 8 children (FP64 sum).
+__global__ void k_embed(Fields fs, Act x, int pool) {
     const long long n = (long long)x.nvox * x.c;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
         const int v = (int)(e / x.c), c = (int)(e % x.c);
         float val = 0.f;
-        if (c < fs.nf) val = (float)(fs.s[c] * fs.f[c][v]);
+        if (c < fs.nf) {
+            if (pool == 1) {
+                val = (float)(fs.s[c] * fs.f[c][v]);
+            } else {
+                int nn, d, h, w;
+                decode(x, v, nn, d, h, w);
+                const int D = 2 * x.d, H = 2 * x.h, W = 2 * x.w;
+                const double *f = fs.f[c] + (long long)nn * D * H * W;
+                double sum = 0.0;
+#pragma unroll
+                for (int q = 0; q < 8; q++)
+                    sum += f[((long long)(2 * d + (q >> 2)) * H + (2 * h + ((q >> 1) & 1))) * W + 2 * w + (q & 1)];
+                val = (float)(fs.s[c] * 0.125 * sum);
+            }
+        }
         x.p[(long long)v * x.ld + c] = __float2bfloat16(val);
     }
 }
@@ -451,8 +467,9 @@ int nn_up2_bwd(const nn_act *dy, const nn_act *dx, void *stream) {
     return done(cudaGetLastError());
 }
 
-int nn_embed(int nf, const double *const *fields, const double *scales, const nn_act *x, void *stream) {
-    if (bad_act(x) || nf < 1 || nf > NN_MAX_FIELDS || nf > x->c || !fields || !scales) return BBMG_BAD_ARGS;
+int nn_embed(int nf, const double *const *fields, const double *scales, int pool, const nn_act *x, void *stream) {
+    if (bad_act(x) || nf < 1 || nf > NN_MAX_FIELDS || nf > x->c || !fields || !scales || (pool != 1 && pool != 2))
+        return BBMG_BAD_ARGS;
     Fields fs{};
     fs.nf = nf;
     for (int i = 0; i < nf; i++) {
@@ -461,7 +478,7 @@ int nn_embed(int nf, const double *const *fields, const double *scales, const nn
         fs.s[i] = scales[i];
     }
     const Act a = act_of(x);
-    k_embed<<<grid_elems((long long)a.nvox * a.c), 256, 0, (cudaStream_t)stream>>>(fs, a);
+    k_embed<<<grid_elems((long long)a.nvox * a.c), 256, 0, (cudaStream_t)stream>>>(fs, a, pool);
     return done(cudaGetLastError());
 }
 

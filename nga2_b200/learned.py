@@ -66,7 +66,7 @@ def lib():
         "nn_pool2_bwd": [A, A, I, P],
         "nn_up2": [A, A, P],
         "nn_up2_bwd": [A, A, P],
-        "nn_embed": [I, C.POINTER(P), C.POINTER(D), A, P],
+        "nn_embed": [I, C.POINTER(P), C.POINTER(D), I, A, P],
         "nn_head": [A, P, P, P, P],
         "nn_head_bwd": [A, P, P, A, P, P, P],
         "nn_mse": [P, P, D, LL, P, P, P],
@@ -209,13 +209,15 @@ class UNet:
         return b
 
     # ------------------------------------------------------------ forward
-    def embed(self, b, fields, scales):
+    def embed(self, b, fields, scales, pool=1):
+        """Input channels from FP64 fields on the network's grid (pool = 1) or
+        on the grid twice as fine (pool = 2, 2x2x2 means)."""
         if len(fields) != self.nf:
             raise ValueError(f"expected {self.nf} input fields")
         fp = (C.c_void_p * self.nf)(*[f.data_ptr() for f in fields])
         sc = (C.c_double * self.nf)(*scales)
         x0, _k = self._act(b["x0"], b["shape"][0])
-        _check(self.lib.nn_embed(self.nf, fp, sc, x0, self.stream), "embed")
+        _check(self.lib.nn_embed(self.nf, fp, sc, pool, x0, self.stream), "embed")
 
     def forward(self, b):
         """Run the network on b["x0"]; the prediction lands in b["out"]."""
@@ -374,27 +376,10 @@ class LearnedGuess:
         net = self.net
         nz, ny, nx = rec["rhs"].shape
         f, s, bmax = self.fields(rec)
-        if not self.coarse:
-            b = net.buffers((1, nz, ny, nx), train)
-            net.embed(b, f, s)
-            return b, bmax
-        b = net.buffers((1, nz // 2, ny // 2, nx // 2), train)
-        fine = self._fine_input((1, nz, ny, nx))
-        fp = (C.c_void_p * net.nf)(*[t.data_ptr() for t in f])
-        sc = (C.c_double * net.nf)(*s)
-        xf, _k1 = net._act(fine, (1, nz, ny, nx))
-        x0, _k2 = net._act(b["x0"], b["shape"][0])
-        _check(net.lib.nn_embed(net.nf, fp, sc, xf, net.stream), "embed")
-        _check(net.lib.nn_pool2(xf, x0, net.stream), "pool input")
+        k = 2 if self.coarse else 1
+        b = net.buffers((1, nz // k, ny // k, nx // k), train)
+        net.embed(b, f, s, pool=k)
         return b, bmax
-
-    def _fine_input(self, shape):
-        key = ("fine",) + tuple(shape)
-        if key not in self.net._bufs:
-            n, d, h, w = shape
-            self.net._bufs[key] = self.net.torch.empty((n * d * h * w, CIN0), dtype=self.net.torch.bfloat16,
-                                                        device=self.net.device)
-        return self.net._bufs[key]
 
     def guess(self, rec, out):
         """Write the predicted dp (FP64, rec's shape) into `out`."""

@@ -21,7 +21,9 @@ GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 
 CASES = [((8, 8, 8), (True, True, True)), ((12, 10, 9), (True, False, True)), ((9, 7, 5), (False, False, False)),
          ((17, 17, 17), (True, True, True)), ((32, 32, 1), (True, True, False)), ((10, 6, 12), (False, True, False)),
-         ((13, 8, 11), (True, True, True))]
+         ((13, 8, 11), (True, True, True)),
+         # sizes whose coarse levels run as one fused cooperative launch
+         ((16, 16, 16), (True, True, True)), ((24, 16, 24), (True, False, True)), ((20, 20, 20), (False, False, False))]
 IDS = ["x".join(map(str, d)) + "-" + "".join("p" if p else "w" for p in per) for d, per in CASES]
 
 

@@ -161,8 +161,12 @@ def test_elementwise_kernels(L):
     eg = torch.empty((2 * 4 * 6 * 8, 16), dtype=torch.bfloat16, device="cuda")
     fp = (C.c_void_p * 3)(*[t.data_ptr() for t in f])
     ss = (C.c_double * 3)(*sc)
-    assert L.nn_embed(3, fp, ss, C.byref(act(eg, sh2)), None) == 0
+    assert L.nn_embed(3, fp, ss, 1, C.byref(act(eg, sh2)), None) == 0
     close_bf16(from_cl(eg, sh2), U.embed([t.cpu().numpy() for t in f], sc, sh2))
+    # ... and from fields on the grid twice as fine (2x2x2 means)
+    ec = torch.empty((2 * 2 * 3 * 4, 16), dtype=torch.bfloat16, device="cuda")
+    assert L.nn_embed(3, fp, ss, 2, C.byref(act(ec, sh1)), None) == 0
+    close_bf16(from_cl(ec, sh1), U.pool2(U.embed([t.cpu().numpy() for t in f], sc, sh2)))
 
 
 def test_head_loss_adam_apply(L):
