@@ -31,7 +31,7 @@ extern "C" {
 /* status codes */
 #define BBMG_OK          0  /* converged: rerr <= rcvg                          */
 #define BBMG_MAXIT       1  /* stopped at maxit without reaching rcvg          */
-#define BBMG_STAGNATION  2  /* mixed precision: the residual stopped decreasing */
+#define BBMG_STAGNATION  2  /* reserved: mixed precision falls back to FP64    */
 #define BBMG_NONFINITE   3  /* NaN or Inf appeared in the residual             */
 #define BBMG_BAD_ARGS    4  /* invalid argument (also a stencil outside 3x3x3) */
 #define BBMG_NOT_SETUP   5  /* solve before setup (ils_class.f90:684)          */
@@ -44,7 +44,9 @@ extern "C" {
 
 /* arithmetic of the solve */
 #define BBMG_PREC_FP64   0  /* every step in FP64, the reference's arithmetic   */
-#define BBMG_PREC_MIXED  1  /* FP32 V-cycle inside an FP64 outer iteration      */
+#define BBMG_PREC_MIXED  1  /* FP32 V-cycle inside an FP64 outer iteration; when
+                               the residual falls by < 10 % over 3 iterations the
+                               solve continues with the FP64 method           */
 
 typedef struct bbmg_handle bbmg_handle;
 
@@ -86,6 +88,9 @@ typedef struct {
     int status;            /* status of the last solve                       */
     long long launches;    /* kernel launches of the last solve              */
     int level1_stencil;    /* level-1 storage: 27, 7, or 4 (symmetric 7-pt)  */
+    int fallback_it;       /* mixed precision: iteration after which the solve
+                              continued in FP64 because the FP32 V-cycle stopped
+                              reducing the residual (0 = never)               */
 } bbmg_info;
 
 /* Fill `p` with the ILS values: pcg_bbox, FP64, V(2,2), ncell_coarsest 300,
@@ -170,7 +175,9 @@ int bbmg_debug_step(bbmg_handle *h, int step, int level, int arg, int prec);
 /* Device time of one stage, for roofline measurements: the stage runs `reps`
  * times back to back on the handle's stream between two CUDA events; returns
  * the average milliseconds per repetition in *ms.  BBMG_STEP_RELAX times one
- * sweep as the V-cycle runs it (by colour phases on 7-point levels). */
+ * sweep as the V-cycle runs it (by colour phases on 7-point levels);
+ * BBMG_STEP_CYCLE times cycle(level) as the solve runs it, the single-launch
+ * coarse levels included. */
 int bbmg_profile_step(bbmg_handle *h, int step, int level, int arg, int prec, int reps, double *ms);
 /* dense coarsest matrix (row-major np x np), its LU (row-major, unit lower
  * below the diagonal) and pivots; any pointer may be NULL. */

@@ -6,6 +6,7 @@
 // src/solver/ils_class.f90:162-226 (init), 230-376 (setup), 674-822 (solve).
 // One iteration of a solve is captured once into a CUDA graph and replayed;
 // the host reads back one double per iteration for the convergence test.
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -67,12 +68,11 @@ struct bbmg_handle {
     std::vector<Level> lv;  // 1-based: lv[0] unused
     // coarsest dense problem
     int np = 0, lu_info = 0, npinned = 0;
-    // coarse tail of the V-cycle in one cooperative launch from level tail_n0
+    // coarse tail of the V-cycle in one cluster launch from level tail_n0
     // (0: every level runs pass by pass)
     int tail_n0 = 0;
-    bool tail_off = false;        // cooperative capture unavailable: pass by pass
-    TailBar *tbar = nullptr;
-    int tail_blocks[2] = {0, 0};  // grid per precision (0 = not sized yet)
+    bool tail_off = false;        // cluster launch unavailable or not capturable: pass by pass
+    int tail_blocks[2] = {0, 0};  // cluster size per precision (0 = not sized yet)
     size_t tail_smem_b = 0;
     int tail_mat_in_smem = 0;
     double *OP = nullptr, *LU = nullptr;
@@ -193,8 +193,13 @@ int vcycle_tail(bbmg_handle *h, int n) {
         t.f = P::f(l);
         t.r = P::r(l);
         t.c2f = m < h->nlvl ? P::c2f(l) : nullptr;
-        t.bar = h->tbar;
     }
+    A.split = A.n - 1;
+    for (int m = 0; m < A.n - 1; m++) {
+        const Lay &L = A.lv[m].L;
+        if ((long long)L.nx * L.ny * L.nz <= kTailBlockCells) { A.split = m; break; }
+    }
+    if (const char *env = getenv("BBMG_TAIL_SPLIT")) A.split = std::max(0, std::min(A.n - 1, atoi(env)));
     A.pre = h->prm.relax_pre;
     A.post = h->prm.relax_post;
     A.direct = h->prm.use_direct_solve;
@@ -203,7 +208,11 @@ int vcycle_tail(bbmg_handle *h, int n) {
     A.piv = h->piv;
     A.pinned = h->pinned;
     int &blocks = h->tail_blocks[PrecIdx<T>::value];
-    if (!blocks) CU(h, tail_grid<T>(h->tail_smem_b, &blocks));
+    if (!blocks && tail_grid<T>(h->tail_smem_b, &blocks) != cudaSuccess) {
+        cudaGetLastError();
+        h->tail_off = true;  // no cluster of 8 fits: the levels run pass by pass
+        return BBMG_NOT_SETUP;
+    }
     CU(h, launch_vtail<T>(A, blocks, h->tail_smem_b, h->stream));
     return BBMG_OK;
 }
@@ -291,8 +300,8 @@ int get_graph(bbmg_handle *h, int mode, int par, cudaGraphExec_t *out) {
     int st = record_iteration(h, mode, par);
     cudaError_t e = cudaStreamEndCapture(h->stream, &g);
     if ((st || e != cudaSuccess) && h->tail_n0 && !h->tail_off) {
-        // a cooperative launch that cannot be captured here: record the
-        // coarse levels pass by pass instead
+        // a cluster launch that cannot be captured here: record the coarse
+        // levels pass by pass instead
         if (g) cudaGraphDestroy(g);
         g = nullptr;
         cudaGetLastError();
@@ -365,7 +374,6 @@ int bbmg_destroy(bbmg_handle *h) {
     }
     dfree(h->OP); dfree(h->LU); dfree(h->piv); dfree(h->pinned); dfree(h->d_info); dfree(h->d_flag);
     dfree(h->sol); dfree(h->pp); dfree(h->pp2); dfree(h->Ap); dfree(h->x2); dfree(h->sc); dfree(h->part); dfree(h->dscal);
-    dfree(h->tbar);
     dfree(h->d_opr_in); dfree(h->d_stc); dfree(h->d_io);
     if (h->h_scal) cudaFreeHost(h->h_scal);
     if (h->ev0) cudaEventDestroy(h->ev0);
@@ -487,7 +495,7 @@ int bbmg_create(const bbmg_grid *grid, const bbmg_params *params, bbmg_handle **
     {
         // the coarse tail: the first level >= 2 at or below tail_cells cells
         // from which every level can be fused (27-point, periodic sizes even)
-        long long tail_cells = 1LL << 21;
+        long long tail_cells = kTailCells;
         if (const char *env = getenv("BBMG_TAIL_CELLS")) tail_cells = atoll(env);
         for (int n = 2; prm.ncycle == 1 && tail_cells > 0 && n < h->nlvl; n++) {
             const Lay &L = h->lv[n].L;
@@ -496,12 +504,7 @@ int bbmg_create(const bbmg_grid *grid, const bbmg_params *params, bbmg_handle **
             for (int m = n; m <= h->nlvl; m++) ok = ok && h->lv[m].fuse;
             if (ok) { h->tail_n0 = n; break; }
         }
-        if (h->tail_n0) {
-            unsigned *tb = nullptr;
-            if ((st = dalloc(h, &tb, 4))) return bail(st);
-            h->tbar = reinterpret_cast<TailBar *>(tb);
-            h->tail_smem_b = tail_smem(h->np, &h->tail_mat_in_smem);
-        }
+        if (h->tail_n0) h->tail_smem_b = tail_smem(h->np, &h->tail_mat_in_smem);
     }
     if (cudaMallocHost((void **)&h->h_scal, 8 * sizeof(double)) != cudaSuccess) return bail(fail(h, BBMG_NO_MEMORY, "pinned host"));
     if (cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess)
@@ -697,7 +700,6 @@ int bbmg_solve(bbmg_handle *h, const double *rhs, double *sol, int *it_out, doub
     int it = -1;
     double rerr = HUGE_VAL;
     CU(h, cudaEventRecord(h->ev0, s));
-    if (h->tbar) CU(h, cudaMemsetAsync(&h->tbar->err, 0, sizeof(unsigned), s));
     // rhs/initial guess into the level-1 arrays; overlap zero, then periodic
     // images (bbmg_class.f90:611-624; ils_class.f90:693-700)
     CU(h, cudaMemsetAsync(l1.f, 0, sizeof(double) * L.plane, s));
@@ -728,6 +730,7 @@ int bbmg_solve(bbmg_handle *h, const double *rhs, double *sol, int *it_out, doub
     double rnorm = res0;
     if (by_rhs && h->h_scal[3] > 0.0) rnorm = h->h_scal[3];
     int status = BBMG_OK;
+    int fallback_it = 0;
     double *xout = l1.v;
     long long launches = by_rhs ? 6 : 4;  // two copies-in, residual, max (two) [, max of rhs (two)]
     if (res0 == 0.0) {
@@ -761,45 +764,51 @@ int bbmg_solve(bbmg_handle *h, const double *rhs, double *sol, int *it_out, doub
             launches += 1;
         }
         cudaGraphExec_t ge[2] = {nullptr, nullptr};
-        const bool pingpong = krylov || mixed;
+        bool pingpong = krylov || mixed;
         if ((st = get_graph(h, mode, 0, &ge[0]))) return st;
         if (pingpong && (st = get_graph(h, mode, 1, &ge[1]))) return st;
-        double prev = HUGE_VAL;
-        int stall = 0;
+        std::vector<double> hist;
+        hist.reserve(h->prm.maxit + 1);
         for (int n = 1; n <= h->prm.maxit; n++) {
             const int par = pingpong ? ((n - 1) & 1) : 0;
-            if (!krylov && mixed) xout = par ? l1.v : h->x2;  // the buffer this iteration writes
+            if (mode == 2) xout = par ? l1.v : h->x2;  // the buffer this iteration writes
             CU(h, cudaGraphLaunch(ge[par], s));
             launches += h->gkernels[mode][par];
             double mr = 0.0;
             if ((st = sync_read(h, &mr, 1))) return st;
             rerr = mr / rnorm;  // bbmg_class.f90:696,723 (rnorm = res0 there)
             it = n;
+            hist.push_back(rerr);
             if (!(rerr == rerr) || std::isinf(rerr)) {
                 status = fail(h, BBMG_NONFINITE, "residual became non-finite at iteration %d", n);
                 break;
             }
             if (rerr <= h->prm.rcvg) break;
-            if (mixed) {
-                // FP32 preconditioning cannot reduce below its rounding floor:
-                // report stagnation instead of spinning to maxit
-                if (rerr > 0.95 * prev) stall++;
-                else stall = 0;
-                if (stall >= 5) {
-                    status = fail(h, BBMG_STAGNATION, "residual stagnated at %g after %d iterations", rerr, n);
-                    break;
+            // An FP32 V-cycle cannot resolve error components below its rounding
+            // floor (high-contrast coefficients make them large): when the
+            // residual drops by less than 10 % over three iterations, the rest
+            // of the solve runs the plain FP64 method from the current iterate.
+            if (mode >= 2 && n >= 4 && rerr > 0.9 * hist[n - 4]) {
+                if (mode == 3) {
+                    // restart CG (beta = 0) with the FP64 V-cycle as preconditioner
+                    CU(h, cudaMemsetAsync(l1.v, 0, sizeof(double) * L.plane, s));
+                    CU(h, cudaMemsetAsync(h->sc, 0, sizeof(CgScal), s));
+                    mode = 1;
+                } else {
+                    // mgsolve's cycles act on lvl(1)%v in place: move x there
+                    if (xout != l1.v)
+                        CU(h, cudaMemcpyAsync(l1.v, xout, sizeof(double) * L.plane, cudaMemcpyDeviceToDevice, s));
+                    xout = l1.v;
+                    mode = 0;
+                    pingpong = false;
                 }
+                ge[0] = ge[1] = nullptr;
+                if ((st = get_graph(h, mode, 0, &ge[0]))) return st;
+                if (pingpong && (st = get_graph(h, mode, 1, &ge[1]))) return st;
+                fallback_it = n;
             }
-            prev = rerr;
         }
         if (status == BBMG_OK && rerr > h->prm.rcvg) status = BBMG_MAXIT;
-        if (h->tbar) {
-            unsigned terr = 0;
-            CU(h, cudaMemcpyAsync(h->h_scal + 5, &h->tbar->err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-            CU(h, cudaStreamSynchronize(s));
-            memcpy(&terr, h->h_scal + 5, sizeof(unsigned));
-            if (terr) status = fail(h, BBMG_CUDA, "a grid barrier of the coarse-level kernel timed out");
-        }
     }
     // solution out (ils_class.f90:782-788)
     if (sol_dev) {
@@ -823,6 +832,7 @@ int bbmg_solve(bbmg_handle *h, const double *rhs, double *sol, int *it_out, doub
     h->info.true_rerr = -1.0;
     h->info.status = status;
     h->info.launches = launches + 1;
+    h->info.fallback_it = fallback_it;
     if (it_out) *it_out = it;
     if (rerr_out) *rerr_out = rerr;
     return status;
@@ -959,7 +969,8 @@ int bbmg_profile_step(bbmg_handle *h, int step, int n, int arg, int prec, int re
     if (!h->setup_done) return fail(h, BBMG_NOT_SETUP, "not set up");
     if (n < 1 || n > h->nlvl) return fail(h, BBMG_BAD_ARGS, "level %d out of range", n);
     if (prec == 1 && h->prm.precision != BBMG_PREC_MIXED) return fail(h, BBMG_BAD_ARGS, "no FP32 copy (FP64 handle)");
-    if (step != BBMG_STEP_RELAX && step != BBMG_STEP_RESIDUAL && step != BBMG_STEP_RESTRICT && step != BBMG_STEP_PROLONG)
+    if (step != BBMG_STEP_RELAX && step != BBMG_STEP_RESIDUAL && step != BBMG_STEP_RESTRICT &&
+        step != BBMG_STEP_PROLONG && step != BBMG_STEP_CYCLE)
         return fail(h, BBMG_BAD_ARGS, "step %d cannot be profiled", step);
     if ((step == BBMG_STEP_RESTRICT || step == BBMG_STEP_PROLONG) && n >= h->nlvl)
         return fail(h, BBMG_BAD_ARGS, "no coarser level");
@@ -969,6 +980,11 @@ int bbmg_profile_step(bbmg_handle *h, int step, int n, int arg, int prec, int re
     CU(h, cudaEventRecord(h->ev0, s));
     for (int r = 0; r < reps; r++) {
         cudaError_t e = cudaSuccess;
+        if (step == BBMG_STEP_CYCLE) {  // cycle(n) as the solve runs it (the fused tail included)
+            int st = prec == 1 ? vcycle<float>(h, n) : vcycle<double>(h, n);
+            if (st) return st;
+            continue;
+        }
         if (prec == 1) {
             using P = LvlPtr<float>;
             if (step == BBMG_STEP_RELAX) e = launch_relax_sweeps<float>(l.L, l.nb, l.npt, l.fuse, P::opr(l), P::v(l), P::f(l), arg >= 0 ? 1 : -1, 1, s);

@@ -351,7 +351,7 @@ __global__ void k_dense_operator(Lay L, const double *__restrict__ opr, double *
 // thread block (the DGESV factorisation of bbmg_class.f90:912-913, done once
 // per setup because the reference's per-call factorisation is deterministic).
 // Pivot: the first row holding the largest magnitude.  Then marks the
-// unknowns whose pivot is below n*eps*max|pivot| (a singular coarsest
+// unknowns whose pivot is below 1000*n*eps*max|pivot| (a singular coarsest
 // matrix); the solve sets those to zero.
 __global__ void k_lu(double *__restrict__ A, int n, int *__restrict__ piv, int *__restrict__ pinned,
                      int *__restrict__ info_out) {
@@ -414,7 +414,11 @@ __global__ void k_lu(double *__restrict__ A, int n, int *__restrict__ piv, int *
         if (tid < s) sval[tid] = fmax(sval[tid], sval[tid + s]);
         __syncthreads();
     }
-    double tol = (double)n * kEps * sval[0];
+    // round-off pivots of a singular (periodic / all-Neumann) coarsest matrix
+    // reach ~1e-14 of the largest once density contrasts of 1e3 enter the
+    // Galerkin operators, while genuine pivots stay above ~1e-3 of it: pin
+    // within three decades of the round-off level n*eps*max|pivot|
+    double tol = 1000.0 * (double)n * kEps * sval[0];
     for (int k = tid; k < n; k += nt) pinned[k] = fabs(A[(long long)k * n + k]) <= tol ? 1 : 0;
     if (tid == 0) *info_out = s_info;
 }

@@ -40,14 +40,10 @@ template <typename T>
 cudaError_t launch_coarse_solve(const Lay &L, const double *LU, const int *piv, const int *pinned, const T *f, T *v,
                                 cudaStream_t s);
 
-// the coarse tail of the V-cycle in one cooperative launch (levels n0..nlvl,
-// 27-point operators, V-cycle only)
+// the coarse tail of the V-cycle in one launch of one thread-block cluster
+// (levels n0..nlvl, 27-point operators, V-cycle only)
 struct Off27 {
     int o[27];
-};
-struct TailBar {
-    unsigned count, gen;  // grid barrier state, zeroed before every launch
-    unsigned err;         // set when a barrier wait runs out; cleared by the host
 };
 template <typename T>
 struct TailLvl {
@@ -56,17 +52,19 @@ struct TailLvl {
     const T *opr;          // 27 coefficient planes
     T *v, *f, *r;
     const T *c2f;          // prolongation weights of this level (to the next coarser one)
-    TailBar *bar;
 };
 constexpr int kTailMax = 8;            // levels in one launch (kernel parameters stay under 4 KB)
 constexpr int kTailThreads = 512;
-constexpr int kTailBlocksPerSm = 1;
-constexpr unsigned kTailSpinLimit = 1u << 24;  // polls of 64 ns naps: about a second
+constexpr int kTailClusterMax = 16;    // blocks of the cluster (non-portable size; 8 if refused)
+constexpr long long kTailCells = 1LL << 15;  // first fused level: at most 32^3 cells (larger
+                                             // levels need more than one cluster's bandwidth)
 constexpr size_t kTailSmemMax = 100 * 1024;
+constexpr long long kTailBlockCells = 4096;  // levels this small run inside one block
 template <typename T>
 struct TailArgs {
     TailLvl<T> lv[kTailMax];
     int n;                 // levels in lv; lv[n-1] is the coarsest
+    int split;             // levels >= split (when split < n-1) run inside one block
     int pre, post, direct, mat_in_smem;
     const double *LU;
     const int *piv, *pinned;

@@ -280,10 +280,16 @@ __device__ __forceinline__ void restrict_point(const Lay &F, const Lay &C, const
     const int rk0 = -pmod(F.zper, fk - 1, F.nz), rk1 = pmod(F.zper, fk + 1, F.nz);
     const int rj0 = -pmod(F.yper, fj - 1, F.ny), rj1 = pmod(F.yper, fj + 1, F.ny);
     const int ri0 = -pmod(F.xper, fi - 1, F.nx), ri1 = pmod(F.xper, fi + 1, F.nx);
+    // all 27 offsets unrolled, the ones outside [r0, r1] predicated off: the
+    // loads issue together, the terms enter the sum in the same order
     T s = T(0);
-    for (int rk = rk0; rk <= rk1; rk++)
-        for (int rj = rj0; rj <= rj1; rj++)
-            for (int ri = ri0; ri <= ri1; ri++) {
+#pragma unroll
+    for (int rk = -1; rk <= 1; rk++)
+#pragma unroll
+        for (int rj = -1; rj <= 1; rj++)
+#pragma unroll
+            for (int ri = -1; ri <= 1; ri++) {
+                if (rk < rk0 || rk > rk1 || rj < rj0 || rj > rj1 || ri < ri0 || ri > ri1) continue;
                 const long long fid = F.idx(fi + ri, fj + rj, fk + rk);
                 s = O::mac(s, c2f[(long long)q8((1 - ri) / 2, (1 - rj) / 2, (1 - rk) / 2) * F.plane + fid], rF[fid]);
             }
@@ -317,10 +323,15 @@ __device__ __forceinline__ void prolong_point(const Lay &F, const Lay &C, const 
     const int n1 = i & 1, n2 = j & 1, n3 = k & 1, ci = i >> 1, cj = j >> 1, ck = k >> 1;
     const long long id = F.idx(i, j, k);
     T e = T(0);
-    for (int pk = 0; pk <= n3; pk++)
-        for (int pj = 0; pj <= n2; pj++)
-            for (int pi = 0; pi <= n1; pi++)
+#pragma unroll
+    for (int pk = 0; pk <= 1; pk++)
+#pragma unroll
+        for (int pj = 0; pj <= 1; pj++)
+#pragma unroll
+            for (int pi = 0; pi <= 1; pi++) {
+                if (pk > n3 || pj > n2 || pi > n1) continue;  // predicated: same terms, same order
                 e = O::mac(e, c2f[(long long)q8(pi, pj, pk) * F.plane + id], vC[C.idx(ci + pi, cj + pj, ck + pk)]);
+            }
     const T val = O::add(vF[id], e);
     vF[id] = val;
     if (on_periodic_face(F, i, j, k)) write_images(F, vF, i, j, k, val);
@@ -903,65 +914,31 @@ cudaError_t launch_defect_fused(const Lay &L, const NbrOff &nb, int npt, const d
 }
 
 // ---------------------------------------------------------------------------
-// The coarse tail of the V-cycle in one launch.  Below a few million cells a
-// level's colour passes, residual, restriction and prolongation each take a
-// few microseconds of work but a full kernel launch; this persistent kernel
-// runs cycle(n0) (bbmg_class.f90:732-776) for every level n0..nlvl with one
-// grid barrier between dependent passes instead.  Each pass calls the same
-// per-point functions as the single-pass kernels, so the FP64 result is
-// bit-identical.  The launch is cooperative (every block resident), and every
-// barrier wait is bounded: a wait that runs out sets the error flag and the
-// kernel returns, so a fault can never hang the GPU.
-__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_release_u32(unsigned *p, unsigned v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ unsigned atom_add_acq_rel_u32(unsigned *p, unsigned v) {
-    unsigned old;
-    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
-    return old;
+// The coarse tail of the V-cycle in one launch.  On levels of at most a few
+// hundred thousand cells a colour pass, residual, restriction or prolongation
+// is a few microseconds of work but a full kernel launch (about 35 launches
+// per level and cycle).  This kernel runs cycle(n0) (bbmg_class.f90:732-776)
+// for every level n0..nlvl inside one thread-block cluster: the passes are
+// separated by the cluster's hardware barrier, whose release/acquire
+// semantics make each pass's global-memory writes visible to the next.  A
+// cluster is scheduled as a unit, so no block can wait on one that is not
+// running, and no barrier can outlive its kernel.  Each pass calls the same
+// per-point functions as the single-pass kernels, so FP64 results stay
+// bit-identical.
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
 
-// Sense-free generation barrier over all blocks of the grid.  Returns false
-// (and raises bar->err) if a wait exceeded kTailSpinLimit polls (about a
-// second); callers then return without touching memory again.
-__device__ bool tail_sync(TailBar *bar) {
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int ok = 1;
-        if (ld_acquire_u32(&bar->err)) {
-            ok = 0;
-        } else {
-            const unsigned g = ld_acquire_u32(&bar->gen);
-            if (atom_add_acq_rel_u32(&bar->count, 1u) == gridDim.x - 1) {
-                bar->count = 0;  // ordered before the release of the next generation
-                st_release_u32(&bar->gen, g + 1u);
-            } else {
-                unsigned spins = 0;
-                while (ld_acquire_u32(&bar->gen) == g) {
-                    if (++spins > kTailSpinLimit) {
-                        atomicExch(&bar->err, 1u);
-                        ok = 0;
-                        break;
-                    }
-                    __nanosleep(64);
-                }
-            }
-        }
-        s_ok = ok;
-    }
-    __syncthreads();
-    return s_ok != 0;
+// The passes of the tail, over the threads [tid, nth) of either the whole
+// cluster (CL: a cluster barrier after each pass) or block 0 alone.
+template <bool CL>
+__device__ __forceinline__ void pass_sync() {
+    if (CL) cluster_sync_all();
+    else __syncthreads();
 }
 
-template <typename T>
-__device__ bool tail_relax(const TailLvl<T> &l, int dir, bool &go) {
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+template <bool CL, typename T>
+__device__ void tail_relax(const TailLvl<T> &l, int dir, int tid, int nth) {
     for (int c = 0; c < 8; c++) {
         const int col = dir > 0 ? c : 7 - c;  // colours 1..8 forward, 8..1 backward
         const int px = col & 1, py = (col >> 1) & 1, pz = (col >> 2) & 1;
@@ -975,58 +952,76 @@ __device__ bool tail_relax(const TailLvl<T> &l, int dir, bool &go) {
             const int j = py + 2 * (row % nb), k = pz + 2 * (row / nb);
             gs_points<T, 27, 1>(L, l.off[px], l.opr, l.v, l.f, L.G + L.row(j, k) * L.P + hb + a, px, j, k, a, 1);
         }
-        if (!(go = tail_sync(l.bar))) return false;
+        pass_sync<CL>();
     }
-    return true;
 }
 
+// pre-smoothing, residual and restriction of level l into c (bbmg_class.f90:750-763)
+template <bool CL, typename T>
+__device__ void tail_down(const TailArgs<T> &A, const TailLvl<T> &l, const TailLvl<T> &c, int tid, int nth) {
+    int dir = 1;
+    for (int i = 0; i < A.pre; i++, dir = -dir) tail_relax<CL>(l, dir, tid, nth);
+    const Lay &L = l.L;
+    for (int it = tid; it < L.nx * L.ny * L.nz; it += nth) {
+        const int i = it % L.nx, row = it / L.nx;
+        residual_point<T, 27>(L, l.off[0].o, l.off[1].o, l.opr, l.v, l.f, l.r, i, row % L.ny, row / L.ny);
+    }
+    pass_sync<CL>();
+    const Lay &C = c.L;
+    for (int it = tid; it < C.nx * C.ny * C.nz; it += nth) {
+        const int i = it % C.nx, row = it / C.nx;
+        restrict_point<T>(L, C, l.c2f, l.r, c.f, c.v, i, row % C.ny, row / C.ny);
+    }
+    pass_sync<CL>();
+}
+
+// prolongation + correction into l from c, post-smoothing (bbmg_class.f90:766-775)
+template <bool CL, typename T>
+__device__ void tail_up(const TailArgs<T> &A, const TailLvl<T> &l, const TailLvl<T> &c, int tid, int nth) {
+    const Lay &F = l.L;
+    for (int it = tid; it < F.nx * F.ny * F.nz; it += nth) {
+        const int i = it % F.nx, row = it / F.nx;
+        prolong_point<T>(F, c.L, l.c2f, c.v, l.v, i, row % F.ny, row / F.ny);
+    }
+    pass_sync<CL>();
+    int dir = (A.pre & 1) ? -1 : 1;
+    for (int i = 0; i < A.post; i++, dir = -dir) tail_relax<CL>(l, dir, tid, nth);
+}
+
+// coarsest level (bbmg_class.f90:741-748): block 0 solves with the stored LU
+template <bool CL, typename T>
+__device__ void tail_coarsest(const TailArgs<T> &A, double *sm, int tid, int nth) {
+    const TailLvl<T> &lc = A.lv[A.n - 1];
+    if (A.direct) {
+        if (blockIdx.x == 0) coarse_solve_block<T>(lc.L, A.LU, A.piv, A.pinned, lc.f, lc.v, A.mat_in_smem, sm);
+        pass_sync<CL>();
+        return;
+    }
+    int dir = 1;
+    for (int i = 0; i < A.pre + A.post; i++, dir = -dir) tail_relax<CL>(lc, dir, tid, nth);
+}
+
+// The launch is one cluster.  Levels [0, A.split) run on every block of it;
+// when A.split < A.n - 1 the levels [A.split, A.n) -- a few thousand cells or
+// fewer -- run inside block 0 with block-wide barriers while the other blocks
+// wait at one cluster barrier; otherwise only the coarsest level is left.
 template <typename T>
 __global__ void __launch_bounds__(kTailThreads) k_vtail(const __grid_constant__ TailArgs<T> A) {
     extern __shared__ double sm[];
     const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
-    bool go = true;
-    // down: pre-smoothing, residual, restriction (bbmg_class.f90:750-763)
-    for (int n = 0; n + 1 < A.n; n++) {
-        const TailLvl<T> &l = A.lv[n], &c = A.lv[n + 1];
-        int dir = 1;
-        for (int i = 0; i < A.pre; i++, dir = -dir)
-            if (!tail_relax(l, dir, go)) return;
-        const Lay &L = l.L;
-        for (int it = tid; it < L.nx * L.ny * L.nz; it += nth) {
-            const int i = it % L.nx, row = it / L.nx;
-            residual_point<T, 27>(L, l.off[0].o, l.off[1].o, l.opr, l.v, l.f, l.r, i, row % L.ny, row / L.ny);
+    for (int n = 0; n < A.split; n++) tail_down<true>(A, A.lv[n], A.lv[n + 1], tid, nth);
+    if (A.split < A.n - 1) {
+        if (blockIdx.x == 0) {
+            const int t = threadIdx.x, nt = blockDim.x;
+            for (int n = A.split; n + 1 < A.n; n++) tail_down<false>(A, A.lv[n], A.lv[n + 1], t, nt);
+            tail_coarsest<false>(A, sm, t, nt);
+            for (int n = A.n - 2; n >= A.split; n--) tail_up<false>(A, A.lv[n], A.lv[n + 1], t, nt);
         }
-        if (!tail_sync(l.bar)) return;
-        const Lay &C = c.L;
-        for (int it = tid; it < C.nx * C.ny * C.nz; it += nth) {
-            const int i = it % C.nx, row = it / C.nx;
-            restrict_point<T>(L, C, l.c2f, l.r, c.f, c.v, i, row % C.ny, row / C.ny);
-        }
-        if (!tail_sync(l.bar)) return;
-    }
-    // coarsest level (bbmg_class.f90:741-748)
-    const TailLvl<T> &lc = A.lv[A.n - 1];
-    if (A.direct) {
-        if (blockIdx.x == 0) coarse_solve_block<T>(lc.L, A.LU, A.piv, A.pinned, lc.f, lc.v, A.mat_in_smem, sm);
-        if (!tail_sync(lc.bar)) return;
+        cluster_sync_all();
     } else {
-        int dir = 1;
-        for (int i = 0; i < A.pre + A.post; i++, dir = -dir)
-            if (!tail_relax(lc, dir, go)) return;
+        tail_coarsest<true>(A, sm, tid, nth);
     }
-    // up: prolongation + correction, post-smoothing (bbmg_class.f90:766-775)
-    for (int n = A.n - 2; n >= 0; n--) {
-        const TailLvl<T> &l = A.lv[n], &c = A.lv[n + 1];
-        const Lay &F = l.L;
-        for (int it = tid; it < F.nx * F.ny * F.nz; it += nth) {
-            const int i = it % F.nx, row = it / F.nx;
-            prolong_point<T>(F, c.L, l.c2f, c.v, l.v, i, row % F.ny, row / F.ny);
-        }
-        if (!tail_sync(l.bar)) return;
-        int dir = (A.pre & 1) ? -1 : 1;
-        for (int i = 0; i < A.post; i++, dir = -dir)
-            if (!tail_relax(l, dir, go)) return;
-    }
+    for (int n = A.split - 1; n >= 0; n--) tail_up<true>(A, A.lv[n], A.lv[n + 1], tid, nth);
 }
 
 size_t tail_smem(int np, int *mat_in_smem) {
@@ -1035,34 +1030,45 @@ size_t tail_smem(int np, int *mat_in_smem) {
     return *mat_in_smem ? full : sizeof(double) * (size_t)np;
 }
 
+static cudaLaunchConfig_t tail_cfg(int cl, size_t smem, cudaStream_t s, cudaLaunchAttribute *at) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cl);
+    cfg.blockDim = dim3(kTailThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cl;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cfg;
+}
+
+// The largest cluster (16 blocks, else 8) the device can schedule for k_vtail.
 template <typename T>
 cudaError_t tail_grid(size_t smem, int *blocks) {
-    int dev = 0, nsm = 0, occ = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t e = cudaFuncSetAttribute(k_vtail<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (e == cudaSuccess && smem > 48 * 1024)
         e = cudaFuncSetAttribute(k_vtail<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_vtail<T>, kTailThreads, smem);
     if (e != cudaSuccess) return e;
-    if (occ < 1) return cudaErrorLaunchOutOfResources;
-    *blocks = nsm * (occ < kTailBlocksPerSm ? occ : kTailBlocksPerSm);
-    return cudaSuccess;
+    for (int cl = kTailClusterMax; cl >= 8; cl /= 2) {
+        cudaLaunchAttribute at[1];
+        cudaLaunchConfig_t cfg = tail_cfg(cl, smem, nullptr, at);
+        int nc = 0;
+        if (cudaOccupancyMaxActiveClusters(&nc, k_vtail<T>, &cfg) == cudaSuccess && nc >= 1) {
+            *blocks = cl;
+            return cudaSuccess;
+        }
+        cudaGetLastError();
+    }
+    return cudaErrorLaunchOutOfResources;
 }
 
 template <typename T>
 cudaError_t launch_vtail(const TailArgs<T> &A, int blocks, size_t smem, cudaStream_t s) {
-    cudaError_t e = cudaMemsetAsync(A.lv[0].bar, 0, 2 * sizeof(unsigned), s);  // count, gen; err persists
-    if (e != cudaSuccess) return e;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(blocks);
-    cfg.blockDim = dim3(kTailThreads);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = s;
     cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeCooperative;
-    at[0].val.cooperative = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
+    cudaLaunchConfig_t cfg = tail_cfg(blocks, smem, s, at);
     BB_CHECK_LAUNCH(cudaLaunchKernelEx(&cfg, k_vtail<T>, A));
     return cudaSuccess;
 }

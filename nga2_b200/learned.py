@@ -348,12 +348,15 @@ class UNet:
 class LearnedGuess:
     """A trained UNet turned into an initial guess for bbmg_solve.
 
-    Inputs of a solve: its rhs b, the previous pressure and (``use_rho``) the
-    density.  The network predicts dp / (kappa max|b|) and the guess is that
-    times kappa max|b| (the problem is linear in b, so the scale is taken out
-    of the network).  With ``coarse`` the network runs on the grid twice as
-    coarse (inputs pooled 2x2x2, prediction interpolated trilinearly back),
-    which is how a network trained at 128^3 serves a 256^3 solve."""
+    Inputs of a solve: its rhs b, the previous solve's solution p_prev (the
+    previous pressure increment) and (``use_rho``) the density.  The guess is
+    p_prev + kappa max|b| net(...): the network predicts the change of the
+    increment from one solve to the next, scaled by max|b| (the problem is
+    linear in b, so the scale is taken out of the network), and a network that
+    outputs zero reproduces the plain warm start.  With ``coarse`` the network
+    runs on the grid twice as coarse (inputs pooled 2x2x2, prediction
+    interpolated trilinearly back), which is how a network trained at 128^3
+    serves a 256^3 solve."""
 
     def __init__(self, net: UNet, kappa=1.0, use_rho=True, ratio=1000.0, coarse=False):
         self.net, self.kappa, self.use_rho, self.ratio, self.coarse = net, float(kappa), use_rho, ratio, coarse
@@ -387,16 +390,16 @@ class LearnedGuess:
         b, bmax = self._input(rec, False)
         net.forward(b)
         n, d, h, w = b["shape"][0]
-        _check(net.lib.nn_apply(None, net._ptr(b["out"]), self.kappa * bmax, n, d, h, w, 2 if self.coarse else 1,
-                                net._ptr(out), net.stream), "apply")
+        base = rec["p_prev"].contiguous()
+        _check(net.lib.nn_apply(net._ptr(base), net._ptr(b["out"]), self.kappa * bmax, n, d, h, w,
+                                2 if self.coarse else 1, net._ptr(out), net.stream), "apply")
         return out
 
     def train_step(self, rec, lr):
         net = self.net
         b, bmax = self._input(rec, True)
         net.forward(b)
-        target = rec["dp"] if not self.coarse else rec["dp_coarse"]
-        loss = net.loss_grad(b, target, 1.0 / (self.kappa * bmax))
+        loss = net.loss_grad(b, rec["target"], 1.0 / (self.kappa * bmax))
         net.grads.zero_()
         net.backward(b)
         net.adam(lr)
@@ -404,8 +407,8 @@ class LearnedGuess:
 
 
 def fit_kappa(records):
-    """Median of max|dp| / max|rhs| over the training records."""
-    r = [float(rec["dp"].abs().max()) / float(rec["rhs"].abs().max()) for rec in records]
+    """Median of max|dp - p_prev| / max|rhs| over the training records."""
+    r = [float((rec["dp"] - rec["p_prev"]).abs().max()) / float(rec["rhs"].abs().max()) for rec in records]
     return float(np.median(r))
 
 
@@ -414,10 +417,12 @@ def train(guess: LearnedGuess, records, steps, lr=2e-3, lr_final=2e-4, seed=0, l
     decay; returns the per-step losses (normalised MSE)."""
     torch = guess.net.torch
     rng = np.random.default_rng(seed)
-    if guess.coarse:
-        for rec in records:
-            if "dp_coarse" not in rec:
-                rec["dp_coarse"] = torch.nn.functional.avg_pool3d(rec["dp"][None, None], 2)[0, 0].contiguous()
+    for rec in records:  # the network's target: the change from the warm start, on its grid
+        if "target" not in rec:
+            t = rec["dp"] - rec["p_prev"]
+            if guess.coarse:
+                t = torch.nn.functional.avg_pool3d(t[None, None], 2)[0, 0]
+            rec["target"] = t.contiguous()
     losses = []
     for t in range(steps):
         lr_t = lr_final + 0.5 * (lr - lr_final) * (1.0 + math.cos(math.pi * t / max(1, steps)))

@@ -513,13 +513,16 @@ void orc_recompute_direct(obbmg *b) {
     /* A periodic or all-Neumann problem makes the coarsest matrix singular;
        its LU then ends with a pivot of round-off size.  Dividing by it (what
        DGESV does) injects an arbitrarily large null-space component; with
-       pin_singular the unknown of every pivot below np*eps*max|pivot| is set
-       to zero instead, i.e. the consistent part of the system is solved. */
+       pin_singular the unknown of every pivot below 1000*np*eps*max|pivot|
+       (three decades above the round-off level: with density contrasts of
+       1e3 the round-off pivot reaches ~1e-14 of the largest, genuine ones
+       stay above ~1e-3) is set to zero instead, i.e. the consistent part of
+       the system is solved. */
     free(b->pinned);
     b->pinned = calloc(np, sizeof(int));
     double umax = 0.0;
     for (int k = 0; k < np; k++) umax = fmax(umax, fabs(b->LU[(long)k * np + k]));
-    double tol = (double)np * ORC_EPS * umax;
+    double tol = 1000.0 * (double)np * ORC_EPS * umax;
     for (int k = 0; k < np; k++) b->pinned[k] = b->pin_singular && fabs(b->LU[(long)k * np + k]) <= tol;
 }
 

@@ -304,10 +304,11 @@ def test_training_reduces_the_loss():
 def test_learned_guess_saves_iterations():
     """Train on the first steps of a drop sequence the plain GPU multigrid
     generates, then solve the following steps from the network's guess and
-    from zero (NGA2's choice) to the same max|b - A x| <= 1e-10 max|b|."""
+    from zero (NGA2's choice) to the same max|b - A x| <= 1e-10 max|b|; the
+    plain warm start (the previous solve's solution) is measured beside it."""
     torch.manual_seed(0)
     n = 32
-    seq = SQ.DropSequence(n, seed=11, ndrops=10, rmin=3.0 / n, rmax=6.0 / n, noise=1e-3, device="cuda")
+    seq = SQ.DropSequence(n, seed=11, ndrops=10, rmin=3.0 / n, rmax=6.0 / n, device="cuda")
     solve = SQ.bbmg_solver(n)
     recs = [seq.step(solve) for _ in range(56)]
     assert all(st == 0 for _, _, st in solve.stats)
@@ -318,24 +319,28 @@ def test_learned_guess_saves_iterations():
     assert np.mean(losses[-50:]) < 0.5 * np.mean(losses[:20])
     h = solve.handle
     h.set_residual_norm(B.NORM_RHS)
-    its0, its1 = [], []
+    its0, its1, itsw = [], [], []
     for rec in test_recs:
         h.setup(SQ_STC(), rec["opr"].contiguous())
         b = rec["rhs"].contiguous()
         x0 = torch.zeros_like(b)
         _, it0, _, st0 = h.solve(b, x0)
+        xw = rec["p_prev"].clone()
+        _, itw, _, stw = h.solve(b, xw)
         x1 = torch.empty_like(b)
         guess.guess(rec, x1)
         torch.cuda.synchronize()
         _, it1, rerr1, st1 = h.solve(b, x1)
-        assert st0 == 0 and st1 == 0
-        # both stop at the same absolute residual: check it in FP64 here
-        for x in (x0, x1):
+        assert st0 == 0 and st1 == 0 and stw == 0
+        # all stop at the same absolute residual: check it in FP64 here
+        for x in (x0, x1, xw):
             r = b - apply7(rec["opr"], x)
             # the PCG stops on its recurrence residual; the true one may drift a little
             assert float(r.abs().max()) <= 1.5e-10 * float(b.abs().max())
         its0.append(it0)
         its1.append(it1)
+        itsw.append(itw)
+    print("iterations zero / warm / learned:", its0, itsw, its1)
     assert np.mean(its1) < np.mean(its0), (its0, its1)
 
 

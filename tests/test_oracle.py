@@ -245,3 +245,21 @@ def test_golden_fixtures(name):
 def P_hash(pb):
     from tests.golden.make_golden import problem_sha
     return problem_sha(pb)
+
+
+def test_pivots_of_high_contrast_singular_coarse_matrix():
+    """The first step of the two-phase drop sequence at 128^3 (triply periodic,
+    density ratio 1000): the 4^3 coarsest matrix is singular; its round-off
+    pivot (~2e-14 of the largest) must be pinned, and it must be the only one
+    (the genuine pivots stay above 1e-3 of the largest)."""
+    import torch
+    from nga2_b200 import sequence as SQ
+    seq = SQ.DropSequence(128, seed=5, noise=1e-3)
+    oprs = []
+    seq.step(lambda opr, rhs: (oprs.append(opr.numpy().copy()), torch.zeros_like(rhs))[1])
+    o = OracleBBMG(128, 128, 128, True, True, True, method=PCG_BBOX, release=True)
+    o.setup(P.STC7, oprs[0])
+    _, LU, _, _ = o.direct()
+    d = np.sort(np.abs(np.diag(LU)))
+    assert o.npinned == 1
+    assert d[0] / d[-1] < 1e-12 and d[1] / d[-1] > 1e-3
