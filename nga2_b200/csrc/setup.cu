@@ -428,17 +428,19 @@ __global__ void k_lu(double *__restrict__ A, int n, int *__restrict__ piv, int *
 // for every interior cell whose neighbour is interior or a periodic image
 // (a coupling to a non-periodic overlap cell multiplies a zero value either
 // way).  Clears *flag on the first mismatch.
+// rows (j,k) on the y dimension of the grid, i on x: no 64-bit index division;
+// one flag update per warp that saw a mismatch
 __global__ void k_check_sym7(Lay L, const double *__restrict__ opr, int *flag) {
-    const long long total = (long long)L.nx * L.ny * L.nz;
-    for (long long t = gtid(); t < total; t += gstride()) {
-        int i, j, k;
-        interior_cell(L, t, i, j, k);
-        const long long id = L.idx(i, j, k);
-        bool ok = true;
-        if (i > 0 || L.xper) ok = ok && opr[q27(-1, 0, 0) * L.plane + id] == opr[q27(1, 0, 0) * L.plane + L.idx(i - 1, j, k)];
-        if (j > 0 || L.yper) ok = ok && opr[q27(0, -1, 0) * L.plane + id] == opr[q27(0, 1, 0) * L.plane + L.idx(i, j - 1, k)];
-        if (k > 0 || L.zper) ok = ok && opr[q27(0, 0, -1) * L.plane + id] == opr[q27(0, 0, 1) * L.plane + L.idx(i, j, k - 1)];
-        if (!ok) atomicAnd(flag, 0);
+    for (int row = blockIdx.y * blockDim.y + threadIdx.y; row < L.ny * L.nz; row += gridDim.y * blockDim.y) {
+        const int j = row % L.ny, k = row / L.ny;
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L.nx; i += gridDim.x * blockDim.x) {
+            const long long id = L.idx(i, j, k);
+            bool ok = true;
+            if (i > 0 || L.xper) ok = ok && opr[q27(-1, 0, 0) * L.plane + id] == opr[q27(1, 0, 0) * L.plane + L.idx(i - 1, j, k)];
+            if (j > 0 || L.yper) ok = ok && opr[q27(0, -1, 0) * L.plane + id] == opr[q27(0, 1, 0) * L.plane + L.idx(i, j - 1, k)];
+            if (k > 0 || L.zper) ok = ok && opr[q27(0, 0, -1) * L.plane + id] == opr[q27(0, 0, 1) * L.plane + L.idx(i, j, k - 1)];
+            if (!ok) atomicAnd(flag, 0);
+        }
     }
 }
 
@@ -507,7 +509,12 @@ cudaError_t setup_operator(const Lay &F, const Lay &C, const double *oprF, const
 
 cudaError_t check_symmetric7(const Lay &L, const double *opr, int *flag, cudaStream_t s) {
     long long n = (long long)L.nx * L.ny * L.nz;
-    k_check_sym7<<<grid_for(n, 256), 256, 0, s>>>(L, opr, flag);
+    (void)n;
+    const int bx = L.nx >= 64 ? 64 : 32, by = 256 / bx;
+    const int gx = (L.nx + bx - 1) / bx;
+    long long gy = ((long long)L.ny * L.nz + by - 1) / by;
+    if (gy > 65535) gy = 65535;
+    k_check_sym7<<<dim3(gx, (unsigned)gy), dim3(bx, by), 0, s>>>(L, opr, flag);
     BB_LAUNCH_CHECK();
     return cudaSuccess;
 }

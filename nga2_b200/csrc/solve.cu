@@ -14,6 +14,8 @@
 // points of one half-row (16-byte vector loads); neighbour offsets that are
 // not a multiple of VW (the odd x-neighbour) fall back to scalar loads that
 // hit the lines the aligned loads just brought in.
+#include <cstdlib>
+
 #include "setup.cuh"
 
 namespace bbmg {
@@ -233,6 +235,12 @@ __global__ void __launch_bounds__(256) k_relax_phase7(Lay L, const T *__restrict
     }
 }
 
+// 16-byte asynchronous global -> shared copy (cp.async, L1 bypassed).
+__device__ __forceinline__ void cp16(float *dst, const float *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+
 // Residual r = f - sum_l opr(l) v(nbr) on the interior, periodic images
 // written (bbmg_class.f90:831-844).  With f == nullptr the kernel returns the
 // operator product itself.
@@ -264,6 +272,67 @@ __global__ void __launch_bounds__(256) k_residual(Lay L, NbrOff nb, const T *__r
     FOR_ROWS(L.ny * L.nz) {
         const int j = row % L.ny, k = row / L.ny;
         FOR_CHUNKS(L.nx) residual_point<T, NPT>(L, nb.off[0], nb.off[1], opr, v, f, r, x_of(L, ch), j, k);
+    }
+}
+
+// Residual of the FP32 symmetric 7-point level (planes D, E, N, T) with its
+// operands staged in shared memory: one warp per (j,k) row; the 24 segments
+// (both x-halves of D, E, N, T, f, v of the row, N and v of row j-1, v of row
+// j+1, T and v of plane k-1, v of plane k+1) are copied with 16-byte cp.async,
+// each from 4 elements before the half-row to 4 after it, so the i-1 / i+1
+// neighbours (other half, overlap included) are on chip.  Same terms in the
+// same order as residual_point: identical bits.
+__global__ void __launch_bounds__(128) k_residual_staged(Lay L, const float *__restrict__ opr,
+                                                          const float *__restrict__ v, const float *__restrict__ f,
+                                                          float *__restrict__ r, int na) {
+    pdl_entry();
+    extern __shared__ float smf[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int seg = na + 8;
+    float *S = smf + (size_t)warp * 24 * seg;
+    const long long P = L.plane;
+    const int nrows = L.ny * L.nz;
+    for (int row = blockIdx.x * 4 + warp; row < nrows; row += gridDim.x * 4) {
+        const int j = row % L.ny, k = row / L.ny;
+        const long long r0 = L.G + L.row(j, k) * L.P;
+        const long long rjm = L.G + L.row(j - 1, k) * L.P, rjp = L.G + L.row(j + 1, k) * L.P;
+        const long long rkm = L.G + L.row(j, k - 1) * L.P, rkp = L.G + L.row(j, k + 1) * L.P;
+        __syncwarp();
+#pragma unroll
+        for (int h = 0; h < 2; h++) {  // h = 0: odd-x half (offset 0), h = 1: even-x half (offset B0)
+            const long long hb = (h ? L.B0 : 0) - 4;
+            const float *src[12] = {opr + r0 + hb,         opr + P + r0 + hb,     opr + 2 * P + r0 + hb,
+                                    opr + 3 * P + r0 + hb, f + r0 + hb,           v + r0 + hb,
+                                    opr + 2 * P + rjm + hb, v + rjm + hb,         v + rjp + hb,
+                                    opr + 3 * P + rkm + hb, v + rkm + hb,         v + rkp + hb};
+#pragma unroll
+            for (int q = 0; q < 12; q++)
+                for (int e = lane * 4; e < seg; e += 128) cp16(S + (h * 12 + q) * seg + e, src[q] + e);
+        }
+        asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+        __syncwarp();
+        // segment q of half h at S[(12 h + q) seg + 4 + position]
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const float *Sh = S + h * 12 * seg + 4, *So = S + (1 - h) * 12 * seg + 4;
+            // x-neighbours in the other half: odd point a (i = 2a+1) has i-1 at even a, i+1 at even a+1;
+            // even point a (i = 2a) has i-1 at odd a-1, i+1 at odd a
+            const int om = h ? -1 : 0, op = h ? 0 : 1;
+            for (int a = lane; a < na; a += 32) {  // lane-strided: conflict-free shared loads
+                float sum = 0.f;
+                sum = fmaf(Sh[9 * seg + a], Sh[10 * seg + a], sum);          // B: T(k-1) v(k-1)
+                sum = fmaf(Sh[6 * seg + a], Sh[7 * seg + a], sum);           // S: N(j-1) v(j-1)
+                sum = fmaf(So[1 * seg + a + om], So[5 * seg + a + om], sum); // W: E(i-1) v(i-1)
+                sum = fmaf(Sh[0 * seg + a], Sh[5 * seg + a], sum);           // C: D v
+                sum = fmaf(Sh[1 * seg + a], So[5 * seg + a + op], sum);      // E: E(i) v(i+1)
+                sum = fmaf(Sh[2 * seg + a], Sh[8 * seg + a], sum);           // N: N(i) v(j+1)
+                sum = fmaf(Sh[3 * seg + a], Sh[11 * seg + a], sum);          // T: T(i) v(k+1)
+                const float out = Sh[4 * seg + a] - sum;
+                r[r0 + (h ? L.B0 : 0) + a] = out;
+                const int i = h ? 2 * a : 2 * a + 1;
+                if (on_periodic_face(L, i, j, k)) write_images(L, r, i, j, k, out);
+            }
+        }
     }
 }
 
@@ -344,6 +413,149 @@ __global__ void __launch_bounds__(256) k_prolong(Lay F, Lay C, const T *__restri
     FOR_ROWS(F.ny * F.nz) {
         const int j = row % F.ny, k = row / F.ny;
         FOR_CHUNKS(F.nx) prolong_point<T>(F, C, c2f, vC, vF, x_of(F, ch), j, k);
+    }
+}
+
+// Restriction of an FP32 level with an even x size into the next coarser one,
+// operands staged in shared memory: one warp per coarse (cj,ck) row.  For each
+// of the 9 fine rows (2cj+rj, 2ck+rk) it copies both x-halves of r_f and the
+// three weight planes a coarse point reads there (even half: q8(0,pj,pk) for
+// ri = 0; odd half: q8(0,pj,pk) for ri = +1 and q8(1,pj,pk) for ri = -1,
+// pj = (1-rj)/2, pk = (1-rk)/2), each from 4 elements before the half-row to
+// 4 after it.  Same terms in the same order as restrict_point.
+__global__ void __launch_bounds__(128) k_restrict_staged(Lay F, Lay C, const float *__restrict__ c2f,
+                                                          const float *__restrict__ rF, float *__restrict__ fC,
+                                                          float *__restrict__ vC, int na) {
+    pdl_entry();
+    extern __shared__ float smf[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int seg = na + 8;
+    float *S = smf + (size_t)warp * 45 * seg;
+    const long long P = F.plane;
+    const int nrows = C.ny * C.nz;
+    for (int row = blockIdx.x * 4 + warp; row < nrows; row += gridDim.x * 4) {
+        const int cj = row % C.ny, ck = row / C.ny;
+        const int fj = 2 * cj, fk = 2 * ck;
+        const int rk0 = -pmod(F.zper, fk - 1, F.nz), rk1 = pmod(F.zper, fk + 1, F.nz);
+        const int rj0 = -pmod(F.yper, fj - 1, F.ny), rj1 = pmod(F.yper, fj + 1, F.ny);
+        __syncwarp();
+        for (int rk = -1; rk <= 1; rk++)
+            for (int rj = -1; rj <= 1; rj++) {
+                const int b = 5 * ((rk + 1) * 3 + (rj + 1));
+                const int pj = (1 - rj) / 2, pk = (1 - rk) / 2;
+                const long long fr = F.G + F.row(fj + rj, fk + rk) * F.P - 4;
+                for (int e = lane * 4; e < seg; e += 128) {
+                    cp16(S + (b + 0) * seg + e, rF + fr + e);                              // r odd half
+                    cp16(S + (b + 1) * seg + e, rF + fr + F.B0 + e);                       // r even half
+                    cp16(S + (b + 2) * seg + e, c2f + q8(0, pj, pk) * P + fr + F.B0 + e);  // ri = 0
+                    cp16(S + (b + 3) * seg + e, c2f + q8(0, pj, pk) * P + fr + e);         // ri = +1
+                    cp16(S + (b + 4) * seg + e, c2f + q8(1, pj, pk) * P + fr + e);         // ri = -1
+                }
+            }
+        asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+        __syncwarp();
+        for (int c0 = lane; c0 < C.nx; c0 += 32) {  // lane-strided coarse points
+            {
+                const int ci = c0;
+                const int fi = 2 * ci;
+                const int ri0 = -pmod(F.xper, fi - 1, F.nx), ri1 = pmod(F.xper, fi + 1, F.nx);
+                float sum = 0.f;
+#pragma unroll
+                for (int rk = -1; rk <= 1; rk++)
+#pragma unroll
+                    for (int rj = -1; rj <= 1; rj++)
+#pragma unroll
+                        for (int ri = -1; ri <= 1; ri++) {
+                            if (rk < rk0 || rk > rk1 || rj < rj0 || rj > rj1 || ri < ri0 || ri > ri1) continue;
+                            const float *Sb = S + 5 * ((rk + 1) * 3 + (rj + 1)) * seg + 4;
+                            // fi = 2ci: even position ci; fi+1: odd ci; fi-1: odd ci-1
+                            const float w = ri == 0 ? Sb[2 * seg + ci] : (ri > 0 ? Sb[3 * seg + ci] : Sb[4 * seg + ci - 1]);
+                            const float rv = ri == 0 ? Sb[seg + ci] : (ri > 0 ? Sb[ci] : Sb[ci - 1]);
+                            sum = fmaf(w, rv, sum);
+                        }
+                const long long cid = C.idx(ci, cj, ck);
+                fC[cid] = sum;
+                vC[cid] = 0.f;
+                if (on_periodic_face(C, ci, cj, ck)) {
+                    write_images(C, fC, ci, cj, ck, sum);
+                    write_images(C, vC, ci, cj, ck, 0.f);
+                }
+            }
+        }
+    }
+}
+
+// Prolongation + correction of an FP32 level with an even x size, operands
+// staged in shared memory: one warp per fine (j,k) row.  It copies both x-halves
+// of v_f, the weight planes the row's parity class uses (q8(pi,pj,pk) with
+// pj <= j&1, pk <= k&1; the even half only needs pi = 0) and both x-halves of
+// the (up to four) coarse rows it interpolates from, then applies
+// prolong_point's sum term for term.  Requires na = nx/2 (the coarse x size)
+// to be a multiple of 8, so every copied segment is 16-byte aligned.
+__global__ void __launch_bounds__(128) k_prolong_staged(Lay F, Lay C, const float *__restrict__ c2f,
+                                                         const float *__restrict__ vC, float *__restrict__ vF,
+                                                         int na) {
+    pdl_entry();
+    extern __shared__ float smf[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int seg = na + 8;
+    float *S = smf + (size_t)warp * 22 * seg;
+    // segments: 0,1 v_f odd/even half; 2 + 3*(pj+2pk) + {0: even pi=0, 1: odd pi=0, 2: odd pi=1};
+    // 14 + 2*(pj+2pk) + {0: coarse odd half, 1: coarse even half}
+    const long long P = F.plane;
+    const int nrows = F.ny * F.nz;
+    for (int row = blockIdx.x * 4 + warp; row < nrows; row += gridDim.x * 4) {
+        const int j = row % F.ny, k = row / F.ny;
+        const int n2 = j & 1, n3 = k & 1, cj = j >> 1, ck = k >> 1;
+        const long long r0 = F.G + F.row(j, k) * F.P;
+        __syncwarp();
+        for (int e = lane * 4; e < na; e += 128) {
+            cp16(S + e, vF + r0 + e);
+            cp16(S + seg + e, vF + r0 + F.B0 + e);
+        }
+        for (int pk = 0; pk <= n3; pk++)
+            for (int pj = 0; pj <= n2; pj++) {
+                const int b = 2 + 3 * (pj + 2 * pk);
+                const long long cr = C.G + C.row(cj + pj, ck + pk) * C.P;
+                for (int e = lane * 4; e < na; e += 128) {
+                    cp16(S + b * seg + e, c2f + q8(0, pj, pk) * P + r0 + F.B0 + e);
+                    cp16(S + (b + 1) * seg + e, c2f + q8(0, pj, pk) * P + r0 + e);
+                    cp16(S + (b + 2) * seg + e, c2f + q8(1, pj, pk) * P + r0 + e);
+                }
+                // coarse odd half: positions < C.nx/2; even half: <= C.nx/2 (overlap
+                // included); both copied up to the next multiple of 4 above C.nx/2
+                const int cb = 14 + 2 * (pj + 2 * pk), ccl = ((C.nx >> 1) + 4) & ~3;
+                for (int e = lane * 4; e < ccl; e += 128) {
+                    cp16(S + cb * seg + e, vC + cr + e);
+                    cp16(S + (cb + 1) * seg + e, vC + cr + C.B0 + e);
+                }
+            }
+        asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+        __syncwarp();
+#pragma unroll
+        for (int h = 0; h < 2; h++) {  // h = 0: odd-x fine points (n1 = 1), h = 1: even-x (n1 = 0)
+            const int n1 = 1 - h;
+            for (int a = lane; a < na; a += 32) {  // lane-strided: conflict-free shared loads
+                const int i = h ? 2 * a : 2 * a + 1, ci = i >> 1;
+                float ev = 0.f;
+#pragma unroll
+                for (int pk = 0; pk <= 1; pk++)
+#pragma unroll
+                    for (int pj = 0; pj <= 1; pj++)
+#pragma unroll
+                        for (int pi = 0; pi <= 1; pi++) {
+                            if (pk > n3 || pj > n2 || pi > n1) continue;
+                            const int b = 2 + 3 * (pj + 2 * pk) + (h ? 0 : 1 + pi);
+                            const int cx = ci + pi, cb = 14 + 2 * (pj + 2 * pk);
+                            // coarse x-split: odd cx at odd-half position (cx-1)/2, even at even-half cx/2
+                            const float vc = (cx & 1) ? S[cb * seg + ((cx - 1) >> 1)] : S[(cb + 1) * seg + (cx >> 1)];
+                            ev = fmaf(S[b * seg + a], vc, ev);
+                        }
+                const float out = S[h * seg + a] + ev;
+                vF[r0 + (h ? F.B0 : 0) + a] = out;
+                if (on_periodic_face(F, i, j, k)) write_images(F, vF, i, j, k, out);
+            }
+        }
     }
 }
 
@@ -739,6 +951,14 @@ static PhaseCols phase_cols(const Lay &L, const NbrOff &nb, int w, int vw_cap, i
     return p;
 }
 
+// the shared-memory-staged FP32 kernels (residual, restriction, prolongation)
+// serve levels whose half-rows hold a multiple of 4 points (nx even), unless
+// BBMG_NO_STAGED is set (then the register kernels run: same bits)
+static bool use_staged(const Lay &L) {
+    static const bool off = getenv("BBMG_NO_STAGED") != nullptr;
+    return !off && !(L.nx & 1) && (L.nx >> 1) % 4 == 0;
+}
+
 template <typename T, int NPT>
 static cudaError_t launch_phase(const Lay &L, const PhaseCols &pc, int vw, long long rows, int chunks, const T *opr,
                                 T *v, const T *f, cudaStream_t s) {
@@ -787,6 +1007,24 @@ cudaError_t launch_relax_sweeps(const Lay &L, const NbrOff &nb, int npt, bool fu
 template <typename T>
 cudaError_t launch_residual(const Lay &L, const NbrOff &nb, int npt, const T *opr, const T *v, const T *f, T *r,
                             cudaStream_t s) {
+    if constexpr (sizeof(T) == 4) {
+        const int na = L.nx >> 1;
+        const size_t smem = sizeof(float) * 24 * (size_t)(na + 8) * 4;
+        if (npt == 4 && f && use_staged(L) && smem <= 200 * 1024) {
+            static bool attr = false;
+            if (!attr && smem > 48 * 1024) {
+                cudaError_t e = cudaFuncSetAttribute(k_residual_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     200 * 1024);
+                if (e != cudaSuccess) return e;
+                attr = true;
+            }
+            long long gx = ((long long)L.ny * L.nz + 3) / 4;
+            if (gx > 148LL * 16) gx = 148LL * 16;
+            BB_CHECK_LAUNCH((launch_k(k_residual_staged, dim3((unsigned)gx), dim3(128), smem, s, L,
+                                      (const float *)opr, (const float *)v, (const float *)f, (float *)r, na)));
+            return cudaSuccess;
+        }
+    }
     const Geo g = geo_rows(L.nx, (long long)L.ny * L.nz);
     if (npt == 4) BB_CHECK_LAUNCH((launch_k(k_residual<T, 4>, g.grid, g.block, 0, s, L, nb, opr, v, f, r)));
     else if (npt == 7) BB_CHECK_LAUNCH((launch_k(k_residual<T, 7>, g.grid, g.block, 0, s, L, nb, opr, v, f, r)));
@@ -796,6 +1034,24 @@ cudaError_t launch_residual(const Lay &L, const NbrOff &nb, int npt, const T *op
 
 template <typename T>
 cudaError_t launch_restrict(const Lay &F, const Lay &C, const T *c2f, const T *rF, T *fC, T *vC, cudaStream_t s) {
+    if constexpr (sizeof(T) == 4) {
+        const int na = F.nx >> 1;
+        const size_t smem = sizeof(float) * 45 * (size_t)(na + 8) * 4;
+        if (use_staged(F) && C.nx == na && smem <= 200 * 1024) {
+            static bool attr = false;
+            if (!attr && smem > 48 * 1024) {
+                cudaError_t e = cudaFuncSetAttribute(k_restrict_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     200 * 1024);
+                if (e != cudaSuccess) return e;
+                attr = true;
+            }
+            long long gx = ((long long)C.ny * C.nz + 3) / 4;
+            if (gx > 148LL * 16) gx = 148LL * 16;
+            BB_CHECK_LAUNCH((launch_k(k_restrict_staged, dim3((unsigned)gx), dim3(128), smem, s, F, C,
+                                      (const float *)c2f, (const float *)rF, (float *)fC, (float *)vC, na)));
+            return cudaSuccess;
+        }
+    }
     const Geo g = geo_rows(C.nx, (long long)C.ny * C.nz);
     BB_CHECK_LAUNCH((launch_k(k_restrict<T>, g.grid, g.block, 0, s, F, C, c2f, rF, fC, vC)));
     return cudaSuccess;
@@ -803,6 +1059,25 @@ cudaError_t launch_restrict(const Lay &F, const Lay &C, const T *c2f, const T *r
 
 template <typename T>
 cudaError_t launch_prolong(const Lay &F, const Lay &C, const T *c2f, const T *vC, T *vF, cudaStream_t s) {
+    if constexpr (sizeof(T) == 4) {
+        const int na = F.nx >> 1;
+        const size_t smem = sizeof(float) * 22 * (size_t)(na + 8) * 4;
+        // coarse half-rows (x size nx/2, overlap included) fit in na + 8 elements
+        if (use_staged(F) && C.nx == na && (C.nx % 8) == 0 && smem <= 200 * 1024) {
+            static bool attr = false;
+            if (!attr && smem > 48 * 1024) {
+                cudaError_t e = cudaFuncSetAttribute(k_prolong_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     200 * 1024);
+                if (e != cudaSuccess) return e;
+                attr = true;
+            }
+            long long gx = ((long long)F.ny * F.nz + 3) / 4;
+            if (gx > 148LL * 16) gx = 148LL * 16;
+            BB_CHECK_LAUNCH((launch_k(k_prolong_staged, dim3((unsigned)gx), dim3(128), smem, s, F, C,
+                                      (const float *)c2f, (const float *)vC, (float *)vF, na)));
+            return cudaSuccess;
+        }
+    }
     const Geo g = geo_rows(F.nx, (long long)F.ny * F.nz);
     BB_CHECK_LAUNCH((launch_k(k_prolong<T>, g.grid, g.block, 0, s, F, C, c2f, vC, vF)));
     return cudaSuccess;

@@ -90,23 +90,23 @@ def assemble_operator(xn, yn, zn, per, rho=None):
         dzmi = dzmi.copy(); dzmi[0] = 0.0; dzmi[-1] = 0.0
     vol = (dx[None, None, :] * dy[None, :, None]) * dz[:, None, None]
 
-    def face_inv_rho(axis, n):
-        # 1/rho on faces 1..n+1 along axis (face f sits between cells f-1 and f)
+    def face_rho(axis, n):
+        # rho on faces 1..n+1 along axis (face f sits between cells f-1 and f),
+        # the arithmetic mean of the two cells (the staggered rho_U of tpns)
         if rho is None:
             return None
         r = np.moveaxis(rho, axis, -1)
         lo = np.concatenate([r[..., -1:], r], axis=-1)       # cell f-1 (periodic wrap at f=1)
         hi = np.concatenate([r, r[..., :1]], axis=-1)        # cell f
-        rf = 0.5 * (lo + hi)
-        return np.moveaxis(1.0 / rf, -1, axis)
+        return np.moveaxis(0.5 * (lo + hi), -1, axis)
 
     opr = np.empty((nz, ny, nx, 7))
     # x: per-direction east/west contributions (tpns_class.f90:1571-1584)
-    irx = face_inv_rho(2, nx)
-    iry = face_inv_rho(1, ny)
-    irz = face_inv_rho(0, nz)
+    rfx = face_rho(2, nx)
+    rfy = face_rho(1, ny)
+    rfz = face_rho(0, nz)
 
-    def terms(di, dmi_lo, dmi_hi, ir, axis):
+    def terms(di, dmi_lo, dmi_hi, rf, axis):
         # divp(1)*divu(-1,i+1), divp(0)*divu(0,i), divp(1)*divu(0,i+1), divp(0)*divu(-1,i)
         shp = [1, 1, 1]
         shp[axis] = -1
@@ -115,17 +115,18 @@ def assemble_operator(xn, yn, zn, per, rho=None):
         w_diag = (-di) * lo
         e_off = di * hi
         w_off = (-di) * (-lo)
-        if ir is not None:
+        if rf is not None:
+            # each face term divided by the face density (tpns_class.f90:1571-1584)
             sl_hi = [slice(None)] * 3; sl_hi[axis] = slice(1, None)
             sl_lo = [slice(None)] * 3; sl_lo[axis] = slice(0, -1)
-            rhi, rlo = ir[tuple(sl_hi)], ir[tuple(sl_lo)]
+            rhi, rlo = rf[tuple(sl_hi)], rf[tuple(sl_lo)]
             e_diag = e_diag / rhi; w_diag = w_diag / rlo
             e_off = e_off / rhi; w_off = w_off / rlo
         return e_diag, w_diag, e_off, w_off
 
-    xe, xw, xo_e, xo_w = terms(dxi, dxmi[:-1], dxmi[1:], irx, 2)
-    ye, yw, yo_e, yo_w = terms(dyi, dymi[:-1], dymi[1:], iry, 1)
-    ze, zw, zo_e, zo_w = terms(dzi, dzmi[:-1], dzmi[1:], irz, 0)
+    xe, xw, xo_e, xo_w = terms(dxi, dxmi[:-1], dxmi[1:], rfx, 2)
+    ye, yw, yo_e, yo_w = terms(dyi, dymi[:-1], dymi[1:], rfy, 1)
+    ze, zw, zo_e, zo_w = terms(dzi, dzmi[:-1], dzmi[1:], rfz, 0)
     full = (nz, ny, nx)
     opr[..., 0] = np.broadcast_to(((((xe + xw) + ye) + yw) + ze) + zw, full)
     opr[..., 1] = np.broadcast_to(xo_e, full)

@@ -1,0 +1,31 @@
+"""Helper of tests/test_gpu_parity.py::test_staged_fp32_relax_matches_register_kernel:
+run FP32 level-1 relaxation sweeps, a residual, a restriction and a
+prolongation on a fixed symmetric problem and save the results, so the staged
+and the register kernels (BBMG_NO_STAGED) can be compared bit for bit across
+two processes."""
+import sys
+
+import numpy as np
+
+from nga2_b200 import problems as P
+from nga2_b200.bbmg import BBMG, MIXED, PCG_BBOX
+
+n, out = int(sys.argv[1]), sys.argv[2]
+pb = P.drops_poisson(n, seed=4, ndrops=6, rmin=2.0, rmax=5.0)  # n a power of 2: exactly symmetric
+g = BBMG(n, n, n, pb.xper, pb.yper, pb.zper, method=PCG_BBOX, precision=MIXED)
+g.setup(pb.stc, pb.opr)
+assert g.info["level1_stencil"] == 4
+rng = np.random.default_rng(3)
+shp = (n + 2, n + 2, n + 2)
+g.put(1, "v", rng.standard_normal(shp), prec=1)
+g.put(1, "f", rng.standard_normal(shp), prec=1)
+for d in (1, -1, 1):
+    g.step("relax", 1, d, prec=1)
+g.step("residual", 1, 0, prec=1)
+r1 = g.get(1, "r", prec=1)
+g.step("restrict", 1, 0, prec=1)
+f2 = g.get(2, "f", prec=1)
+nx2, ny2, nz2 = g.level_dims(2)
+g.put(2, "v", rng.standard_normal((nz2 + 2, ny2 + 2, nx2 + 2)), prec=1)
+g.step("prolong", 1, 0, prec=1)
+np.savez(out, v=g.get(1, "v", prec=1), r=r1, f2=f2)

@@ -253,5 +253,26 @@ def test_residual_norm_rhs(method, precision):
     _, it_rhs, rerr_rhs, st_rhs = g.solve(pb.rhs, guess.copy())
     g.set_residual_norm(NORM_GUESS)
     _, it_ref, rerr_ref, st_ref = g.solve(pb.rhs, guess.copy())
-    assert st_rhs == 0 and st_ref == 0 and rerr_rhs <= 1e-10
+    # under the reference's rerr the guess's residual must drop another 1e-10,
+    # which can lie below the FP64 floor: MAXIT is then the honest outcome
+    assert st_rhs == 0 and rerr_rhs <= 1e-10 and st_ref in (0, 1)
     assert it_rhs < it_ref and it_rhs < it0, (it_rhs, it_ref, it0)
+
+
+@pytest.mark.parametrize("n", [32, 64])
+def test_staged_fp32_relax_matches_register_kernel(n, tmp_path):
+    """The shared-memory-staged FP32 residual, restriction and prolongation of
+    level 1 give the same bits as the register kernels they replace (run in a
+    second process with BBMG_NO_STAGED=1)."""
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    probe = os.path.join(root, "tests", "fp32_relax_probe.py")
+    env = dict(os.environ, PYTHONPATH=root)
+    a, b = str(tmp_path / "staged.npz"), str(tmp_path / "register.npz")
+    subprocess.run([sys.executable, probe, str(n), a], check=True, env=env)
+    env["BBMG_NO_STAGED"] = "1"
+    subprocess.run([sys.executable, probe, str(n), b], check=True, env=env)
+    za, zb = np.load(a), np.load(b)
+    for key in ("v", "r", "f2"):
+        assert np.array_equal(za[key], zb[key]), key
