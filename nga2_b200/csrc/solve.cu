@@ -241,6 +241,67 @@ __device__ __forceinline__ void cp16(float *dst, const float *src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
 }
 
+// One colour of the FP32 27-point Gauss-Seidel with its operands staged in
+// shared memory: one warp per half-row of the colour.  It copies the 27
+// coefficient planes and f at its points, and for each of the 9 rows
+// (j+dy, k+dz) the v values of its own x-half (not for the row itself: v(i)
+// is not read) and of the other x-half (from 4 elements before to 4 after,
+// for the i-1 / i+1 neighbours), then updates its points term for term as
+// gs_points does (column-major order, centre last): identical bits.
+// Requires na (points per half-row) to be a multiple of 4.
+__global__ void __launch_bounds__(128) k_relax27_staged(Lay L, const float *__restrict__ opr, float *v,
+                                                         const float *__restrict__ f, int px, int py, int pz,
+                                                         int fuse, int na) {
+    pdl_entry();
+    extern __shared__ float smf[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int seg = na + 8;
+    float *S = smf + (size_t)warp * 46 * seg;
+    // segments: 0..26 coefficient planes; 27 f; 28 + 2*(row) own half v, 29 + 2*(row) other half v,
+    // row = (dy+1) + 3*(dz+1)
+    const int nb = (L.ny - py + 1) >> 1, nc = (L.nz - pz + 1) >> 1;
+    const int nrows = nb * nc;
+    const long long hown = px ? 0 : L.B0, hoth = px ? L.B0 : 0;
+    const long long P = L.plane;
+    const int om = px ? 4 : 3, op = px ? 5 : 4;  // other-half index of i-1 / i+1 (slack 4)
+    for (int row = blockIdx.x * 4 + warp; row < nrows; row += gridDim.x * 4) {
+        const int j = py + 2 * (row % nb), k = pz + 2 * (row / nb);
+        const long long r0 = L.G + L.row(j, k) * L.P;
+        __syncwarp();
+        for (int e = lane * 4; e < na; e += 128) {
+#pragma unroll
+            for (int q = 0; q < 27; q++) cp16(S + q * seg + e, opr + q * P + r0 + hown + e);
+            cp16(S + 27 * seg + e, f + r0 + hown + e);
+        }
+#pragma unroll
+        for (int rr = 0; rr < 9; rr++) {
+            const int dy = rr % 3 - 1, dz = rr / 3 - 1;
+            const long long rb = L.G + L.row(j + dy, k + dz) * L.P;
+            for (int e = lane * 4; e < seg; e += 128) {
+                if (rr != 4 && e < na) cp16(S + (28 + 2 * rr) * seg + e, v + rb + hown + e);
+                cp16(S + (29 + 2 * rr) * seg + e, v + rb + hoth - 4 + e);
+            }
+        }
+        asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+        __syncwarp();
+        for (int a = lane; a < na; a += 32) {
+            float sum = 0.f;
+#pragma unroll
+            for (int q = 0; q < 27; q++) {
+                if (q == 13) continue;
+                const int dx = q % 3 - 1, rr = q / 3;  // rr = (dy+1) + 3 (dz+1)
+                const float vv = dx == 0 ? S[(28 + 2 * rr) * seg + a]
+                                         : S[(29 + 2 * rr) * seg + a + (dx < 0 ? om : op)];
+                sum = fmaf(S[q * seg + a], vv, sum);
+            }
+            const float out = (S[27 * seg + a] - sum) / (S[13 * seg + a] + (float)kEps);
+            v[r0 + hown + a] = out;
+            const int i = px + 2 * a;
+            if (fuse && on_periodic_face(L, i, j, k)) write_images(L, v, i, j, k, out);
+        }
+    }
+}
+
 // Residual r = f - sum_l opr(l) v(nbr) on the interior, periodic images
 // written (bbmg_class.f90:831-844).  With f == nullptr the kernel returns the
 // operator product itself.
@@ -888,10 +949,37 @@ template <> int vw_for<float>(int n) { return (n % 4 == 0) ? 4 : ((n % 2 == 0) ?
 template <> int vw_for<double>(int n) { return (n % 2 == 0) ? 2 : 1; }
 template <typename T> struct VwMax { static constexpr int value = sizeof(T) == 4 ? 4 : 2; };
 
+// the shared-memory-staged FP32 kernels (27-point colours, level-1 residual,
+// restriction, prolongation)
+// serve levels whose half-rows hold a multiple of 4 points (nx even), unless
+// BBMG_NO_STAGED is set (then the register kernels run: same bits)
+static bool use_staged(const Lay &L) {
+    static const bool off = getenv("BBMG_NO_STAGED") != nullptr;
+    return !off && !(L.nx & 1) && (L.nx >> 1) % 4 == 0;
+}
+
 template <typename T, int NPT>
 static cudaError_t launch_colour(const Lay &L, const Off27 &off, const T *opr, T *v, const T *f, int px, int py,
                                  int pz, int fuse, cudaStream_t s) {
     const int na = (L.nx - px + 1) >> 1;
+    if constexpr (sizeof(T) == 4 && NPT == 27) {
+        const size_t smem = sizeof(float) * 46 * (size_t)(na + 8) * 4;
+        if (use_staged(L) && smem <= 200 * 1024) {
+            static bool attr = false;
+            if (!attr && smem > 48 * 1024) {
+                cudaError_t e = cudaFuncSetAttribute(k_relax27_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     200 * 1024);
+                if (e != cudaSuccess) return e;
+                attr = true;
+            }
+            const long long nrows = (long long)((L.ny - py + 1) >> 1) * ((L.nz - pz + 1) >> 1);
+            long long gx = (nrows + 3) / 4;
+            if (gx > 148LL * 8) gx = 148LL * 8;
+            BB_CHECK_LAUNCH((launch_k(k_relax27_staged, dim3((unsigned)gx), dim3(128), smem, s, L,
+                                      (const float *)opr, (float *)v, (const float *)f, px, py, pz, fuse, na)));
+            return cudaSuccess;
+        }
+    }
     const long long nrows = (long long)((L.ny - py + 1) >> 1) * ((L.nz - pz + 1) >> 1);
     const int vw = vw_for<T>(na);
     const Geo g = geo_rows(na / vw, nrows);
@@ -951,13 +1039,6 @@ static PhaseCols phase_cols(const Lay &L, const NbrOff &nb, int w, int vw_cap, i
     return p;
 }
 
-// the shared-memory-staged FP32 kernels (residual, restriction, prolongation)
-// serve levels whose half-rows hold a multiple of 4 points (nx even), unless
-// BBMG_NO_STAGED is set (then the register kernels run: same bits)
-static bool use_staged(const Lay &L) {
-    static const bool off = getenv("BBMG_NO_STAGED") != nullptr;
-    return !off && !(L.nx & 1) && (L.nx >> 1) % 4 == 0;
-}
 
 template <typename T, int NPT>
 static cudaError_t launch_phase(const Lay &L, const PhaseCols &pc, int vw, long long rows, int chunks, const T *opr,
