@@ -302,6 +302,61 @@ __global__ void __launch_bounds__(128) k_relax27_staged(Lay L, const float *__re
     }
 }
 
+// Residual of an FP32 27-point level with its operands staged as in
+// k_relax27_staged: one warp per x-half of a (j,k) row (both halves of every
+// row, so blockIdx/warp walk 2 * ny * nz jobs); here the row's own v is copied
+// too and the centre term enters the sum in its column-major place, as in
+// residual_point: identical bits.
+__global__ void __launch_bounds__(128) k_residual27_staged(Lay L, const float *__restrict__ opr,
+                                                            const float *__restrict__ v, const float *__restrict__ f,
+                                                            float *__restrict__ r, int na) {
+    pdl_entry();
+    extern __shared__ float smf[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int seg = na + 8;
+    float *S = smf + (size_t)warp * 46 * seg;
+    const long long P = L.plane;
+    const int njobs = 2 * L.ny * L.nz;
+    for (int job = blockIdx.x * 4 + warp; job < njobs; job += gridDim.x * 4) {
+        const int px = job & 1, row = job >> 1;  // px = 1: odd-x half, 0: even-x half
+        const int j = row % L.ny, k = row / L.ny;
+        const long long hown = px ? 0 : L.B0, hoth = px ? L.B0 : 0;
+        const int om = px ? 4 : 3, op = px ? 5 : 4;
+        const long long r0 = L.G + L.row(j, k) * L.P;
+        __syncwarp();
+        for (int e = lane * 4; e < na; e += 128) {
+#pragma unroll
+            for (int q = 0; q < 27; q++) cp16(S + q * seg + e, opr + q * P + r0 + hown + e);
+            cp16(S + 27 * seg + e, f + r0 + hown + e);
+        }
+#pragma unroll
+        for (int rr = 0; rr < 9; rr++) {
+            const int dy = rr % 3 - 1, dz = rr / 3 - 1;
+            const long long rb = L.G + L.row(j + dy, k + dz) * L.P;
+            for (int e = lane * 4; e < seg; e += 128) {
+                if (e < na) cp16(S + (28 + 2 * rr) * seg + e, v + rb + hown + e);
+                cp16(S + (29 + 2 * rr) * seg + e, v + rb + hoth - 4 + e);
+            }
+        }
+        asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+        __syncwarp();
+        for (int a = lane; a < na; a += 32) {
+            float sum = 0.f;
+#pragma unroll
+            for (int q = 0; q < 27; q++) {
+                const int dx = q % 3 - 1, rr = q / 3;
+                const float vv = dx == 0 ? S[(28 + 2 * rr) * seg + a]
+                                         : S[(29 + 2 * rr) * seg + a + (dx < 0 ? om : op)];
+                sum = fmaf(S[q * seg + a], vv, sum);
+            }
+            const float out = S[27 * seg + a] - sum;
+            r[r0 + hown + a] = out;
+            const int i = px + 2 * a;
+            if (on_periodic_face(L, i, j, k)) write_images(L, r, i, j, k, out);
+        }
+    }
+}
+
 // Residual r = f - sum_l opr(l) v(nbr) on the interior, periodic images
 // written (bbmg_class.f90:831-844).  With f == nullptr the kernel returns the
 // operator product itself.
@@ -1090,6 +1145,21 @@ cudaError_t launch_residual(const Lay &L, const NbrOff &nb, int npt, const T *op
                             cudaStream_t s) {
     if constexpr (sizeof(T) == 4) {
         const int na = L.nx >> 1;
+        const size_t smem27 = sizeof(float) * 46 * (size_t)(na + 8) * 4;
+        if (npt == 27 && f && use_staged(L) && smem27 <= 200 * 1024) {
+            static bool attr27 = false;
+            if (!attr27 && smem27 > 48 * 1024) {
+                cudaError_t e = cudaFuncSetAttribute(k_residual27_staged,
+                                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+                if (e != cudaSuccess) return e;
+                attr27 = true;
+            }
+            long long gx = (2LL * L.ny * L.nz + 3) / 4;
+            if (gx > 148LL * 8) gx = 148LL * 8;
+            BB_CHECK_LAUNCH((launch_k(k_residual27_staged, dim3((unsigned)gx), dim3(128), smem27, s, L,
+                                      (const float *)opr, (const float *)v, (const float *)f, (float *)r, na)));
+            return cudaSuccess;
+        }
         const size_t smem = sizeof(float) * 24 * (size_t)(na + 8) * 4;
         if (npt == 4 && f && use_staged(L) && smem <= 200 * 1024) {
             static bool attr = false;

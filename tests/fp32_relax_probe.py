@@ -1,6 +1,7 @@
 """Helper of tests/test_gpu_parity.py::test_staged_fp32_relax_matches_register_kernel:
 run FP32 level-1 relaxation sweeps, a residual, a restriction, a
-prolongation and level-2 (27-point) relaxation sweeps on a fixed symmetric
+prolongation, level-2 (27-point) relaxation sweeps and a residual on a fixed
+symmetric
 problem and save the results, so the staged and the register kernels
 (BBMG_NO_STAGED) can be compared bit for bit across two processes."""
 import sys
@@ -33,4 +34,5 @@ v1 = g.get(1, "v", prec=1)
 g.put(2, "f", rng.standard_normal((nz2 + 2, ny2 + 2, nx2 + 2)), prec=1)
 for d in (1, -1):
     g.step("relax", 2, d, prec=1)
-np.savez(out, v=v1, r=r1, f2=f2, v2=g.get(2, "v", prec=1))
+g.step("residual", 2, 0, prec=1)
+np.savez(out, v=v1, r=r1, f2=f2, v2=g.get(2, "v", prec=1), r2=g.get(2, "r", prec=1))

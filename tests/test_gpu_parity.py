@@ -262,7 +262,7 @@ def test_residual_norm_rhs(method, precision):
 @pytest.mark.parametrize("n", [32, 64])
 def test_staged_fp32_relax_matches_register_kernel(n, tmp_path):
     """The shared-memory-staged FP32 kernels (level-1 residual, restriction and
-    prolongation, 27-point colours on level 2) give the same bits as the
+    prolongation, 27-point colours and residual on level 2) give the same bits as the
     register kernels they replace (run in a second process with
     BBMG_NO_STAGED=1)."""
     import subprocess
@@ -275,5 +275,5 @@ def test_staged_fp32_relax_matches_register_kernel(n, tmp_path):
     env["BBMG_NO_STAGED"] = "1"
     subprocess.run([sys.executable, probe, str(n), b], check=True, env=env)
     za, zb = np.load(a), np.load(b)
-    for key in ("v", "r", "f2", "v2"):
+    for key in ("v", "r", "f2", "v2", "r2"):
         assert np.array_equal(za[key], zb[key]), key
