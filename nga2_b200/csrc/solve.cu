@@ -236,7 +236,7 @@ __global__ void __launch_bounds__(256) k_relax_phase7(Lay L, const T *__restrict
 }
 
 // 16-byte asynchronous global -> shared copy (cp.async, L1 bypassed).
-__device__ __forceinline__ void cp16(float *dst, const float *src) {
+__device__ __forceinline__ void cp16(void *dst, const void *src) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
 }
@@ -249,14 +249,18 @@ __device__ __forceinline__ void cp16(float *dst, const float *src) {
 // for the i-1 / i+1 neighbours), then updates its points term for term as
 // gs_points does (column-major order, centre last): identical bits.
 // Requires na (points per half-row) to be a multiple of 4.
-__global__ void __launch_bounds__(128) k_relax27_staged(Lay L, const float *__restrict__ opr, float *v,
-                                                         const float *__restrict__ f, int px, int py, int pz,
+template <typename T>
+__global__ void __launch_bounds__(128) k_relax27_staged(Lay L, const T *__restrict__ opr, T *v,
+                                                         const T *__restrict__ f, int px, int py, int pz,
                                                          int fuse, int na) {
     pdl_entry();
-    extern __shared__ float smf[];
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T *smf = reinterpret_cast<T *>(smraw);
+    using O = Ops<T, ExactOf<T>::value>;
+    constexpr int EPC = 16 / sizeof(T);  // elements per 16-byte copy
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int seg = na + 8;
-    float *S = smf + (size_t)warp * 46 * seg;
+    T *S = smf + (size_t)warp * 46 * seg;
     // segments: 0..26 coefficient planes; 27 f; 28 + 2*(row) own half v, 29 + 2*(row) other half v,
     // row = (dy+1) + 3*(dz+1)
     const int nb = (L.ny - py + 1) >> 1, nc = (L.nz - pz + 1) >> 1;
@@ -268,7 +272,7 @@ __global__ void __launch_bounds__(128) k_relax27_staged(Lay L, const float *__re
         const int j = py + 2 * (row % nb), k = pz + 2 * (row / nb);
         const long long r0 = L.G + L.row(j, k) * L.P;
         __syncwarp();
-        for (int e = lane * 4; e < na; e += 128) {
+        for (int e = lane * EPC; e < na; e += 32 * EPC) {
 #pragma unroll
             for (int q = 0; q < 27; q++) cp16(S + q * seg + e, opr + q * P + r0 + hown + e);
             cp16(S + 27 * seg + e, f + r0 + hown + e);
@@ -277,7 +281,7 @@ __global__ void __launch_bounds__(128) k_relax27_staged(Lay L, const float *__re
         for (int rr = 0; rr < 9; rr++) {
             const int dy = rr % 3 - 1, dz = rr / 3 - 1;
             const long long rb = L.G + L.row(j + dy, k + dz) * L.P;
-            for (int e = lane * 4; e < seg; e += 128) {
+            for (int e = lane * EPC; e < seg; e += 32 * EPC) {
                 if (rr != 4 && e < na) cp16(S + (28 + 2 * rr) * seg + e, v + rb + hown + e);
                 cp16(S + (29 + 2 * rr) * seg + e, v + rb + hoth - 4 + e);
             }
@@ -285,16 +289,16 @@ __global__ void __launch_bounds__(128) k_relax27_staged(Lay L, const float *__re
         asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
         __syncwarp();
         for (int a = lane; a < na; a += 32) {
-            float sum = 0.f;
+            T sum = T(0);
 #pragma unroll
             for (int q = 0; q < 27; q++) {
                 if (q == 13) continue;
                 const int dx = q % 3 - 1, rr = q / 3;  // rr = (dy+1) + 3 (dz+1)
-                const float vv = dx == 0 ? S[(28 + 2 * rr) * seg + a]
+                const T vv = dx == 0 ? S[(28 + 2 * rr) * seg + a]
                                          : S[(29 + 2 * rr) * seg + a + (dx < 0 ? om : op)];
-                sum = fmaf(S[q * seg + a], vv, sum);
+                sum = O::mac(sum, S[q * seg + a], vv);
             }
-            const float out = (S[27 * seg + a] - sum) / (S[13 * seg + a] + (float)kEps);
+            const T out = O::div(O::sub(S[27 * seg + a], sum), O::add(S[13 * seg + a], T(kEps)));
             v[r0 + hown + a] = out;
             const int i = px + 2 * a;
             if (fuse && on_periodic_face(L, i, j, k)) write_images(L, v, i, j, k, out);
@@ -307,14 +311,18 @@ __global__ void __launch_bounds__(128) k_relax27_staged(Lay L, const float *__re
 // row, so blockIdx/warp walk 2 * ny * nz jobs); here the row's own v is copied
 // too and the centre term enters the sum in its column-major place, as in
 // residual_point: identical bits.
-__global__ void __launch_bounds__(128) k_residual27_staged(Lay L, const float *__restrict__ opr,
-                                                            const float *__restrict__ v, const float *__restrict__ f,
-                                                            float *__restrict__ r, int na) {
+template <typename T>
+__global__ void __launch_bounds__(128) k_residual27_staged(Lay L, const T *__restrict__ opr,
+                                                            const T *__restrict__ v, const T *__restrict__ f,
+                                                            T *__restrict__ r, int na) {
     pdl_entry();
-    extern __shared__ float smf[];
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T *smf = reinterpret_cast<T *>(smraw);
+    using O = Ops<T, ExactOf<T>::value>;
+    constexpr int EPC = 16 / sizeof(T);  // elements per 16-byte copy
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int seg = na + 8;
-    float *S = smf + (size_t)warp * 46 * seg;
+    T *S = smf + (size_t)warp * 46 * seg;
     const long long P = L.plane;
     const int njobs = 2 * L.ny * L.nz;
     for (int job = blockIdx.x * 4 + warp; job < njobs; job += gridDim.x * 4) {
@@ -324,7 +332,7 @@ __global__ void __launch_bounds__(128) k_residual27_staged(Lay L, const float *_
         const int om = px ? 4 : 3, op = px ? 5 : 4;
         const long long r0 = L.G + L.row(j, k) * L.P;
         __syncwarp();
-        for (int e = lane * 4; e < na; e += 128) {
+        for (int e = lane * EPC; e < na; e += 32 * EPC) {
 #pragma unroll
             for (int q = 0; q < 27; q++) cp16(S + q * seg + e, opr + q * P + r0 + hown + e);
             cp16(S + 27 * seg + e, f + r0 + hown + e);
@@ -333,7 +341,7 @@ __global__ void __launch_bounds__(128) k_residual27_staged(Lay L, const float *_
         for (int rr = 0; rr < 9; rr++) {
             const int dy = rr % 3 - 1, dz = rr / 3 - 1;
             const long long rb = L.G + L.row(j + dy, k + dz) * L.P;
-            for (int e = lane * 4; e < seg; e += 128) {
+            for (int e = lane * EPC; e < seg; e += 32 * EPC) {
                 if (e < na) cp16(S + (28 + 2 * rr) * seg + e, v + rb + hown + e);
                 cp16(S + (29 + 2 * rr) * seg + e, v + rb + hoth - 4 + e);
             }
@@ -341,15 +349,15 @@ __global__ void __launch_bounds__(128) k_residual27_staged(Lay L, const float *_
         asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
         __syncwarp();
         for (int a = lane; a < na; a += 32) {
-            float sum = 0.f;
+            T sum = T(0);
 #pragma unroll
             for (int q = 0; q < 27; q++) {
                 const int dx = q % 3 - 1, rr = q / 3;
-                const float vv = dx == 0 ? S[(28 + 2 * rr) * seg + a]
+                const T vv = dx == 0 ? S[(28 + 2 * rr) * seg + a]
                                          : S[(29 + 2 * rr) * seg + a + (dx < 0 ? om : op)];
-                sum = fmaf(S[q * seg + a], vv, sum);
+                sum = O::mac(sum, S[q * seg + a], vv);
             }
-            const float out = S[27 * seg + a] - sum;
+            const T out = O::sub(S[27 * seg + a], sum);
             r[r0 + hown + a] = out;
             const int i = px + 2 * a;
             if (on_periodic_face(L, i, j, k)) write_images(L, r, i, j, k, out);
@@ -398,14 +406,18 @@ __global__ void __launch_bounds__(256) k_residual(Lay L, NbrOff nb, const T *__r
 // each from 4 elements before the half-row to 4 after it, so the i-1 / i+1
 // neighbours (other half, overlap included) are on chip.  Same terms in the
 // same order as residual_point: identical bits.
-__global__ void __launch_bounds__(128) k_residual_staged(Lay L, const float *__restrict__ opr,
-                                                          const float *__restrict__ v, const float *__restrict__ f,
-                                                          float *__restrict__ r, int na) {
+template <typename T>
+__global__ void __launch_bounds__(128) k_residual_staged(Lay L, const T *__restrict__ opr,
+                                                          const T *__restrict__ v, const T *__restrict__ f,
+                                                          T *__restrict__ r, int na) {
     pdl_entry();
-    extern __shared__ float smf[];
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T *smf = reinterpret_cast<T *>(smraw);
+    using O = Ops<T, ExactOf<T>::value>;
+    constexpr int EPC = 16 / sizeof(T);  // elements per 16-byte copy
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int seg = na + 8;
-    float *S = smf + (size_t)warp * 24 * seg;
+    T *S = smf + (size_t)warp * 24 * seg;
     const long long P = L.plane;
     const int nrows = L.ny * L.nz;
     for (int row = blockIdx.x * 4 + warp; row < nrows; row += gridDim.x * 4) {
@@ -417,33 +429,33 @@ __global__ void __launch_bounds__(128) k_residual_staged(Lay L, const float *__r
 #pragma unroll
         for (int h = 0; h < 2; h++) {  // h = 0: odd-x half (offset 0), h = 1: even-x half (offset B0)
             const long long hb = (h ? L.B0 : 0) - 4;
-            const float *src[12] = {opr + r0 + hb,         opr + P + r0 + hb,     opr + 2 * P + r0 + hb,
+            const T *src[12] = {opr + r0 + hb,         opr + P + r0 + hb,     opr + 2 * P + r0 + hb,
                                     opr + 3 * P + r0 + hb, f + r0 + hb,           v + r0 + hb,
                                     opr + 2 * P + rjm + hb, v + rjm + hb,         v + rjp + hb,
                                     opr + 3 * P + rkm + hb, v + rkm + hb,         v + rkp + hb};
 #pragma unroll
             for (int q = 0; q < 12; q++)
-                for (int e = lane * 4; e < seg; e += 128) cp16(S + (h * 12 + q) * seg + e, src[q] + e);
+                for (int e = lane * EPC; e < seg; e += 32 * EPC) cp16(S + (h * 12 + q) * seg + e, src[q] + e);
         }
         asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
         __syncwarp();
         // segment q of half h at S[(12 h + q) seg + 4 + position]
 #pragma unroll
         for (int h = 0; h < 2; h++) {
-            const float *Sh = S + h * 12 * seg + 4, *So = S + (1 - h) * 12 * seg + 4;
+            const T *Sh = S + h * 12 * seg + 4, *So = S + (1 - h) * 12 * seg + 4;
             // x-neighbours in the other half: odd point a (i = 2a+1) has i-1 at even a, i+1 at even a+1;
             // even point a (i = 2a) has i-1 at odd a-1, i+1 at odd a
             const int om = h ? -1 : 0, op = h ? 0 : 1;
             for (int a = lane; a < na; a += 32) {  // lane-strided: conflict-free shared loads
-                float sum = 0.f;
-                sum = fmaf(Sh[9 * seg + a], Sh[10 * seg + a], sum);          // B: T(k-1) v(k-1)
-                sum = fmaf(Sh[6 * seg + a], Sh[7 * seg + a], sum);           // S: N(j-1) v(j-1)
-                sum = fmaf(So[1 * seg + a + om], So[5 * seg + a + om], sum); // W: E(i-1) v(i-1)
-                sum = fmaf(Sh[0 * seg + a], Sh[5 * seg + a], sum);           // C: D v
-                sum = fmaf(Sh[1 * seg + a], So[5 * seg + a + op], sum);      // E: E(i) v(i+1)
-                sum = fmaf(Sh[2 * seg + a], Sh[8 * seg + a], sum);           // N: N(i) v(j+1)
-                sum = fmaf(Sh[3 * seg + a], Sh[11 * seg + a], sum);          // T: T(i) v(k+1)
-                const float out = Sh[4 * seg + a] - sum;
+                T sum = T(0);
+                sum = O::mac(sum, Sh[9 * seg + a], Sh[10 * seg + a]);          // B: T(k-1) v(k-1)
+                sum = O::mac(sum, Sh[6 * seg + a], Sh[7 * seg + a]);           // S: N(j-1) v(j-1)
+                sum = O::mac(sum, So[1 * seg + a + om], So[5 * seg + a + om]); // W: E(i-1) v(i-1)
+                sum = O::mac(sum, Sh[0 * seg + a], Sh[5 * seg + a]);           // C: D v
+                sum = O::mac(sum, Sh[1 * seg + a], So[5 * seg + a + op]);      // E: E(i) v(i+1)
+                sum = O::mac(sum, Sh[2 * seg + a], Sh[8 * seg + a]);           // N: N(i) v(j+1)
+                sum = O::mac(sum, Sh[3 * seg + a], Sh[11 * seg + a]);          // T: T(i) v(k+1)
+                const T out = O::sub(Sh[4 * seg + a], sum);
                 r[r0 + (h ? L.B0 : 0) + a] = out;
                 const int i = h ? 2 * a : 2 * a + 1;
                 if (on_periodic_face(L, i, j, k)) write_images(L, r, i, j, k, out);
@@ -539,14 +551,18 @@ __global__ void __launch_bounds__(256) k_prolong(Lay F, Lay C, const T *__restri
 // ri = 0; odd half: q8(0,pj,pk) for ri = +1 and q8(1,pj,pk) for ri = -1,
 // pj = (1-rj)/2, pk = (1-rk)/2), each from 4 elements before the half-row to
 // 4 after it.  Same terms in the same order as restrict_point.
-__global__ void __launch_bounds__(128) k_restrict_staged(Lay F, Lay C, const float *__restrict__ c2f,
-                                                          const float *__restrict__ rF, float *__restrict__ fC,
-                                                          float *__restrict__ vC, int na) {
+template <typename T>
+__global__ void __launch_bounds__(128) k_restrict_staged(Lay F, Lay C, const T *__restrict__ c2f,
+                                                          const T *__restrict__ rF, T *__restrict__ fC,
+                                                          T *__restrict__ vC, int na) {
     pdl_entry();
-    extern __shared__ float smf[];
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T *smf = reinterpret_cast<T *>(smraw);
+    using O = Ops<T, ExactOf<T>::value>;
+    constexpr int EPC = 16 / sizeof(T);  // elements per 16-byte copy
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int seg = na + 8;
-    float *S = smf + (size_t)warp * 45 * seg;
+    T *S = smf + (size_t)warp * 45 * seg;
     const long long P = F.plane;
     const int nrows = C.ny * C.nz;
     for (int row = blockIdx.x * 4 + warp; row < nrows; row += gridDim.x * 4) {
@@ -560,7 +576,7 @@ __global__ void __launch_bounds__(128) k_restrict_staged(Lay F, Lay C, const flo
                 const int b = 5 * ((rk + 1) * 3 + (rj + 1));
                 const int pj = (1 - rj) / 2, pk = (1 - rk) / 2;
                 const long long fr = F.G + F.row(fj + rj, fk + rk) * F.P - 4;
-                for (int e = lane * 4; e < seg; e += 128) {
+                for (int e = lane * EPC; e < seg; e += 32 * EPC) {
                     cp16(S + (b + 0) * seg + e, rF + fr + e);                              // r odd half
                     cp16(S + (b + 1) * seg + e, rF + fr + F.B0 + e);                       // r even half
                     cp16(S + (b + 2) * seg + e, c2f + q8(0, pj, pk) * P + fr + F.B0 + e);  // ri = 0
@@ -575,7 +591,7 @@ __global__ void __launch_bounds__(128) k_restrict_staged(Lay F, Lay C, const flo
                 const int ci = c0;
                 const int fi = 2 * ci;
                 const int ri0 = -pmod(F.xper, fi - 1, F.nx), ri1 = pmod(F.xper, fi + 1, F.nx);
-                float sum = 0.f;
+                T sum = T(0);
 #pragma unroll
                 for (int rk = -1; rk <= 1; rk++)
 #pragma unroll
@@ -583,18 +599,18 @@ __global__ void __launch_bounds__(128) k_restrict_staged(Lay F, Lay C, const flo
 #pragma unroll
                         for (int ri = -1; ri <= 1; ri++) {
                             if (rk < rk0 || rk > rk1 || rj < rj0 || rj > rj1 || ri < ri0 || ri > ri1) continue;
-                            const float *Sb = S + 5 * ((rk + 1) * 3 + (rj + 1)) * seg + 4;
+                            const T *Sb = S + 5 * ((rk + 1) * 3 + (rj + 1)) * seg + 4;
                             // fi = 2ci: even position ci; fi+1: odd ci; fi-1: odd ci-1
-                            const float w = ri == 0 ? Sb[2 * seg + ci] : (ri > 0 ? Sb[3 * seg + ci] : Sb[4 * seg + ci - 1]);
-                            const float rv = ri == 0 ? Sb[seg + ci] : (ri > 0 ? Sb[ci] : Sb[ci - 1]);
-                            sum = fmaf(w, rv, sum);
+                            const T w = ri == 0 ? Sb[2 * seg + ci] : (ri > 0 ? Sb[3 * seg + ci] : Sb[4 * seg + ci - 1]);
+                            const T rv = ri == 0 ? Sb[seg + ci] : (ri > 0 ? Sb[ci] : Sb[ci - 1]);
+                            sum = O::mac(sum, w, rv);
                         }
                 const long long cid = C.idx(ci, cj, ck);
                 fC[cid] = sum;
-                vC[cid] = 0.f;
+                vC[cid] = T(0);
                 if (on_periodic_face(C, ci, cj, ck)) {
                     write_images(C, fC, ci, cj, ck, sum);
-                    write_images(C, vC, ci, cj, ck, 0.f);
+                    write_images(C, vC, ci, cj, ck, T(0));
                 }
             }
         }
@@ -608,14 +624,18 @@ __global__ void __launch_bounds__(128) k_restrict_staged(Lay F, Lay C, const flo
 // the (up to four) coarse rows it interpolates from, then applies
 // prolong_point's sum term for term.  Requires na = nx/2 (the coarse x size)
 // to be a multiple of 8, so every copied segment is 16-byte aligned.
-__global__ void __launch_bounds__(128) k_prolong_staged(Lay F, Lay C, const float *__restrict__ c2f,
-                                                         const float *__restrict__ vC, float *__restrict__ vF,
+template <typename T>
+__global__ void __launch_bounds__(128) k_prolong_staged(Lay F, Lay C, const T *__restrict__ c2f,
+                                                         const T *__restrict__ vC, T *__restrict__ vF,
                                                          int na) {
     pdl_entry();
-    extern __shared__ float smf[];
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T *smf = reinterpret_cast<T *>(smraw);
+    using O = Ops<T, ExactOf<T>::value>;
+    constexpr int EPC = 16 / sizeof(T);  // elements per 16-byte copy
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int seg = na + 8;
-    float *S = smf + (size_t)warp * 22 * seg;
+    T *S = smf + (size_t)warp * 22 * seg;
     // segments: 0,1 v_f odd/even half; 2 + 3*(pj+2pk) + {0: even pi=0, 1: odd pi=0, 2: odd pi=1};
     // 14 + 2*(pj+2pk) + {0: coarse odd half, 1: coarse even half}
     const long long P = F.plane;
@@ -625,7 +645,7 @@ __global__ void __launch_bounds__(128) k_prolong_staged(Lay F, Lay C, const floa
         const int n2 = j & 1, n3 = k & 1, cj = j >> 1, ck = k >> 1;
         const long long r0 = F.G + F.row(j, k) * F.P;
         __syncwarp();
-        for (int e = lane * 4; e < na; e += 128) {
+        for (int e = lane * EPC; e < na; e += 32 * EPC) {
             cp16(S + e, vF + r0 + e);
             cp16(S + seg + e, vF + r0 + F.B0 + e);
         }
@@ -633,7 +653,7 @@ __global__ void __launch_bounds__(128) k_prolong_staged(Lay F, Lay C, const floa
             for (int pj = 0; pj <= n2; pj++) {
                 const int b = 2 + 3 * (pj + 2 * pk);
                 const long long cr = C.G + C.row(cj + pj, ck + pk) * C.P;
-                for (int e = lane * 4; e < na; e += 128) {
+                for (int e = lane * EPC; e < na; e += 32 * EPC) {
                     cp16(S + b * seg + e, c2f + q8(0, pj, pk) * P + r0 + F.B0 + e);
                     cp16(S + (b + 1) * seg + e, c2f + q8(0, pj, pk) * P + r0 + e);
                     cp16(S + (b + 2) * seg + e, c2f + q8(1, pj, pk) * P + r0 + e);
@@ -641,7 +661,7 @@ __global__ void __launch_bounds__(128) k_prolong_staged(Lay F, Lay C, const floa
                 // coarse odd half: positions < C.nx/2; even half: <= C.nx/2 (overlap
                 // included); both copied up to the next multiple of 4 above C.nx/2
                 const int cb = 14 + 2 * (pj + 2 * pk), ccl = ((C.nx >> 1) + 4) & ~3;
-                for (int e = lane * 4; e < ccl; e += 128) {
+                for (int e = lane * EPC; e < ccl; e += 32 * EPC) {
                     cp16(S + cb * seg + e, vC + cr + e);
                     cp16(S + (cb + 1) * seg + e, vC + cr + C.B0 + e);
                 }
@@ -653,7 +673,7 @@ __global__ void __launch_bounds__(128) k_prolong_staged(Lay F, Lay C, const floa
             const int n1 = 1 - h;
             for (int a = lane; a < na; a += 32) {  // lane-strided: conflict-free shared loads
                 const int i = h ? 2 * a : 2 * a + 1, ci = i >> 1;
-                float ev = 0.f;
+                T ev = T(0);
 #pragma unroll
                 for (int pk = 0; pk <= 1; pk++)
 #pragma unroll
@@ -664,10 +684,10 @@ __global__ void __launch_bounds__(128) k_prolong_staged(Lay F, Lay C, const floa
                             const int b = 2 + 3 * (pj + 2 * pk) + (h ? 0 : 1 + pi);
                             const int cx = ci + pi, cb = 14 + 2 * (pj + 2 * pk);
                             // coarse x-split: odd cx at odd-half position (cx-1)/2, even at even-half cx/2
-                            const float vc = (cx & 1) ? S[cb * seg + ((cx - 1) >> 1)] : S[(cb + 1) * seg + (cx >> 1)];
-                            ev = fmaf(S[b * seg + a], vc, ev);
+                            const T vc = (cx & 1) ? S[cb * seg + ((cx - 1) >> 1)] : S[(cb + 1) * seg + (cx >> 1)];
+                            ev = O::mac(ev, S[b * seg + a], vc);
                         }
-                const float out = S[h * seg + a] + ev;
+                const T out = O::add(S[h * seg + a], ev);
                 vF[r0 + (h ? F.B0 : 0) + a] = out;
                 if (on_periodic_face(F, i, j, k)) write_images(F, vF, i, j, k, out);
             }
@@ -1017,12 +1037,12 @@ template <typename T, int NPT>
 static cudaError_t launch_colour(const Lay &L, const Off27 &off, const T *opr, T *v, const T *f, int px, int py,
                                  int pz, int fuse, cudaStream_t s) {
     const int na = (L.nx - px + 1) >> 1;
-    if constexpr (sizeof(T) == 4 && NPT == 27) {
-        const size_t smem = sizeof(float) * 46 * (size_t)(na + 8) * 4;
+    if constexpr (NPT == 27) {
+        const size_t smem = sizeof(T) * 46 * (size_t)(na + 8) * 4;
         if (use_staged(L) && smem <= 200 * 1024) {
             static bool attr = false;
             if (!attr && smem > 48 * 1024) {
-                cudaError_t e = cudaFuncSetAttribute(k_relax27_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                cudaError_t e = cudaFuncSetAttribute(k_relax27_staged<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                      200 * 1024);
                 if (e != cudaSuccess) return e;
                 attr = true;
@@ -1030,8 +1050,8 @@ static cudaError_t launch_colour(const Lay &L, const Off27 &off, const T *opr, T
             const long long nrows = (long long)((L.ny - py + 1) >> 1) * ((L.nz - pz + 1) >> 1);
             long long gx = (nrows + 3) / 4;
             if (gx > 148LL * 8) gx = 148LL * 8;
-            BB_CHECK_LAUNCH((launch_k(k_relax27_staged, dim3((unsigned)gx), dim3(128), smem, s, L,
-                                      (const float *)opr, (float *)v, (const float *)f, px, py, pz, fuse, na)));
+            BB_CHECK_LAUNCH((launch_k(k_relax27_staged<T>, dim3((unsigned)gx), dim3(128), smem, s, L, opr, v, f, px,
+                                      py, pz, fuse, na)));
             return cudaSuccess;
         }
     }
@@ -1143,36 +1163,25 @@ cudaError_t launch_relax_sweeps(const Lay &L, const NbrOff &nb, int npt, bool fu
 template <typename T>
 cudaError_t launch_residual(const Lay &L, const NbrOff &nb, int npt, const T *opr, const T *v, const T *f, T *r,
                             cudaStream_t s) {
-    if constexpr (sizeof(T) == 4) {
-        const int na = L.nx >> 1;
-        const size_t smem27 = sizeof(float) * 46 * (size_t)(na + 8) * 4;
-        if (npt == 27 && f && use_staged(L) && smem27 <= 200 * 1024) {
-            static bool attr27 = false;
-            if (!attr27 && smem27 > 48 * 1024) {
-                cudaError_t e = cudaFuncSetAttribute(k_residual27_staged,
-                                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    const int na = L.nx >> 1;
+    // measured at 256^3: staged wins for 27-point levels in both precisions and
+    // ties on the FP32 7-point level; the FP64 7-point segments need 104 KB of
+    // shared memory per block (two blocks per SM) and lose to the register kernel
+    if (f && use_staged(L) && (npt == 27 || (npt == 4 && sizeof(T) == 4))) {
+        const int nseg = npt == 27 ? 46 : 24;
+        const size_t smem = sizeof(T) * nseg * (size_t)(na + 8) * 4;
+        auto kern = npt == 27 ? k_residual27_staged<T> : k_residual_staged<T>;
+        if (smem <= 200 * 1024) {
+            static bool attr[2] = {false, false};
+            if (!attr[npt == 27] && smem > 48 * 1024) {
+                cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
                 if (e != cudaSuccess) return e;
-                attr27 = true;
+                attr[npt == 27] = true;
             }
-            long long gx = (2LL * L.ny * L.nz + 3) / 4;
-            if (gx > 148LL * 8) gx = 148LL * 8;
-            BB_CHECK_LAUNCH((launch_k(k_residual27_staged, dim3((unsigned)gx), dim3(128), smem27, s, L,
-                                      (const float *)opr, (const float *)v, (const float *)f, (float *)r, na)));
-            return cudaSuccess;
-        }
-        const size_t smem = sizeof(float) * 24 * (size_t)(na + 8) * 4;
-        if (npt == 4 && f && use_staged(L) && smem <= 200 * 1024) {
-            static bool attr = false;
-            if (!attr && smem > 48 * 1024) {
-                cudaError_t e = cudaFuncSetAttribute(k_residual_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                     200 * 1024);
-                if (e != cudaSuccess) return e;
-                attr = true;
-            }
-            long long gx = ((long long)L.ny * L.nz + 3) / 4;
+            const long long jobs = npt == 27 ? 2LL * L.ny * L.nz : (long long)L.ny * L.nz;
+            long long gx = (jobs + 3) / 4;
             if (gx > 148LL * 16) gx = 148LL * 16;
-            BB_CHECK_LAUNCH((launch_k(k_residual_staged, dim3((unsigned)gx), dim3(128), smem, s, L,
-                                      (const float *)opr, (const float *)v, (const float *)f, (float *)r, na)));
+            BB_CHECK_LAUNCH((launch_k(kern, dim3((unsigned)gx), dim3(128), smem, s, L, opr, v, f, r, na)));
             return cudaSuccess;
         }
     }
@@ -1185,23 +1194,23 @@ cudaError_t launch_residual(const Lay &L, const NbrOff &nb, int npt, const T *op
 
 template <typename T>
 cudaError_t launch_restrict(const Lay &F, const Lay &C, const T *c2f, const T *rF, T *fC, T *vC, cudaStream_t s) {
-    if constexpr (sizeof(T) == 4) {
-        const int na = F.nx >> 1;
-        const size_t smem = sizeof(float) * 45 * (size_t)(na + 8) * 4;
-        if (use_staged(F) && C.nx == na && smem <= 200 * 1024) {
-            static bool attr = false;
-            if (!attr && smem > 48 * 1024) {
-                cudaError_t e = cudaFuncSetAttribute(k_restrict_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                     200 * 1024);
-                if (e != cudaSuccess) return e;
-                attr = true;
-            }
-            long long gx = ((long long)C.ny * C.nz + 3) / 4;
-            if (gx > 148LL * 16) gx = 148LL * 16;
-            BB_CHECK_LAUNCH((launch_k(k_restrict_staged, dim3((unsigned)gx), dim3(128), smem, s, F, C,
-                                      (const float *)c2f, (const float *)rF, (float *)fC, (float *)vC, na)));
-            return cudaSuccess;
+    const int na = F.nx >> 1;
+    const size_t smem = sizeof(T) * 45 * (size_t)(na + 8) * 4;
+    // FP64 segments fill up to 196 KB per block (one block per SM): slower than
+    // the register kernel at 256^3, so the staged restriction is FP32 only
+    if (sizeof(T) == 4 && use_staged(F) && C.nx == na && smem <= 200 * 1024) {
+        static bool attr = false;
+        if (!attr && smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(k_restrict_staged<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 200 * 1024);
+            if (e != cudaSuccess) return e;
+            attr = true;
         }
+        long long gx = ((long long)C.ny * C.nz + 3) / 4;
+        if (gx > 148LL * 16) gx = 148LL * 16;
+        BB_CHECK_LAUNCH((launch_k(k_restrict_staged<T>, dim3((unsigned)gx), dim3(128), smem, s, F, C, c2f, rF, fC, vC,
+                                  na)));
+        return cudaSuccess;
     }
     const Geo g = geo_rows(C.nx, (long long)C.ny * C.nz);
     BB_CHECK_LAUNCH((launch_k(k_restrict<T>, g.grid, g.block, 0, s, F, C, c2f, rF, fC, vC)));
@@ -1210,24 +1219,21 @@ cudaError_t launch_restrict(const Lay &F, const Lay &C, const T *c2f, const T *r
 
 template <typename T>
 cudaError_t launch_prolong(const Lay &F, const Lay &C, const T *c2f, const T *vC, T *vF, cudaStream_t s) {
-    if constexpr (sizeof(T) == 4) {
-        const int na = F.nx >> 1;
-        const size_t smem = sizeof(float) * 22 * (size_t)(na + 8) * 4;
-        // coarse half-rows (x size nx/2, overlap included) fit in na + 8 elements
-        if (use_staged(F) && C.nx == na && (C.nx % 8) == 0 && smem <= 200 * 1024) {
-            static bool attr = false;
-            if (!attr && smem > 48 * 1024) {
-                cudaError_t e = cudaFuncSetAttribute(k_prolong_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                     200 * 1024);
-                if (e != cudaSuccess) return e;
-                attr = true;
-            }
-            long long gx = ((long long)F.ny * F.nz + 3) / 4;
-            if (gx > 148LL * 16) gx = 148LL * 16;
-            BB_CHECK_LAUNCH((launch_k(k_prolong_staged, dim3((unsigned)gx), dim3(128), smem, s, F, C,
-                                      (const float *)c2f, (const float *)vC, (float *)vF, na)));
-            return cudaSuccess;
+    const int na = F.nx >> 1;
+    const size_t smem = sizeof(T) * 22 * (size_t)(na + 8) * 4;
+    // coarse half-rows (x size nx/2, overlap included) fit in na + 8 elements
+    if (use_staged(F) && C.nx == na && (C.nx % 8) == 0 && smem <= 200 * 1024) {
+        static bool attr = false;
+        if (!attr && smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(k_prolong_staged<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 200 * 1024);
+            if (e != cudaSuccess) return e;
+            attr = true;
         }
+        long long gx = ((long long)F.ny * F.nz + 3) / 4;
+        if (gx > 148LL * 16) gx = 148LL * 16;
+        BB_CHECK_LAUNCH((launch_k(k_prolong_staged<T>, dim3((unsigned)gx), dim3(128), smem, s, F, C, c2f, vC, vF, na)));
+        return cudaSuccess;
     }
     const Geo g = geo_rows(F.nx, (long long)F.ny * F.nz);
     BB_CHECK_LAUNCH((launch_k(k_prolong<T>, g.grid, g.block, 0, s, F, C, c2f, vC, vF)));
