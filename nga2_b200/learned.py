@@ -432,3 +432,35 @@ def train(guess: LearnedGuess, records, steps, lr=2e-3, lr_final=2e-4, seed=0, l
         if log and (t % 50 == 0 or t == steps - 1):
             log(t, losses[-1])
     return losses
+
+
+def _time_forward(n, reps=5):
+    """Average device milliseconds and TFLOP/s of one forward pass of the
+    3-input U-Net on an n^3 grid (random inputs; for profiling)."""
+    import torch
+    net = UNet(nf=3, seed=0)
+    rng = np.random.default_rng(0)
+    V = n ** 3
+    fields = [torch.from_numpy(rng.standard_normal(V)).cuda() for _ in range(3)]
+    b = net.buffers((1, n, n, n), False)
+    for _ in range(3):
+        net.embed(b, fields, [1.0, 1.0, 1.0])
+        net.forward(b)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        net.embed(b, fields, [1.0, 1.0, 1.0])
+        net.forward(b)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    depth = {"1": 0, "2": 1, "3": 2, "t": 3}
+    flops = sum(2 * 27 * ci * co * (V >> (3 * depth[name[3] if name[:3] in ("enc", "dec") else "t"]))
+                for name, ci, co in layer_spec())
+    return {"n": n, "forward_ms": ms, "gflop": flops / 1e9, "tflops": flops / ms / 1e9}
+
+
+if __name__ == "__main__":
+    import sys
+    print(_time_forward(int(sys.argv[1]) if len(sys.argv) > 1 else 128))
