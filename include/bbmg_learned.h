@@ -32,9 +32,14 @@ typedef struct {
 } nn_act;
 
 /* y = act(conv3x3x3(x, w) + bias); act = ReLU when relu != 0.  wt is the
- * forward packing of nn_pack_weights.  Tensor cores (mma.sync bf16, FP32
- * accumulate). */
+ * forward packing of nn_pack_weights.  Tensor cores with FP32 accumulation:
+ * tcgen05.mma with a TMEM accumulator when the rows hold a multiple of 128
+ * voxels (cout 16..64, 16-byte aligned views), mma.sync otherwise. */
 int nn_conv3(const nn_act *x, const void *wt, const float *bias, const nn_act *y, int relu, void *stream);
+
+/* BBMG_CUDA if a tcgen05 convolution's completion wait ran out since the last
+ * call (the flag is then cleared), else 0.  Synchronises the device. */
+int nn_tc_error(void);
 
 /* dx = conv3x3x3 of dy with the mirrored, transposed weights (wd, the
  * backward packing): the gradient of the convolution input. */

@@ -10,6 +10,7 @@
 // shared-memory staging; everything else is elementwise.
 #include <cuda_bf16.h>
 #include <cstdint>
+#include <cstdlib>
 
 #include "../../include/bbmg_b200.h"
 #include "../../include/bbmg_learned.h"
@@ -113,8 +114,199 @@ __global__ void __launch_bounds__(128) k_conv3(Act x, const bf16 *__restrict__ w
     }
 }
 
+// ---------------------------------------------------------------------------
+// The same convolution on the fifth-generation tensor cores (tcgen05), for
+// grids whose rows hold a multiple of 128 voxels.  One CTA computes a tile of
+// 128 consecutive voxels of one (n, d, h) row against all output channels:
+//   * the 9 input rows (d+dz, h+dy) of the tile with their x-halo (130 voxels,
+//     periodic wrap) are staged once in shared memory in the K-major canonical
+//     layout of the MMA (no swizzle): for each group of 8 channels, the 130
+//     voxels' 16-byte chunks one after another.  A tap (dz, dy, dx) is then
+//     just a descriptor whose start address is shifted by dx chunks;
+//   * the packed weights [tap][cout][cin] are staged as [tap][K-chunk][group of
+//     8 channels][cout][16 bytes];
+//   * one thread issues 27 x cin/16 tcgen05.mma (M = 128, N = cout, K = 16,
+//     BF16 x BF16 -> FP32) into a TMEM accumulator of cout columns, then
+//     tcgen05.commit arrives on an mbarrier;
+//   * the four warps read their 32 TMEM lanes (= 32 voxels) with tcgen05.ld,
+//     add the bias, apply the ReLU and store BF16 rows.
+// The mbarrier wait is bounded: a wait that runs out raises *err, the CTA still
+// frees its TMEM and returns.
+constexpr unsigned kTcSpinLimit = 1u << 22;
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void cpa16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+
+// shared-memory matrix descriptor: K-major, no swizzle (addresses and offsets in bytes)
+__device__ __forceinline__ uint64_t umma_desc(unsigned saddr, unsigned lbo, unsigned sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;  // descriptor version of sm_100
+    return d;                // base offset 0, layout type 0 (no swizzle)
+}
+
+// instruction descriptor, kind::f16: D FP32, A and B BF16, both K-major, M = 128
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
+template <int N>
+__global__ void __launch_bounds__(128, 1) k_conv3_tc(Act x, const bf16 *__restrict__ wt, const float *__restrict__ bias,
+                                                     Act y, int relu, int *err) {
+    extern __shared__ __align__(128) unsigned char smtc[];
+    constexpr int kCols = N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));  // TMEM columns (power of 2)
+    unsigned *tmem_slot = reinterpret_cast<unsigned *>(smtc);
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(smtc + 8);
+    const int cin = x.c, kg = cin >> 3, kc = cin >> 4;
+    unsigned char *A = smtc + 128;                               // [9][kg][130][16 B]
+    unsigned char *B = A + (size_t)9 * kg * 130 * 16;          // [27][kc][2][N][16 B]
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tiles_per_row = x.w >> 7;
+    const int tile = blockIdx.x;
+    const int w0 = (tile % tiles_per_row) << 7;
+    int rowid = tile / tiles_per_row;  // (n, d, h) row
+    const int h = rowid % x.h;
+    rowid /= x.h;
+    const int d = rowid % x.d, n = rowid / x.d;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(kCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)));
+    // stage the weights: chunk (tap, c, g, o) <- wt[tap][o][16c + 8g .. +8]
+    const int nw = 27 * kc * 2 * N;
+    for (int e = tid; e < nw; e += 128) {
+        const int o = e % N, r = e / N, g = r & 1, c = (r >> 1) % kc, tap = (r >> 1) / kc;
+        cpa16(B + (size_t)e * 16, wt + ((size_t)tap * N + o) * cin + c * 16 + g * 8);
+    }
+    // stage the 9 input rows with their x-halo
+    const int na = 9 * kg * 130;
+    for (int e = tid; e < na; e += 128) {
+        const int vv = e % 130, r = e / 130, g = r % kg, rr = r / kg;
+        const int dz = rr / 3 - 1, dy = rr % 3 - 1;
+        const int dd = wrapi(d + dz, x.d), hh = wrapi(h + dy, x.h), ww = wrapi(w0 - 1 + vv, x.w);
+        cpa16(A + (size_t)e * 16, x.p + (size_t)vox(x, n, dd, hh, ww) * x.ld + g * 8);
+    }
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const unsigned tmem = *reinterpret_cast<volatile unsigned *>(tmem_slot);
+
+    if (tid == 0) {
+        const unsigned abase = smem_u32(A), bbase = smem_u32(B);
+        const uint32_t idesc = umma_idesc_bf16(N);
+        int first = 1;
+        for (int rr = 0; rr < 9; rr++)
+            for (int dx = 0; dx < 3; dx++)
+                for (int c = 0; c < kc; c++) {
+                    const int tap = rr * 3 + dx;
+                    const uint64_t ad = umma_desc(abase + ((rr * kg + 2 * c) * 130 + dx) * 16, 130 * 16, 128);
+                    const uint64_t bd = umma_desc(bbase + ((tap * kc + c) * 2) * N * 16, N * 16, 128);
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\t"
+                        "setp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n"
+                        ::"r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(first ? 0 : 1), "r"(0));
+                    first = 0;
+                }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mbar))
+                     : "memory");
+    }
+    // wait for the accumulator (bounded)
+    unsigned done = 0, spins = 0;
+    while (!done) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done) : "r"(smem_u32(mbar)) : "memory");
+        if (!done && ++spins > kTcSpinLimit) {
+            if (lane == 0) atomicExch(err, 1);
+            break;
+        }
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (done) {
+        const int m = warp * 32 + lane;  // TMEM lane = tile row = voxel
+        const long long v = (long long)vox(x, n, d, h, w0 + m);
+#pragma unroll
+        for (int c0 = 0; c0 < N; c0 += 16) {
+            unsigned r[16];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                : "r"(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            __nv_bfloat162 o2[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                float a = __uint_as_float(r[2 * q]) + (bias ? bias[c0 + 2 * q] : 0.f);
+                float b = __uint_as_float(r[2 * q + 1]) + (bias ? bias[c0 + 2 * q + 1] : 0.f);
+                if (relu) { a = fmaxf(a, 0.f); b = fmaxf(b, 0.f); }
+                o2[q] = __floats2bfloat162_rn(a, b);
+            }
+            uint4 *dst = reinterpret_cast<uint4 *>(y.p + v * y.ld + c0);
+            dst[0] = *reinterpret_cast<uint4 *>(&o2[0]);
+            dst[1] = *reinterpret_cast<uint4 *>(&o2[4]);
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols));
+}
+
+int *tc_err_flag() {
+    static int *flag = nullptr;
+    if (!flag && cudaMalloc(&flag, sizeof(int)) == cudaSuccess) cudaMemset(flag, 0, sizeof(int));
+    return flag;
+}
+
+bool tc_eligible(const Act &x, const Act &y) {
+    static const bool off = getenv("BBMG_NO_TCGEN05") != nullptr;
+    if (off || x.w % 128 || x.c % 16 || (y.c != 16 && y.c != 32 && y.c != 48 && y.c != 64)) return false;
+    if (x.ld % 8 || y.ld % 8 || (reinterpret_cast<uintptr_t>(x.p) & 15) || (reinterpret_cast<uintptr_t>(y.p) & 15))
+        return false;
+    const size_t smem = 128 + (size_t)9 * (x.c / 8) * 130 * 16 + (size_t)27 * x.c * y.c * 2;
+    return smem <= 200 * 1024;
+}
+
+template <int N>
+int launch_conv_tc(const Act &x, const bf16 *wt, const float *bias, const Act &y, int relu, cudaStream_t s) {
+    const size_t smem = 128 + (size_t)9 * (x.c / 8) * 130 * 16 + (size_t)27 * x.c * N * 2;
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(k_conv3_tc<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess)
+            return BBMG_CUDA;
+        attr = true;
+    }
+    int *err = tc_err_flag();
+    if (!err) return BBMG_NO_MEMORY;
+    const int tiles = (x.nvox >> 7);
+    k_conv3_tc<N><<<tiles, 128, smem, s>>>(x, wt, bias, y, relu, err);
+    return done(cudaGetLastError());
+}
+
 int launch_conv(const Act &x, const bf16 *wt, const float *bias, const Act &y, int relu, cudaStream_t s) {
     const int blocks = (x.nvox + 63) / 64;
+    // rows of a multiple of 128 voxels: the tcgen05 kernel
+    if (tc_eligible(x, y)) {
+        switch (y.c) {
+        case 16: return launch_conv_tc<16>(x, wt, bias, y, relu, s);
+        case 32: return launch_conv_tc<32>(x, wt, bias, y, relu, s);
+        case 48: return launch_conv_tc<48>(x, wt, bias, y, relu, s);
+        case 64: return launch_conv_tc<64>(x, wt, bias, y, relu, s);
+        }
+    }
     // output widths of the U-Net: 16/32/64/128 forward; the data gradients
     // of the concatenated decoder inputs add 48/96/192
     if (y.c % 8) return BBMG_BAD_ARGS;
@@ -422,6 +614,16 @@ int nn_conv3_wgrad(const nn_act *x, const nn_act *dy, float *dw, float *db, void
     const int nz = (ax.c * ag.c + 24 * 256 - 1) / (24 * 256);
     k_wgrad<<<dim3(nchunk, 27, nz), 256, shm, (cudaStream_t)stream>>>(ax, ag, dw, db, vchunk);
     return done(cudaGetLastError());
+}
+
+int nn_tc_error(void) {
+    int *flag = tc_err_flag();
+    if (!flag) return BBMG_NO_MEMORY;
+    int v = 0;
+    if (cudaDeviceSynchronize() != cudaSuccess || cudaMemcpy(&v, flag, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return BBMG_CUDA;
+    if (v) cudaMemset(flag, 0, sizeof(int));
+    return v ? BBMG_CUDA : BBMG_OK;
 }
 
 int nn_pack_weights(const float *w, int cin, int cout, void *wt, void *wd, void *stream) {

@@ -43,7 +43,7 @@ class Act(C.Structure):
 
 NN_EXPORTS = ["nn_conv3", "nn_conv3_dgrad", "nn_conv3_wgrad", "nn_pack_weights", "nn_relu_bwd", "nn_pool2",
               "nn_pool2_bwd", "nn_up2", "nn_up2_bwd", "nn_embed", "nn_head", "nn_head_bwd", "nn_mse", "nn_adam",
-              "nn_apply"]
+              "nn_apply", "nn_tc_error"]
 
 _NN = None
 
@@ -72,6 +72,7 @@ def lib():
         "nn_mse": [P, P, D, LL, P, P, P],
         "nn_adam": [P, P, P, P, LL, F, F, F, F, I, P],
         "nn_apply": [P, P, D, I, I, I, I, I, P, P],
+        "nn_tc_error": [],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

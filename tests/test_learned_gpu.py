@@ -393,3 +393,52 @@ def test_learned_guess_on_turbulence_sequence():
         its1.append(it1)
     print("turbulence iterations zero / learned:", its0, its1)
     assert np.mean(its1) <= np.mean(its0), (its0, its1)
+
+
+@pytest.mark.parametrize("cin,cout,relu,dgrad", [(16, 16, 1, False), (48, 16, 0, False), (16, 32, 1, False),
+                                                 (16, 64, 0, False), (16, 48, 0, True)])
+def test_tcgen05_convolution(L, cin, cout, relu, dgrad):
+    """Rows of 128 voxels take the tcgen05 path (TMEM accumulator): forward and
+    data-gradient convolutions against the oracle, and no completion timeout."""
+    rng = np.random.default_rng(100 + cin + cout)
+    shape = (1, 3, 2, 128)
+    n, d, h, w = shape
+    if dgrad:   # dy has cin channels, dx the forward's input channels (cout here)
+        dy = bf(rng.standard_normal((n, cin, d, h, w)))
+        wf = bf(rng.standard_normal((27, cout, cin)) / np.sqrt(27 * cin))
+        _, wd = packed(L, wf.numpy())
+        dyg = to_cl(dy)
+        dxg = torch.empty((n * d * h * w, cout), dtype=torch.bfloat16, device="cuda")
+        assert L.nn_conv3_dgrad(C.byref(act(dyg, shape)), P(wd), C.byref(act(dxg, shape)), None) == 0
+        assert L.nn_tc_error() == 0
+        close_bf16(from_cl(dxg, shape), U.conv3_dgrad(dy, wf))
+        return
+    x = bf(rng.standard_normal((n, cin, d, h, w)))
+    wt_ = bf(rng.standard_normal((27, cin, cout)) / np.sqrt(27 * cin))
+    b = torch.as_tensor(rng.standard_normal(cout) * 0.1, dtype=torch.float32)
+    xg = to_cl(x)
+    yg = torch.empty((n * d * h * w, cout), dtype=torch.bfloat16, device="cuda")
+    wt, _ = packed(L, wt_.numpy())
+    bg = b.cuda()
+    assert L.nn_conv3(C.byref(act(xg, shape)), P(wt), P(bg), C.byref(act(yg, shape)), relu, None) == 0
+    assert L.nn_tc_error() == 0
+    ref = U.conv3(x, wt_, b.double())
+    if relu:
+        ref = torch.relu(ref)
+    close_bf16(from_cl(yg, shape), ref)
+
+
+def test_network_with_tcgen05_rows_matches_oracle():
+    """A 128-voxel-wide grid (level-1 convolutions on tcgen05): the forward pass
+    against the oracle with BF16 storage emulated."""
+    shape = (1, 8, 8, 128)
+    net = NL.UNet(nf=2, seed=5)
+    fields, scales, _ = _sample(2, shape, 6)
+    b = net.buffers(shape, False)
+    net.embed(b, fields, scales)
+    out = net.forward(b).cpu().double()
+    assert NL.lib().nn_tc_error() == 0
+    x = U.embed([f.cpu().numpy() for f in fields], scales, shape)
+    ref = U.forward(net.params.cpu().double(), x, round_bf16=True).reshape(-1)
+    rel = float((out - ref).norm() / ref.norm())
+    assert rel < 3e-2, rel
