@@ -271,6 +271,62 @@ def drops_poisson(n=256, seed=0, ndrops=48, rmin=6.0, rmax=20.0, ratio=1000.0, n
                     "rho_min": float(rho.min()), "rho_max": float(rho.max())})
 
 
+def helmholtz_mast(n=256, seed=0, ndrops=48, rmin=6.0, rmax=20.0, L=1e-2, rho_l=1000.0, rho_g=1.0,
+                   c_l=1500.0, c_g=340.0, u_ref=1.0, cfl=0.5, p0=1.0e5, sigma=0.07, noise=0.01,
+                   per=(True, False, True)):
+    """Pressure Helmholtz system of the compressible two-phase solver mast
+    (``src/two_phase/mast_class.f90:3900-3960``, ``update_Helmholtz_LHS/RHS``):
+
+        opr = -dt^2 div(grad(.)/rho_face) + 1/RHOSS2        (no volume factor)
+        rhs = (PA - P)/RHOSS2 - dt div(u)                    (P = 0: first sub-iteration)
+
+    with the mixture bulk modulus of ``mast_class.f90:3494-3499`` away from
+    interface models, RHOSS2 = 1/(VF/(rho_l c_l^2) + (1-VF)/(rho_g c_g^2)).
+    Liquid drops (VF = 1, water-like) in gas (VF = 0, air-like), tanh-smeared
+    over 1.5 cells, in a box of side ``L`` metres; dt = cfl dx/u_ref (a
+    convective time step, so the acoustic CFL is c dt/dx >> 1 and the system is
+    a Poisson problem shifted by a small positive diagonal: nonsingular);
+    u = u_ref curl(A) + N(0, noise u_ref) at the faces, wall-normal velocity zero
+    at walls; PA = p0 + the Laplace jump 2 sigma/R inside each drop + 1e-3 p0
+    N(0, 1) noise.  The 7-point stencil order is NGA2's."""
+    rng = np.random.default_rng(seed)
+    ratio = rho_l / rho_g
+    rho1, centres, radii = drop_density(n, ndrops, rmin, rmax, ratio, rng, per)
+    vf = (rho1 - 1.0) / (ratio - 1.0)
+    rho = rho_g * rho1
+    inv_rhoss2 = vf / (rho_l * c_l * c_l) + (1.0 - vf) / (rho_g * c_g * c_g)
+    xn = uniform_nodes(n, L)
+    lap, vol = assemble_operator(xn, xn, xn, per, rho=rho)  # -vol div(grad/rho_face)
+    dx = L / n
+    dt = cfl * dx / u_ref
+    opr = (dt * dt) * (lap / vol[..., None])
+    opr[..., 0] += inv_rhoss2
+    U, V, W = _solenoidal_faces(rng, xn, xn, xn, Ls=(L, L, L))
+    scale = u_ref / max(np.abs(U).max(), np.abs(V).max(), np.abs(W).max())
+    U = scale * U + noise * u_ref * rng.standard_normal(U.shape)
+    V = scale * V + noise * u_ref * rng.standard_normal(V.shape)
+    W = scale * W + noise * u_ref * rng.standard_normal(W.shape)
+    if per[0]:
+        U[:, :, -1] = U[:, :, 0]
+    else:
+        U[:, :, 0] = 0.0; U[:, :, -1] = 0.0
+    if per[1]:
+        V[:, -1, :] = V[:, 0, :]
+    else:
+        V[:, 0, :] = 0.0; V[:, -1, :] = 0.0
+    if per[2]:
+        W[-1, :, :] = W[0, :, :]
+    else:
+        W[0, :, :] = 0.0; W[-1, :, :] = 0.0
+    jump = 2.0 * sigma / float(np.mean(radii * L))
+    PA = p0 + jump * vf + 1e-3 * p0 * rng.standard_normal(vf.shape)
+    rhs = PA * inv_rhoss2 - dt * divergence(U, V, W, xn, xn, xn)
+    return Problem("helmholtz_mast", n, n, n, per[0], per[1], per[2], STC7.copy(), opr, rhs, vol, seed,
+                   {"ndrops": ndrops, "radii_cells": [rmin, rmax], "L": L, "dt": dt,
+                    "acoustic_cfl": [c_l * dt / dx, c_g * dt / dx], "rho": [rho_l, rho_g],
+                    "c": [c_l, c_g]})
+
+
 def channel_poisson(nx=512, ny=512, nz=512, seed=0, stretch=2.0, Lx=2.0 * math.pi, Ly=2.0,
                     Lz=2.0 * math.pi, noise=0.1):
     """Stretched-grid channel: periodic x/z, walls in y with
