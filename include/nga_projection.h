@@ -1,0 +1,99 @@
+/*
+ * nga_projection.h -- C ABI of the GPU steps either side of the pressure solve.
+ *
+ * NGA2's flow solvers wrap every pressure solve in the same projection steps:
+ *
+ *   update_laplacian   opr = -vol div(grad(.)/rho_face)     tpns_class.f90:1565-1593
+ *   (psolv%setup)      -> bbmg_setup on the device operator
+ *   get_div            div = divp . (U, V, W)               incomp_class.f90:1144-1159,
+ *                                                           tpns_class.f90:1597-1612
+ *   rhs                rhs = -vol div rho / dt              examples/channel/src/simulation.f90:318,
+ *                                                           examples/falling_drop/src/simulation.f90:302
+ *   (psolv%solve)      -> bbmg_solve
+ *   shift_p            p -= (sum vol p) / fluid_vol         incomp_class.f90:1720-1740
+ *   get_pgrad          grad = divu . P                      incomp_class.f90:1163-1184
+ *   correction         P += sol; U -= dt gradx / rho_U ...  falling_drop/src/simulation.f90:308-313
+ *
+ * With these on the GPU the operator, right-hand side, solution and velocity
+ * never leave device memory between time steps.
+ *
+ * Arrays are device (or managed) pointers in NGA2's Fortran layout: i fastest,
+ * then j, then k, each direction padded by `ghost` overlap layers (>= 1: the
+ * divergence reads U(imax+1), the gradient P(imin-1)).  Face arrays (U, V, W,
+ * rho_U, ...) use the cell-sized layout of the reference: U(i,j,k) sits on the
+ * x-face at x(i), the left face of cell i.  The operator is
+ * opr(7, imino_:imaxo_, jmino_:jmaxo_, kmino_:kmaxo_), stencil index fastest,
+ * in the 7-point order of incomp_class.f90:758-764 ([0,0,0], [+1,0,0],
+ * [-1,0,0], [0,+1,0], [0,-1,0], [0,0,+1], [0,0,-1]).
+ *
+ * The mesh is the rectilinear pgrid of the solver (sgrid_class.f90:160-254):
+ * node coordinates x(imin_:imax_+1), extended naively over the overlap.
+ * Walls are the domain faces of non-periodic directions, where the
+ * reference's umask/vmask/wmask = 2 zero the face metrics divu
+ * (incomp_class.f90:529-563); cells inside walls (cfg%VF = 0) are not
+ * represented: every interior cell is fluid.
+ *
+ * Outputs are written on the interior and then synchronised like cfg%sync on
+ * one rank: overlap cells of periodic directions receive their periodic
+ * images; overlap cells outside walls are left as they were (the reference's
+ * whole-array updates of U and P there act on stale gradients).  The arithmetic
+ * is the reference's term for term (FP64, no contraction), so every output
+ * except shift_p's volume average equals the reference's bit for bit.
+ *
+ * Every entry point returns a BBMG_* status (bbmg_b200.h) and never aborts.
+ * All compute runs on the GPU: there is no CPU fallback.
+ */
+#ifndef NGA_PROJECTION_H
+#define NGA_PROJECTION_H
+
+#include "bbmg_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct nga_proj nga_proj;
+
+/* Metrics of the pgrid (sgrid_class.f90:160-254, config_class.f90:108):
+ * x holds the nx+1 node coordinates x(imin_..imax_+1), likewise y and z
+ * (host arrays).  device -1 = the current device. */
+int nga_proj_create(const bbmg_grid *grid, const double *x, const double *y, const double *z, int device,
+                    nga_proj **p);
+int nga_proj_destroy(nga_proj *p);
+/* Launch stream (a cudaStream_t; NULL = the blocking default stream). */
+int nga_proj_set_stream(nga_proj *p, void *stream);
+
+/* update_laplacian (tpns_class.f90:1565-1593): opr(1:7) from the face
+ * densities rho_U, rho_V, rho_W; rho pointers may be NULL for rho = 1
+ * (incomp_class.f90:766-785). */
+int nga_proj_laplacian(nga_proj *p, const double *rho_U, const double *rho_V, const double *rho_W, double *opr);
+
+/* get_div (incomp_class.f90:1144-1159) and the pressure right-hand side of
+ * the time loop in one pass: div = sum(divp_x U(i:i+1)) + ..., and, when rhs
+ * is not NULL, rhs = -vol*div*rho/dt (rho = 1 reproduces the falling-drop
+ * form -vol*div/dt bit for bit).  div may be NULL when only rhs is wanted.
+ * rhs is written on the interior only (the pressure solver reads nothing
+ * else); div is synchronised. */
+int nga_proj_divergence(nga_proj *p, const double *U, const double *V, const double *W, double rho, double dt,
+                        double *div, double *rhs);
+
+/* shift_p (incomp_class.f90:1720-1740): pressure -= sum(vol*pressure)/fluid_vol
+ * over the interior; the subtracted mean is returned in *mean (may be NULL).
+ * The sum is a fixed-order parallel reduction: the mean agrees with the
+ * reference's sequential loop to round-off, not bit for bit. */
+int nga_proj_shift_p(nga_proj *p, double *pressure, double *mean);
+
+/* get_pgrad (incomp_class.f90:1163-1184): face gradients of P. */
+int nga_proj_pgrad(nga_proj *p, const double *P, double *Pgradx, double *Pgrady, double *Pgradz);
+
+/* The velocity correction of the time loop (falling_drop simulation.f90:
+ * 308-313) fused with get_pgrad: P += sol; U -= dt*gradx(sol)/rho_U; V, W
+ * likewise (rho pointers may be NULL for rho = 1).  P may be NULL. */
+int nga_proj_correct(nga_proj *p, const double *sol, double dt, const double *rho_U, const double *rho_V,
+                     const double *rho_W, double *P, double *U, double *V, double *W);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

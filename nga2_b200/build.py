@@ -13,8 +13,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libbbmg_b200.so")
-SOURCES = ["api.cu", "setup.cu", "solve.cu", "noalloc.cu", "unet.cu"]
-HEADERS = ["common.cuh", "layout.cuh", "setup.cuh", "../../include/bbmg_b200.h", "../../include/bbmg_learned.h"]
+SOURCES = ["api.cu", "setup.cu", "solve.cu", "noalloc.cu", "unet.cu", "projection.cu"]
+HEADERS = ["common.cuh", "layout.cuh", "setup.cuh", "../../include/bbmg_b200.h", "../../include/bbmg_learned.h",
+           "../../include/nga_projection.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

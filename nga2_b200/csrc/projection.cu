@@ -1,0 +1,508 @@
+// projection.cu -- the projection steps either side of the pressure solve on
+// the GPU: operator assembly, divergence and right-hand side, mean removal,
+// pressure gradient and velocity correction (nga_projection.h).
+//
+// Every kernel is a single pass over the interior in the caller's padded
+// Fortran layout (i fastest): one thread per cell, consecutive threads on
+// consecutive i, so every array access of a warp is one contiguous run.  The
+// metrics are 1-D (a rectilinear pgrid) and stay in L1.  HBM traffic per
+// cell, FP64: assembly 3 face densities in + 7 coefficients out (80 B);
+// divergence 3 velocities in + div and rhs out (40 B); correction sol,
+// 3 densities, 3 velocities and P in, 3 velocities and P out (96 B);
+// mean removal 2 passes of 8 + 16 B.
+//
+// Arithmetic follows the reference's expressions term for term with
+// __dadd_rn / __dmul_rn / __ddiv_rn (no contraction), so outputs equal the
+// reference's bits; only shift_p's volume sum is reduced in a different
+// (fixed) order.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "../../include/nga_projection.h"
+
+namespace bbmg {
+void set_create_error(const char *msg);  // api.cu
+}
+
+struct nga_proj {
+    bbmg_grid g{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    // per direction (x, y, z): divp(0), divp(1) on the n cells; divu(-1),
+    // divu(0) on the n+1 faces; cell sizes d (for the volume)
+    double *dp0[3] = {nullptr, nullptr, nullptr}, *dp1[3] = {nullptr, nullptr, nullptr};
+    double *du0[3] = {nullptr, nullptr, nullptr}, *du1[3] = {nullptr, nullptr, nullptr};
+    double *d[3] = {nullptr, nullptr, nullptr};
+    double *metrics = nullptr;  // one allocation holding all of the above
+    double *part = nullptr;     // reduction partials + the mean
+    double vol_total = 0.0;
+};
+
+namespace {
+
+constexpr int kRedBlocks = 148 * 8;
+constexpr int kThreads = 256;
+
+int pfail(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    bbmg::set_create_error(buf);
+    return code;
+}
+
+#define PCU(call)                                                                                        \
+    do {                                                                                                 \
+        cudaError_t e_ = (call);                                                                         \
+        if (e_ != cudaSuccess)                                                                           \
+            return pfail(e_ == cudaErrorMemoryAllocation ? BBMG_NO_MEMORY : BBMG_CUDA, "%s: %s (%s:%d)", \
+                         #call, cudaGetErrorString(e_), __FILE__, __LINE__);                             \
+    } while (0)
+
+bool on_device(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Padded-array geometry of the caller's arrays.
+struct Pad {
+    int nx, ny, nz, g;
+    long long sy, sz;  // strides of j and k
+    __host__ __device__ long long at(int i, int j, int k) const {
+        return (long long)(k + g) * sz + (long long)(j + g) * sy + (i + g);
+    }
+};
+
+Pad pad_of(const bbmg_grid &g) {
+    Pad p;
+    p.nx = g.nx; p.ny = g.ny; p.nz = g.nz; p.g = g.ghost;
+    p.sy = g.nx + 2LL * g.ghost;
+    p.sz = p.sy * (g.ny + 2LL * g.ghost);
+    return p;
+}
+
+struct Metrics {
+    const double *dp0x, *dp1x, *du0x, *du1x, *dx;
+    const double *dp0y, *dp1y, *du0y, *du1y, *dy;
+    const double *dp0z, *dp1z, *du0z, *du1z, *dz;
+};
+
+Metrics metrics_of(const nga_proj *p) {
+    return {p->dp0[0], p->dp1[0], p->du0[0], p->du1[0], p->d[0], p->dp0[1], p->dp1[1], p->du0[1],
+            p->du1[1], p->d[1],   p->dp0[2], p->dp1[2], p->du0[2], p->du1[2], p->d[2]};
+}
+
+__device__ __forceinline__ void cell_of(const Pad &P, long long t, int &i, int &j, int &k) {
+    i = (int)(t % P.nx);
+    const long long r = t / P.nx;
+    j = (int)(r % P.ny);
+    k = (int)(r / P.ny);
+}
+
+__device__ __forceinline__ double rho_at(const double *r, long long e) { return r ? r[e] : 1.0; }
+
+// (a*b)/c, the reference's divp*divu/rho_face
+__device__ __forceinline__ double mdv(double a, double b, double c) { return __ddiv_rn(__dmul_rn(a, b), c); }
+
+// update_laplacian (tpns_class.f90:1565-1593), one cell per thread
+__global__ void __launch_bounds__(kThreads) k_laplacian(Pad P, Metrics M, const double *__restrict__ rU,
+                                                         const double *__restrict__ rV,
+                                                         const double *__restrict__ rW, double *__restrict__ opr) {
+    const long long n = (long long)P.nx * P.ny * P.nz;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        cell_of(P, t, i, j, k);
+        const long long e = P.at(i, j, k);
+        const double rUp = rho_at(rU, e + 1), rUm = rho_at(rU, e);
+        const double rVp = rho_at(rV, e + P.sy), rVm = rho_at(rV, e);
+        const double rWp = rho_at(rW, e + P.sz), rWm = rho_at(rW, e);
+        double o[7];
+        o[0] = mdv(M.dp1x[i], M.du0x[i + 1], rUp);
+        o[0] = __dadd_rn(o[0], mdv(M.dp0x[i], M.du1x[i], rUm));
+        o[0] = __dadd_rn(o[0], mdv(M.dp1y[j], M.du0y[j + 1], rVp));
+        o[0] = __dadd_rn(o[0], mdv(M.dp0y[j], M.du1y[j], rVm));
+        o[0] = __dadd_rn(o[0], mdv(M.dp1z[k], M.du0z[k + 1], rWp));
+        o[0] = __dadd_rn(o[0], mdv(M.dp0z[k], M.du1z[k], rWm));
+        o[1] = mdv(M.dp1x[i], M.du1x[i + 1], rUp);
+        o[2] = mdv(M.dp0x[i], M.du0x[i], rUm);
+        o[3] = mdv(M.dp1y[j], M.du1y[j + 1], rVp);
+        o[4] = mdv(M.dp0y[j], M.du0y[j], rVm);
+        o[5] = mdv(M.dp1z[k], M.du1z[k + 1], rWp);
+        o[6] = mdv(M.dp0z[k], M.du0z[k], rWm);
+        // opr = -opr*vol, vol = dx*dy*dz (config_class.f90:108)
+        const double vol = __dmul_rn(__dmul_rn(M.dx[i], M.dy[j]), M.dz[k]);
+        double *out = opr + 7 * e;
+#pragma unroll
+        for (int q = 0; q < 7; q++) out[q] = __dmul_rn(-o[q], vol);
+    }
+}
+
+// get_div (incomp_class.f90:1144-1159) and rhs = -vol*div*rho/dt
+__global__ void __launch_bounds__(kThreads) k_divergence(Pad P, Metrics M, const double *__restrict__ U,
+                                                          const double *__restrict__ V,
+                                                          const double *__restrict__ W, double rho, double dt,
+                                                          double *__restrict__ div, double *__restrict__ rhs) {
+    const long long n = (long long)P.nx * P.ny * P.nz;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        cell_of(P, t, i, j, k);
+        const long long e = P.at(i, j, k);
+        const double sx = __dadd_rn(__dmul_rn(M.dp0x[i], U[e]), __dmul_rn(M.dp1x[i], U[e + 1]));
+        const double sy = __dadd_rn(__dmul_rn(M.dp0y[j], V[e]), __dmul_rn(M.dp1y[j], V[e + P.sy]));
+        const double sz = __dadd_rn(__dmul_rn(M.dp0z[k], W[e]), __dmul_rn(M.dp1z[k], W[e + P.sz]));
+        const double d = __dadd_rn(__dadd_rn(sx, sy), sz);
+        if (div) div[e] = d;
+        if (rhs) {
+            const double vol = __dmul_rn(__dmul_rn(M.dx[i], M.dy[j]), M.dz[k]);
+            rhs[e] = -__ddiv_rn(__dmul_rn(__dmul_rn(vol, d), rho), dt);
+        }
+    }
+}
+
+// block partial sums of vol*p (config_class.f90:196-214 with VF = 1), a fixed
+// grid and a fixed per-thread order: the same bits on every call
+__global__ void __launch_bounds__(kThreads) k_vol_sum(Pad P, Metrics M, const double *__restrict__ p,
+                                                       double *__restrict__ part) {
+    __shared__ double sh[kThreads];
+    const long long n = (long long)P.nx * P.ny * P.nz;
+    double s = 0.0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        cell_of(P, t, i, j, k);
+        const double vol = __dmul_rn(__dmul_rn(M.dx[i], M.dy[j]), M.dz[k]);
+        s = __dadd_rn(s, __dmul_rn(vol, p[P.at(i, j, k)]));
+    }
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int h = kThreads / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) sh[threadIdx.x] = __dadd_rn(sh[threadIdx.x], sh[threadIdx.x + h]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+// mean = (sum of the partials) / fluid_vol into part[kRedBlocks]
+__global__ void __launch_bounds__(kThreads) k_vol_mean(double *__restrict__ part, double fluid_vol) {
+    __shared__ double sh[kThreads];
+    double s = 0.0;
+    for (int b = threadIdx.x; b < kRedBlocks; b += kThreads) s = __dadd_rn(s, part[b]);
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int h = kThreads / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) sh[threadIdx.x] = __dadd_rn(sh[threadIdx.x], sh[threadIdx.x + h]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[kRedBlocks] = __ddiv_rn(sh[0], fluid_vol);
+}
+
+__global__ void __launch_bounds__(kThreads) k_shift(Pad P, const double *__restrict__ mean, double *__restrict__ p) {
+    const long long n = (long long)P.nx * P.ny * P.nz;
+    const double m = *mean;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        cell_of(P, t, i, j, k);
+        const long long e = P.at(i, j, k);
+        p[e] = __dsub_rn(p[e], m);
+    }
+}
+
+// get_pgrad (incomp_class.f90:1163-1184): sum(divu_x(:,i) P(i-1:i)), ...
+__global__ void __launch_bounds__(kThreads) k_pgrad(Pad P, Metrics M, const double *__restrict__ p,
+                                                     double *__restrict__ gx, double *__restrict__ gy,
+                                                     double *__restrict__ gz) {
+    const long long n = (long long)P.nx * P.ny * P.nz;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        cell_of(P, t, i, j, k);
+        const long long e = P.at(i, j, k);
+        const double pc = p[e];
+        gx[e] = __dadd_rn(__dmul_rn(M.du0x[i], p[e - 1]), __dmul_rn(M.du1x[i], pc));
+        gy[e] = __dadd_rn(__dmul_rn(M.du0y[j], p[e - P.sy]), __dmul_rn(M.du1y[j], pc));
+        gz[e] = __dadd_rn(__dmul_rn(M.du0z[k], p[e - P.sz]), __dmul_rn(M.du1z[k], pc));
+    }
+}
+
+// P += sol; U -= dt*gradx(sol)/rho_U; V, W likewise (falling_drop
+// simulation.f90:308-313 with get_pgrad inlined)
+__global__ void __launch_bounds__(kThreads) k_correct(Pad P, Metrics M, const double *__restrict__ s, double dt,
+                                                       const double *__restrict__ rU, const double *__restrict__ rV,
+                                                       const double *__restrict__ rW, double *__restrict__ pres,
+                                                       double *__restrict__ U, double *__restrict__ V,
+                                                       double *__restrict__ W) {
+    const long long n = (long long)P.nx * P.ny * P.nz;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        cell_of(P, t, i, j, k);
+        const long long e = P.at(i, j, k);
+        const double sc = s[e];
+        const double gx = __dadd_rn(__dmul_rn(M.du0x[i], s[e - 1]), __dmul_rn(M.du1x[i], sc));
+        const double gy = __dadd_rn(__dmul_rn(M.du0y[j], s[e - P.sy]), __dmul_rn(M.du1y[j], sc));
+        const double gz = __dadd_rn(__dmul_rn(M.du0z[k], s[e - P.sz]), __dmul_rn(M.du1z[k], sc));
+        if (pres) pres[e] = __dadd_rn(pres[e], sc);
+        U[e] = __dsub_rn(U[e], __ddiv_rn(__dmul_rn(dt, gx), rho_at(rU, e)));
+        V[e] = __dsub_rn(V[e], __ddiv_rn(__dmul_rn(dt, gy), rho_at(rV, e)));
+        W[e] = __dsub_rn(W[e], __ddiv_rn(__dmul_rn(dt, gz), rho_at(rW, e)));
+    }
+}
+
+__device__ __forceinline__ int wrap_coord(int per, int c, int n) {
+    if (!per) return c;
+    if (c < 0) return c + n * ((-c + n - 1) / n);
+    if (c >= n) return c - n * (c / n);
+    return c;
+}
+
+// cfg%sync on one rank: every overlap cell with a coordinate outside the
+// interior of a periodic direction takes the value of the cell reached by
+// wrapping those coordinates (the reference copies x, then y, then z over the
+// full extent of the other directions, which amounts to the same).  Sources
+// are never themselves periodic images, so one gather pass suffices.
+struct SyncArrays {
+    double *a[4];
+    int n;
+};
+
+__global__ void __launch_bounds__(kThreads) k_sync(Pad P, int xper, int yper, int zper, SyncArrays A) {
+    const long long ex = P.nx + 2LL * P.g, ey = P.ny + 2LL * P.g, ez = P.nz + 2LL * P.g;
+    const long long n = ex * ey * ez;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % ex) - P.g;
+        const long long r = t / ex;
+        const int j = (int)(r % ey) - P.g, k = (int)(r / ey) - P.g;
+        const int si = wrap_coord(xper, i, P.nx), sj = wrap_coord(yper, j, P.ny), sk = wrap_coord(zper, k, P.nz);
+        if (si == i && sj == j && sk == k) continue;
+        const long long d = P.at(i, j, k), s = P.at(si, sj, sk);
+        for (int q = 0; q < A.n; q++) A.a[q][d] = A.a[q][s];
+    }
+}
+
+unsigned grid_cells(long long n) {
+    long long b = (n + kThreads - 1) / kThreads;
+    const long long cap = 148LL * 16;
+    if (b > cap) b = cap;
+    return (unsigned)(b < 1 ? 1 : b);
+}
+
+int sync_arrays(nga_proj *p, double *a0, double *a1, double *a2, double *a3) {
+    const bbmg_grid &g = p->g;
+    if (!(g.xper || g.yper || g.zper) || g.ghost == 0) return BBMG_OK;
+    SyncArrays A{{a0, a1, a2, a3}, 0};
+    double *all[4] = {a0, a1, a2, a3};
+    for (double *x : all)
+        if (x) A.a[A.n++] = x;
+    if (A.n == 0) return BBMG_OK;
+    const Pad P = pad_of(g);
+    const long long n = (g.nx + 2LL * g.ghost) * (g.ny + 2LL * g.ghost) * (g.nz + 2LL * g.ghost);
+    k_sync<<<grid_cells(n), kThreads, 0, p->stream>>>(P, g.xper, g.yper, g.zper, A);
+    PCU(cudaGetLastError());
+    return BBMG_OK;
+}
+
+// Metrics of one direction from its n+1 nodes (sgrid_class.f90:160-254 with
+// the naive extension; incomp_class.f90:355-380 for divp/divu; the wall faces
+// of a non-periodic direction get divu = 0, incomp_class.f90:529-563).
+void axis_metrics(const double *x, int n, bool per, std::vector<double> &dp0, std::vector<double> &dp1,
+                  std::vector<double> &du0, std::vector<double> &du1, std::vector<double> &d) {
+    std::vector<double> xe(n + 3), xm(n + 2);
+    for (int i = 0; i <= n; i++) xe[i + 1] = x[i];
+    xe[0] = xe[1] - (xe[2] - xe[1]);
+    xe[n + 2] = xe[n + 1] + (xe[n + 1] - xe[n]);
+    for (int m = 0; m <= n + 1; m++) xm[m] = 0.5 * (xe[m] + xe[m + 1]);
+    dp0.assign(n, 0.0); dp1.assign(n, 0.0); d.assign(n, 0.0);
+    du0.assign(n + 1, 0.0); du1.assign(n + 1, 0.0);
+    for (int c = 0; c < n; c++) {
+        d[c] = xe[c + 2] - xe[c + 1];
+        const double di = 1.0 / d[c];
+        dp0[c] = di * -1.0;
+        dp1[c] = di * 1.0;
+    }
+    for (int f = 0; f <= n; f++) {
+        const bool wall = !per && (f == 0 || f == n);
+        const double dmi = 1.0 / (xm[f + 1] - xm[f]);
+        du0[f] = wall ? 0.0 : dmi * -1.0;
+        du1[f] = wall ? 0.0 : dmi * 1.0;
+    }
+}
+
+int check_dev(const void *a, const char *name) {
+    if (!a) return pfail(BBMG_BAD_ARGS, "%s is NULL", name);
+    if (!on_device(a)) return pfail(BBMG_BAD_ARGS, "%s is not a device pointer", name);
+    return BBMG_OK;
+}
+
+int check_opt(const void *a, const char *name) {
+    if (a && !on_device(a)) return pfail(BBMG_BAD_ARGS, "%s is not a device pointer", name);
+    return BBMG_OK;
+}
+
+#define PCHK(x)                   \
+    do {                          \
+        int st_ = (x);            \
+        if (st_ != BBMG_OK) return st_; \
+    } while (0)
+
+}  // namespace
+
+extern "C" int nga_proj_create(const bbmg_grid *grid, const double *x, const double *y, const double *z, int device,
+                               nga_proj **out) {
+    if (!grid || !x || !y || !z || !out) return pfail(BBMG_BAD_ARGS, "null argument");
+    *out = nullptr;
+    const bbmg_grid g = *grid;
+    if (g.nx < 1 || g.ny < 1 || g.nz < 1) return pfail(BBMG_BAD_ARGS, "grid sizes must be >= 1");
+    if (g.ghost < 1) return pfail(BBMG_BAD_ARGS, "the projection steps need ghost >= 1 (got %d)", g.ghost);
+    const double *xs[3] = {x, y, z};
+    const int ns[3] = {g.nx, g.ny, g.nz}, pers[3] = {g.xper, g.yper, g.zper};
+    for (int a = 0; a < 3; a++)
+        for (int i = 0; i < ns[a]; i++)
+            if (!(xs[a][i + 1] > xs[a][i])) return pfail(BBMG_BAD_ARGS, "nodes of direction %d must increase", a);
+    if (device < 0) PCU(cudaGetDevice(&device));
+    PCU(cudaSetDevice(device));
+    nga_proj *p = new nga_proj;
+    p->g = g;
+    p->device = device;
+    std::vector<double> host;
+    size_t off[3][5];
+    for (int a = 0; a < 3; a++) {
+        std::vector<double> dp0, dp1, du0, du1, d;
+        axis_metrics(xs[a], ns[a], pers[a] != 0, dp0, dp1, du0, du1, d);
+        const std::vector<double> *parts[5] = {&dp0, &dp1, &du0, &du1, &d};
+        for (int q = 0; q < 5; q++) {
+            off[a][q] = host.size();
+            host.insert(host.end(), parts[q]->begin(), parts[q]->end());
+        }
+    }
+    cudaError_t e = cudaMalloc((void **)&p->metrics, host.size() * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&p->part, (kRedBlocks + 1) * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemcpy(p->metrics, host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        nga_proj_destroy(p);
+        return pfail(e == cudaErrorMemoryAllocation ? BBMG_NO_MEMORY : BBMG_CUDA, "projection setup: %s",
+                     cudaGetErrorString(e));
+    }
+    for (int a = 0; a < 3; a++) {
+        p->dp0[a] = p->metrics + off[a][0];
+        p->dp1[a] = p->metrics + off[a][1];
+        p->du0[a] = p->metrics + off[a][2];
+        p->du1[a] = p->metrics + off[a][3];
+        p->d[a] = p->metrics + off[a][4];
+    }
+    // fluid_vol = vol_total = xL*yL*zL (sgrid_class.f90:260-263; config_class.f90:129)
+    const double xL = x[g.nx] - x[0], yL = y[g.ny] - y[0], zL = z[g.nz] - z[0];
+    p->vol_total = xL * yL * zL;
+    *out = p;
+    return BBMG_OK;
+}
+
+extern "C" int nga_proj_destroy(nga_proj *p) {
+    if (!p) return BBMG_OK;
+    cudaSetDevice(p->device);
+    if (p->metrics) cudaFree(p->metrics);
+    if (p->part) cudaFree(p->part);
+    delete p;
+    return BBMG_OK;
+}
+
+extern "C" int nga_proj_set_stream(nga_proj *p, void *stream) {
+    if (!p) return pfail(BBMG_BAD_ARGS, "null projection handle");
+    p->stream = (cudaStream_t)stream;
+    return BBMG_OK;
+}
+
+extern "C" int nga_proj_laplacian(nga_proj *p, const double *rho_U, const double *rho_V, const double *rho_W,
+                                  double *opr) {
+    if (!p) return pfail(BBMG_BAD_ARGS, "null projection handle");
+    PCHK(check_dev(opr, "opr"));
+    PCHK(check_opt(rho_U, "rho_U"));
+    PCHK(check_opt(rho_V, "rho_V"));
+    PCHK(check_opt(rho_W, "rho_W"));
+    PCU(cudaSetDevice(p->device));
+    const Pad P = pad_of(p->g);
+    const long long n = (long long)P.nx * P.ny * P.nz;
+    k_laplacian<<<grid_cells(n), kThreads, 0, p->stream>>>(P, metrics_of(p), rho_U, rho_V, rho_W, opr);
+    PCU(cudaGetLastError());
+    return BBMG_OK;
+}
+
+extern "C" int nga_proj_divergence(nga_proj *p, const double *U, const double *V, const double *W, double rho,
+                                   double dt, double *div, double *rhs) {
+    if (!p) return pfail(BBMG_BAD_ARGS, "null projection handle");
+    PCHK(check_dev(U, "U"));
+    PCHK(check_dev(V, "V"));
+    PCHK(check_dev(W, "W"));
+    PCHK(check_opt(div, "div"));
+    PCHK(check_opt(rhs, "rhs"));
+    if (!div && !rhs) return pfail(BBMG_BAD_ARGS, "div and rhs are both NULL");
+    if (rhs && !(dt != 0.0)) return pfail(BBMG_BAD_ARGS, "dt must be nonzero");
+    PCU(cudaSetDevice(p->device));
+    const Pad P = pad_of(p->g);
+    const long long n = (long long)P.nx * P.ny * P.nz;
+    k_divergence<<<grid_cells(n), kThreads, 0, p->stream>>>(P, metrics_of(p), U, V, W, rho, dt, div, rhs);
+    PCU(cudaGetLastError());
+    // div is synchronised like get_div's cfg%sync; rhs is the solver's input,
+    // which reads the interior only
+    return sync_arrays(p, div, nullptr, nullptr, nullptr);
+}
+
+extern "C" int nga_proj_shift_p(nga_proj *p, double *pressure, double *mean) {
+    if (!p) return pfail(BBMG_BAD_ARGS, "null projection handle");
+    PCHK(check_dev(pressure, "pressure"));
+    PCU(cudaSetDevice(p->device));
+    const Pad P = pad_of(p->g);
+    const long long n = (long long)P.nx * P.ny * P.nz;
+    k_vol_sum<<<kRedBlocks, kThreads, 0, p->stream>>>(P, metrics_of(p), pressure, p->part);
+    PCU(cudaGetLastError());
+    k_vol_mean<<<1, kThreads, 0, p->stream>>>(p->part, p->vol_total);
+    PCU(cudaGetLastError());
+    k_shift<<<grid_cells(n), kThreads, 0, p->stream>>>(P, p->part + kRedBlocks, pressure);
+    PCU(cudaGetLastError());
+    PCHK(sync_arrays(p, pressure, nullptr, nullptr, nullptr));
+    if (mean) {
+        PCU(cudaMemcpyAsync(mean, p->part + kRedBlocks, sizeof(double), cudaMemcpyDefault, p->stream));
+        PCU(cudaStreamSynchronize(p->stream));
+    }
+    return BBMG_OK;
+}
+
+extern "C" int nga_proj_pgrad(nga_proj *p, const double *P_, double *gx, double *gy, double *gz) {
+    if (!p) return pfail(BBMG_BAD_ARGS, "null projection handle");
+    PCHK(check_dev(P_, "P"));
+    PCHK(check_dev(gx, "Pgradx"));
+    PCHK(check_dev(gy, "Pgrady"));
+    PCHK(check_dev(gz, "Pgradz"));
+    PCU(cudaSetDevice(p->device));
+    const Pad P = pad_of(p->g);
+    const long long n = (long long)P.nx * P.ny * P.nz;
+    k_pgrad<<<grid_cells(n), kThreads, 0, p->stream>>>(P, metrics_of(p), P_, gx, gy, gz);
+    PCU(cudaGetLastError());
+    return sync_arrays(p, gx, gy, gz, nullptr);
+}
+
+extern "C" int nga_proj_correct(nga_proj *p, const double *sol, double dt, const double *rho_U, const double *rho_V,
+                                const double *rho_W, double *pres, double *U, double *V, double *W) {
+    if (!p) return pfail(BBMG_BAD_ARGS, "null projection handle");
+    PCHK(check_dev(sol, "sol"));
+    PCHK(check_dev(U, "U"));
+    PCHK(check_dev(V, "V"));
+    PCHK(check_dev(W, "W"));
+    PCHK(check_opt(rho_U, "rho_U"));
+    PCHK(check_opt(rho_V, "rho_V"));
+    PCHK(check_opt(rho_W, "rho_W"));
+    PCHK(check_opt(pres, "P"));
+    PCU(cudaSetDevice(p->device));
+    const Pad P = pad_of(p->g);
+    const long long n = (long long)P.nx * P.ny * P.nz;
+    k_correct<<<grid_cells(n), kThreads, 0, p->stream>>>(P, metrics_of(p), sol, dt, rho_U, rho_V, rho_W, pres, U, V,
+                                                         W);
+    PCU(cudaGetLastError());
+    return sync_arrays(p, U, V, W, pres);
+}

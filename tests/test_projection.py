@@ -1,0 +1,253 @@
+"""The projection steps around the pressure solve (include/nga_projection.h):
+operator assembly, divergence and right-hand side, shift_p, get_pgrad and
+the velocity correction.
+
+CPU: the library exports every declared symbol; the numpy oracle
+(oracle/projection_oracle.py) agrees with the problem generators' operator and
+divergence, and a whole projection through the oracle leaves a
+divergence-free velocity.  GPU: every kernel equals the oracle bit for bit
+(shift_p's mean to round-off), and a projection chained entirely on the
+device (assembly -> setup -> divergence -> solve -> shift -> correction) leaves
+a divergence-free velocity.
+"""
+import math
+import os
+import re
+
+import numpy as np
+import pytest
+
+from nga2_b200 import problems as P
+from oracle import projection_oracle as PO
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    txt = open(os.path.join(ROOT, "include", "nga_projection.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(nga_[a-z_]+)\s*\(", txt)))
+
+
+def test_library_exports_every_projection_symbol():
+    from nga2_b200 import bbmg as B
+    from nga2_b200 import projection as PR
+    lib = B.load()
+    names = header_functions()
+    assert len(names) == 8
+    for n in names:
+        assert hasattr(lib, n), n
+    assert sorted(PR.EXPORTS) == names
+    PR.lib()  # every signature binds
+
+
+def stretched(n, L=1.0, s=1.5):
+    j = np.arange(n + 1, dtype=np.float64)
+    return 0.5 * L * (1.0 + np.tanh(s * (2.0 * j / n - 1.0)) / math.tanh(s))
+
+
+def make_fields(G, rng, rho_cells=None):
+    """Padded random velocities, face densities (arithmetic means of the
+    cells, the generators' rule) and pressure; ghosts random as well."""
+    shp = G.padded
+    U, V, W, Pr = (rng.standard_normal(shp) for _ in range(4))
+    if rho_cells is None:
+        rho_cells = np.exp(rng.uniform(-2.0, 2.0, size=(G.nz, G.ny, G.nx)))
+    rc = np.ones(shp)
+    G.interior(rc)[...] = rho_cells
+    rc = G.sync(rc)
+    g = G.g
+    # non-periodic overlap cells: copy the adjacent interior layer
+    if not G.per[0]:
+        rc[:, :, :g] = rc[:, :, g:g + 1]; rc[:, :, G.nx + g:] = rc[:, :, G.nx + g - 1:G.nx + g]
+    if not G.per[1]:
+        rc[:, :g, :] = rc[:, g:g + 1, :]; rc[:, G.ny + g:, :] = rc[:, G.ny + g - 1:G.ny + g, :]
+    if not G.per[2]:
+        rc[:g] = rc[g:g + 1]; rc[G.nz + g:] = rc[G.nz + g - 1:G.nz + g]
+    rU, rV, rW = np.ones(shp), np.ones(shp), np.ones(shp)
+    rU[:, :, 1:] = 0.5 * (rc[:, :, :-1] + rc[:, :, 1:])
+    rV[:, 1:, :] = 0.5 * (rc[:, :-1, :] + rc[:, 1:, :])
+    rW[1:, :, :] = 0.5 * (rc[:-1, :, :] + rc[1:, :, :])
+    return U, V, W, Pr, (rU, rV, rW), rho_cells
+
+
+def test_oracle_laplacian_matches_generator():
+    """update_laplacian with arithmetic-mean face densities is the generators'
+    -vol div(grad/rho_face) operator, bit for bit."""
+    for per, g in (((True, False, True), 1), ((False, False, False), 2), ((True, True, True), 1)):
+        xn, yn, zn = P.uniform_nodes(12), stretched(10), P.uniform_nodes(9, 2.0)
+        G = PO.Grid(xn, yn, zn, per, g)
+        rng = np.random.default_rng(1)
+        *_, rho, rho_c = make_fields(G, rng)
+        opr = PO.laplacian(G, *rho)
+        ref, vol = P.assemble_operator(xn, yn, zn, per, rho=rho_c)
+        assert np.array_equal(G.interior(opr), ref)
+        assert np.array_equal(G.vol, vol)
+
+
+def test_oracle_divergence_matches_generator():
+    xn, yn, zn = P.uniform_nodes(12), stretched(10), P.uniform_nodes(9, 2.0)
+    G = PO.Grid(xn, yn, zn, (True, False, True), 1)
+    rng = np.random.default_rng(2)
+    U, V, W, *_ = make_fields(G, rng)
+    div, rhs = PO.divergence(G, U, V, W, dt=0.1)
+    g = G.g
+    Uf = U[g:-g, g:-g, g:g + G.nx + 1]
+    Vf = V[g:-g, g:g + G.ny + 1, g:-g]
+    Wf = W[g:g + G.nz + 1, g:-g, g:-g]
+    assert np.array_equal(G.interior(div), P.divergence(Uf, Vf, Wf, xn, yn, zn))
+    assert np.array_equal(G.interior(rhs), -((G.vol * G.interior(div)) * 1.0) / 0.1)
+
+
+def projection_oracle_chain(n=16, per=(True, False, True), seed=3):
+    """One projection through the oracle: assemble, solve (oracle bbmg),
+    shift, correct; returns max|div| before and after."""
+    from oracle.oracle import OracleBBMG, PCG_BBOX
+    xn = P.uniform_nodes(n)
+    G = PO.Grid(xn, xn, xn, per, 1)
+    rng = np.random.default_rng(seed)
+    U, V, W, Pr, rho, _ = make_fields(G, rng)
+    U, V, W = G.sync(U), G.sync(V), G.sync(W)
+    # zero normal velocity on the walls
+    g = G.g
+    if not per[1]:
+        V[:, g, :] = 0.0; V[:, g + n, :] = 0.0
+    dt = 0.01
+    opr = PO.laplacian(G, *rho)
+    div0, rhs = PO.divergence(G, U, V, W, dt=dt)
+    rhs_i = G.interior(rhs).copy()
+    rhs_i -= rhs_i.mean()
+    o = OracleBBMG(n, n, n, *per, method=PCG_BBOX, rcvg=1e-12)
+    o.setup(P.STC7, np.ascontiguousarray(G.interior(opr)))
+    x, it, rerr = o.solve(rhs_i)
+    sol = np.zeros(G.padded)
+    G.interior(sol)[...] = x
+    sol, mean = PO.shift_p(G, G.sync(sol))
+    U1, V1, W1, P1 = PO.correct(G, sol, dt, U, V, W, Pr, *rho)
+    div1, _ = PO.divergence(G, U1, V1, W1)
+    return np.abs(G.interior(div0)).max(), np.abs(G.interior(div1)).max(), abs(mean)
+
+
+def test_oracle_projection_removes_divergence():
+    d0, d1, _ = projection_oracle_chain()
+    assert d1 < 1e-9 * d0, (d0, d1)
+
+
+# ----------------------------------------------------------------------------- GPU
+GCASES = [((12, 10, 9), (True, False, True), 1), ((8, 8, 8), (True, True, True), 2),
+          ((9, 7, 6), (False, False, False), 1), ((16, 12, 10), (False, True, True), 2)]
+GIDS = ["x".join(map(str, d)) + "-" + "".join("p" if p else "w" for p in per) + f"-g{g}" for d, per, g in GCASES]
+
+
+def gpu_setup(dims, per, g, seed):
+    import torch
+    from nga2_b200.projection import Projection
+    nx, ny, nz = dims
+    xn, yn, zn = P.uniform_nodes(nx), stretched(ny), P.uniform_nodes(nz, 2.0)
+    G = PO.Grid(xn, yn, zn, per, g)
+    pr = Projection(xn, yn, zn, *per, ghost=g, device=0)
+    rng = np.random.default_rng(seed)
+    U, V, W, Pr, rho, _ = make_fields(G, rng)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    return G, pr, (U, V, W, Pr, rho), T
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims,per,g", GCASES, ids=GIDS)
+def test_laplacian_bitexact(dims, per, g):
+    G, pr, (U, V, W, Pr, rho), T = gpu_setup(dims, per, g, 1)
+    for r in (rho, (None, None, None)):
+        ref = PO.laplacian(G, *r)
+        opr = pr.update_laplacian(*(None if a is None else T(a) for a in r)).cpu().numpy()
+        assert np.array_equal(G.interior(opr), G.interior(ref))
+    pr.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims,per,g", GCASES, ids=GIDS)
+def test_divergence_and_rhs_bitexact(dims, per, g):
+    G, pr, (U, V, W, Pr, rho), T = gpu_setup(dims, per, g, 2)
+    rng = np.random.default_rng(9)
+    div0 = rng.standard_normal(G.padded)
+    for rho_s, dt in ((1.0, 0.01), (1000.0, 3e-4)):
+        ref_div, ref_rhs = PO.divergence(G, U, V, W, rho=rho_s, dt=dt, div_out=div0)
+        div, rhs = pr.get_div(T(U), T(V), T(W), rho=rho_s, dt=dt, div=T(div0))
+        assert np.array_equal(div.cpu().numpy(), ref_div)
+        assert np.array_equal(G.interior(rhs.cpu().numpy()), G.interior(ref_rhs))
+    pr.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims,per,g", GCASES, ids=GIDS)
+def test_pgrad_and_correct_bitexact(dims, per, g):
+    G, pr, (U, V, W, Pr, rho), T = gpu_setup(dims, per, g, 3)
+    rng = np.random.default_rng(4)
+    S = G.sync(rng.standard_normal(G.padded))
+    gref = PO.pgrad(G, S)
+    z = lambda: T(rng.standard_normal(G.padded))
+    gx, gy, gz = pr.get_pgrad(T(S), z(), z(), z())
+    for a, b in zip((gx, gy, gz), gref):
+        # ghosts outside walls are left as the caller had them
+        assert np.array_equal(G.interior(a.cpu().numpy()), G.interior(b))
+    U1, V1, W1, P1 = PO.correct(G, S, 0.02, U, V, W, Pr, *rho)
+    tU, tV, tW, tP = T(U), T(V), T(W), T(Pr)
+    pr.correct(T(S), 0.02, tU, tV, tW, tP, *(T(r) for r in rho))
+    for a, b in zip((tU, tV, tW, tP), (U1, V1, W1, P1)):
+        assert np.array_equal(a.cpu().numpy(), b)
+    pr.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims,per,g", GCASES, ids=GIDS)
+def test_shift_p(dims, per, g):
+    G, pr, (U, V, W, Pr, rho), T = gpu_setup(dims, per, g, 5)
+    Pr = Pr + 3.0
+    ref, mref = PO.shift_p(G, Pr)
+    t = T(Pr)
+    m = pr.shift_p(t)
+    assert abs(m - mref) <= 1e-14 * abs(mref)
+    out = t.cpu().numpy()
+    assert np.abs(out - ref).max() <= 1e-14 * np.abs(ref).max()
+    # outside walls the overlap is untouched; the periodic overlap holds images
+    assert np.array_equal(out, G.sync(out))
+    pr.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_projection_on_device_removes_divergence(precision):
+    """Assembly -> bbmg_setup on the device operator -> divergence and rhs ->
+    solve -> shift_p -> correction, all on device arrays: the corrected
+    velocity is discretely divergence-free, and the chain matches the oracle's."""
+    import torch
+    from nga2_b200.bbmg import BBMG, FP64, MIXED, PCG_BBOX
+    from nga2_b200.projection import Projection
+    n, per, g = 32, (True, False, True), 1
+    xn = P.uniform_nodes(n)
+    G = PO.Grid(xn, xn, xn, per, g)
+    rng = np.random.default_rng(7)
+    rho_c, _, _ = P.drop_density(n, 4, 2.0, 5.0, 1000.0, rng, per)
+    U, V, W, Pr, rho, _ = make_fields(G, rng, rho_cells=rho_c)
+    U, V, W = G.sync(U), G.sync(V), G.sync(W)
+    V[:, g, :] = 0.0; V[:, g + n, :] = 0.0
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    pr = Projection(xn, xn, xn, *per, ghost=g, device=0)
+    tU, tV, tW, tP = T(U), T(V), T(W), T(Pr)
+    trho = tuple(T(r) for r in rho)
+    dt = 1e-3
+    opr = pr.update_laplacian(*trho)
+    h = BBMG(n, n, n, *per, ghost=g, method=PCG_BBOX, precision=FP64 if precision == "fp64" else MIXED,
+             rcvg=1e-11, device=0)
+    h.setup(P.STC7, opr)
+    div0, rhs = pr.get_div(tU, tV, tW, dt=dt)
+    sol = torch.zeros_like(rhs)
+    _, it, rerr, st = h.solve(rhs, sol)
+    assert st == 0
+    pr.shift_p(sol)
+    pr.correct(sol, dt, tU, tV, tW, tP, *trho)
+    div1, _ = pr.get_div(tU, tV, tW)
+    d0 = G.interior(div0.cpu().numpy())
+    d1 = G.interior(div1.cpu().numpy())
+    assert np.abs(d1).max() < 1e-8 * np.abs(d0).max(), (np.abs(d1).max(), np.abs(d0).max())
+    h.close()
+    pr.close()
