@@ -464,6 +464,170 @@ __global__ void __launch_bounds__(128) k_residual_staged(Lay L, const T *__restr
     }
 }
 
+// Asynchronous global -> shared copy of 4, 8 or 16 bytes.
+template <int BYTES>
+__device__ __forceinline__ void cpa(void *dst, const void *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    if constexpr (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(src), "n"(BYTES) : "memory");
+}
+
+template <typename T>
+struct MarchVec;
+template <> struct MarchVec<float> { using V = float4; static constexpr int W = 4; };
+template <> struct MarchVec<double> { using V = double2; static constexpr int W = 2; };
+
+// VW consecutive shared-memory values, 16-byte aligned, as one vector load
+template <typename T, int VW>
+__device__ __forceinline__ void ldvec(T *dst, const T *src) {
+    using V = typename MarchVec<T>::V;
+    const V x = *reinterpret_cast<const V *>(src);
+    if constexpr (VW == 4) {
+        dst[0] = x.x; dst[1] = x.y; dst[2] = x.z; dst[3] = x.w;
+    } else {
+        dst[0] = x.x; dst[1] = x.y;
+    }
+}
+
+// Residual of the symmetric 7-point level (planes D, E, N, T) by marching up
+// the k columns.  A block owns TY consecutive (j) rows, both x-halves, of a
+// chunk of k-planes; each thread owns VW = 16/sizeof(T) consecutive positions
+// of one half-row.  Plane by plane, a three-slot ring of shared-memory stages
+// is filled with cp.async one plane ahead of the computation: stage(k) holds
+// D, E, N, T and f of plane k on the block's rows, N on row j0-1, and v of
+// plane k+1 on rows j0-1 .. j0+TY (each half-row with its overlap positions -1
+// and na).  The residual of plane k reads stage(k) and stage(k-1) (v of plane
+// k and T of plane k-1), and v(k-1) from a register.  Every array is read from
+// HBM once per block apart from the two halo rows and one extra plane per
+// chunk: ~31 B per cell against the algorithm's 28.  Terms and order are
+// residual_point's (B, S, W, C, E, N, T): the same bits.  Requires an even
+// nx, na = nx/2 a multiple of VW and TH = na/VW a power of two in [8, 128]
+// (the block holds TY = 128/TH rows).
+template <typename T>
+__global__ void __launch_bounds__(256) k_residual_march(Lay L, const T *__restrict__ opr, const T *__restrict__ v,
+                                                         const T *__restrict__ f, T *__restrict__ r, int na,
+                                                         int kchunk) {
+    pdl_entry();
+    using O = Ops<T, ExactOf<T>::value>;
+    constexpr int VW = MarchVec<T>::W;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T *sm = reinterpret_cast<T *>(smraw);
+    const int TH = na / VW, TY = 128 / TH;
+    const int seg = na + 8;                  // position p of a half-row at index p + 4
+    const int rows = 5 * TY + 1 + TY + 2;    // C[5][TY], NH, VT[TY+2]
+    const int SS = rows * 2 * seg;           // elements per stage
+    const int tid = threadIdx.x, c = tid % TH, h = (tid / TH) & 1, jj = tid / (2 * TH);
+    const int j0 = blockIdx.x * TY, j = j0 + jj;
+    const bool valid = j < L.ny;
+    const int k0 = blockIdx.y * kchunk, k1 = min(L.nz, k0 + kchunk);
+    if (k0 >= k1) return;  // uniform over the block
+    const long long P = L.plane, hb = h ? L.B0 : 0;
+    const int pos = c * VW;
+    const int jt = min(j0 + TY, L.ny);  // row after the block's last valid row
+    const bool lo_edge = h == 0 && c == 0, hi_edge = h == 1 && c == TH - 1;
+    const int ovl = h == 0 ? -1 : na;   // overlap position of this half
+    auto goff = [&](int jr, int kr) { return L.G + L.row(jr, kr) * L.P + hb; };
+    // row `rr` of stage slot `sl`, this thread's half (hh = h) or the other
+    auto srow = [&](int sl, int rr, int hh) { return sm + (size_t)sl * SS + (rr * 2 + hh) * seg + 4; };
+    const int RC = 0, RNH = 5 * TY, RVT = 5 * TY + 1;  // first rows of C, NH, VT
+    auto fill = [&](int sl, int kp) {
+        if (valid) {
+            const long long g = goff(j, kp) + pos;
+#pragma unroll
+            for (int q = 0; q < 4; q++) cpa<16>(srow(sl, RC + q * TY + jj, h) + pos, opr + q * P + g);
+            cpa<16>(srow(sl, RC + 4 * TY + jj, h) + pos, f + g);
+            cpa<16>(srow(sl, RVT + jj + 1, h) + pos, v + goff(j, kp + 1) + pos);
+            if (lo_edge) cpa<sizeof(T)>(srow(sl, RC + TY + jj, 0) - 1, opr + P + goff(j, kp) - 1);
+            if (lo_edge || hi_edge) cpa<sizeof(T)>(srow(sl, RVT + jj + 1, h) + ovl, v + goff(j, kp + 1) + ovl);
+        }
+        if (jj == 0) {  // row j0-1 (always a stored row: overlap or interior)
+            cpa<16>(srow(sl, RNH, h) + pos, opr + 2 * P + goff(j0 - 1, kp) + pos);
+            cpa<16>(srow(sl, RVT, h) + pos, v + goff(j0 - 1, kp + 1) + pos);
+            if (lo_edge || hi_edge) cpa<sizeof(T)>(srow(sl, RVT, h) + ovl, v + goff(j0 - 1, kp + 1) + ovl);
+        }
+        if (jj == TY - 1) {
+            cpa<16>(srow(sl, RVT + jt - j0 + 1, h) + pos, v + goff(jt, kp + 1) + pos);
+            if (lo_edge || hi_edge)
+                cpa<sizeof(T)>(srow(sl, RVT + jt - j0 + 1, h) + ovl, v + goff(jt, kp + 1) + ovl);
+        }
+    };
+    auto commit = []() { asm volatile("cp.async.commit_group;" ::: "memory"); };
+    T vm[VW];  // v(k-1) at the thread's positions
+    if (valid) {
+#pragma unroll
+        for (int q = 0; q < VW; q++) vm[q] = v[goff(j, k0 - 1) + pos + q];
+    }
+    // stage(k) lives in slot (k - k0 + 1) % 3
+    fill(0, k0 - 1);
+    commit();
+    fill(1, k0);
+    commit();
+    for (int k = k0; k < k1; k++) {
+        const int sp = (k - k0) % 3, sc = (k - k0 + 1) % 3, sn = (k - k0 + 2) % 3;
+        __syncthreads();  // slot sn (stage k-2) is no longer read
+        if (k + 1 < k1) fill(sn, k + 1);
+        commit();
+        asm volatile("cp.async.wait_group 1;" ::: "memory");
+        __syncthreads();  // stage k complete for every thread
+        if (valid) {
+            const int rs = 2 * seg;
+            const T *Cc = srow(sc, RC, h);
+            const T *Dk = Cc + (0 * TY + jj) * rs, *Ek = Cc + (1 * TY + jj) * rs;
+            const T *Nk = Cc + (2 * TY + jj) * rs, *Tk = Cc + (3 * TY + jj) * rs, *Fk = Cc + (4 * TY + jj) * rs;
+            const T *Eo = srow(sc, RC + TY + jj, 1 - h);                                // E(k), other half
+            const T *Ns = jj ? srow(sc, RC + 2 * TY + jj - 1, h) : srow(sc, RNH, h);    // N(j-1, k)
+            const T *Tm = srow(sp, RC + 3 * TY + jj, h);                                // T(k-1)
+            const T *vS = srow(sp, RVT + jj, h), *vN = srow(sp, RVT + jj + 2, h);       // v(j-1,k), v(j+1,k)
+            const T *vC = srow(sp, RVT + jj + 1, h), *vO = srow(sp, RVT + jj + 1, 1 - h);  // v(k): own, other half
+            const T *vP = srow(sc, RVT + jj + 1, h);                                    // v(k+1)
+            // vector reads of the thread's VW positions (conflict-free); the
+            // other half's v and E also one position either side
+            T tm[VW], ns[VW], vs[VW], dk[VW], vc[VW], ek[VW], nk[VW], vn[VW], tk[VW], vp[VW], fk[VW];
+            T vo[VW + 2], eo[VW + 1];
+            ldvec<T, VW>(tm, Tm + pos); ldvec<T, VW>(ns, Ns + pos); ldvec<T, VW>(vs, vS + pos);
+            ldvec<T, VW>(dk, Dk + pos); ldvec<T, VW>(vc, vC + pos); ldvec<T, VW>(ek, Ek + pos);
+            ldvec<T, VW>(nk, Nk + pos); ldvec<T, VW>(vn, vN + pos); ldvec<T, VW>(tk, Tk + pos);
+            ldvec<T, VW>(vp, vP + pos); ldvec<T, VW>(fk, Fk + pos);
+            ldvec<T, VW>(vo + 1, vO + pos); vo[0] = vO[pos - 1]; vo[VW + 1] = vO[pos + VW];
+            ldvec<T, VW>(eo + 1, Eo + pos); eo[0] = Eo[pos - 1];
+            T res[VW];
+#pragma unroll
+            for (int q = 0; q < VW; q++) {
+                T s = T(0);
+                s = O::mac(s, tm[q], vm[q]);                          // B: T(k-1) v(k-1)
+                s = O::mac(s, ns[q], vs[q]);                          // S: N(j-1) v(j-1)
+                // odd point (h = 0): i-1 at the other half's position a, i+1 at a+1;
+                // even point (h = 1): i-1 at a-1, i+1 at a
+                const T wcoef = h ? eo[q] : eo[q + 1], wval = h ? vo[q] : vo[q + 1];
+                const T eval = h ? vo[q + 1] : vo[q + 2];
+                s = O::mac(s, wcoef, wval);                           // W: E(i-1) v(i-1)
+                s = O::mac(s, dk[q], vc[q]);                          // C: D v
+                s = O::mac(s, ek[q], eval);                           // E: E(i) v(i+1)
+                s = O::mac(s, nk[q], vn[q]);                          // N: N(i) v(j+1)
+                s = O::mac(s, tk[q], vp[q]);                          // T: T(i) v(k+1)
+                res[q] = O::sub(fk[q], s);
+            }
+            T *dst = r + goff(j, k) + pos;
+            if constexpr (VW == 4)
+                *reinterpret_cast<float4 *>(dst) = make_float4(res[0], res[1], res[2], res[3]);
+            else
+                *reinterpret_cast<double2 *>(dst) = make_double2(res[0], res[1]);
+            if (L.xper || L.yper || L.zper) {
+#pragma unroll
+                for (int q = 0; q < VW; q++) {
+                    const int i = h ? 2 * (pos + q) : 2 * (pos + q) + 1;
+                    if (on_periodic_face(L, i, j, k)) write_images(L, r, i, j, k, res[q]);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < VW; q++) vm[q] = vc[q];
+        }
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
 // Restriction f_c = sum_r f2c(r) r_f(2c + r) (bbmg_class.f90:805-827), with
 // f2c(r) = c2f((1-r)/2, 2c+r) (bbmg_class.f90:1218-1222) read straight from the
 // fine prolongation weights.  Also zeroes the coarse correction v_c, the first
@@ -1164,6 +1328,43 @@ template <typename T>
 cudaError_t launch_residual(const Lay &L, const NbrOff &nb, int npt, const T *opr, const T *v, const T *f, T *r,
                             cudaStream_t s) {
     const int na = L.nx >> 1;
+    // symmetric 7-point level: column marching (both precisions, same bits as
+    // the register kernel)
+    if (f && npt == 4 && use_staged(L)) {
+        constexpr int VW = MarchVec<T>::W;
+        const int TH = na / VW;
+        if (!(L.nx & 1) && na % VW == 0 && TH >= 8 && TH <= 128 && (TH & (TH - 1)) == 0) {
+            const int TY = 128 / TH, seg = na + 8;
+            const size_t smem = sizeof(T) * (size_t)seg * 2 * (5 * TY + 1 + TY + 2) * 3;
+            static bool attr[2] = {false, false};
+            if (smem <= 200 * 1024 && !attr[sizeof(T) == 8]) {
+                if (cudaFuncSetAttribute(k_residual_march<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) ==
+                    cudaSuccess)
+                    attr[sizeof(T) == 8] = true;
+            }
+            if (smem <= 200 * 1024 && attr[sizeof(T) == 8]) {
+                int oc = 0;
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&oc, k_residual_march<T>, 256, smem) != cudaSuccess ||
+                    oc < 1)
+                    oc = 1;
+                int nsm = 148;
+                {
+                    int dev = 0;
+                    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+                }
+                // about two waves of resident blocks: the second wave evens out the SMs
+                const int jtiles = (L.ny + TY - 1) / TY;
+                int nch = 2 * nsm * oc / jtiles;
+                if (nch > L.nz) nch = L.nz;
+                if (nch < 1) nch = 1;
+                const int kchunk = (L.nz + nch - 1) / nch;
+                nch = (L.nz + kchunk - 1) / kchunk;
+                BB_CHECK_LAUNCH((launch_k(k_residual_march<T>, dim3(jtiles, nch), dim3(256), smem, s, L, opr, v, f, r,
+                                          na, kchunk)));
+                return cudaSuccess;
+            }
+        }
+    }
     // measured at 256^3: staged wins for 27-point levels in both precisions and
     // ties on the FP32 7-point level; the FP64 7-point segments need 104 KB of
     // shared memory per block (two blocks per SM) and lose to the register kernel

@@ -275,5 +275,5 @@ def test_staged_fp32_relax_matches_register_kernel(n, tmp_path):
     env["BBMG_NO_STAGED"] = "1"
     subprocess.run([sys.executable, probe, str(n), b], check=True, env=env)
     za, zb = np.load(a), np.load(b)
-    for key in ("v", "r", "f2", "v2", "r2"):
+    for key in ("v", "r", "f2", "v2", "r2", "r64"):
         assert np.array_equal(za[key], zb[key]), key
