@@ -1097,6 +1097,187 @@ __global__ void __launch_bounds__(256) k_cg_pap_fused(Lay L, NbrOff nb, const do
     if (block_leader()) part[block_id()] = acc;
 }
 
+// pp_new = zz + beta*pp_old and Ap = A pp_new with the block partial of
+// pp_new . Ap, for the symmetric 7-point level-1 operator, by k-column
+// marching (the structure of k_residual_march): a block of NT threads owns TY
+// rows (both halves) of a chunk of k-planes, a thread VW = 2 consecutive
+// positions of one half-row.  A two-slot ring of cp.async stages holds, for
+// plane k, D, E, N, T on the block's rows and N on row j0-1, and zz and pp_old
+// of plane k+1 on rows j0-1 .. j0+TY with the overlap positions; from those
+// the block forms the direction p of plane k+1 in a two-slot shared ring.
+// Ap(k) reads p(k-1) and T(k-1) from registers, p(k) and p(k+1) from the
+// ring.  Each point's arithmetic is k_cg_pap_fused's, so pp_new and Ap are
+// the same bits; the partial sums group the products differently.
+template <typename TZ, int NT>
+__global__ void __launch_bounds__(NT) k_cg_pap_march(Lay L, const double *__restrict__ opr,
+                                                      const TZ *__restrict__ zz, const double *__restrict__ pp_old,
+                                                      double *__restrict__ pp_new, double *__restrict__ Ap,
+                                                      const CgScal *__restrict__ sc, double *__restrict__ part,
+                                                      int na, int kchunk) {
+    pdl_entry();
+    __shared__ double red[NT];
+    extern __shared__ __align__(16) unsigned char smraw[];
+    using O = Ops<double, true>;
+    constexpr int VW = 2;
+    const double beta = sc->beta;
+    const int TH = na / VW, TY = NT / (2 * TH);
+    const int seg = na + 8;  // position p of a half-row at index p + 4
+    const int rowsO = 4 * TY + 1, rowsV = TY + 2;
+    const size_t bO = (size_t)rowsO * 2 * seg * sizeof(double), bZ = (size_t)rowsV * 2 * seg * sizeof(TZ);
+    const size_t bP = (size_t)rowsV * 2 * seg * sizeof(double), bS = bO + bZ + bP;
+    auto sO = [&](int sl, int rr, int hh) {
+        return reinterpret_cast<double *>(smraw + sl * bS) + (rr * 2 + hh) * seg + 4;
+    };
+    auto sZ = [&](int sl, int rr, int hh) {
+        return reinterpret_cast<TZ *>(smraw + sl * bS + bO) + (rr * 2 + hh) * seg + 4;
+    };
+    auto sP = [&](int sl, int rr, int hh) {
+        return reinterpret_cast<double *>(smraw + sl * bS + bO + bZ) + (rr * 2 + hh) * seg + 4;
+    };
+    auto pR = [&](int sl, int rr, int hh) {
+        return reinterpret_cast<double *>(smraw + 2 * bS + sl * bP) + (rr * 2 + hh) * seg + 4;
+    };
+    const int tid = threadIdx.x, c = tid % TH, h = (tid / TH) & 1, jj = tid / (2 * TH);
+    const int j0 = blockIdx.x * TY, j = j0 + jj;
+    const bool valid = j < L.ny;
+    const int k0 = blockIdx.y * kchunk, k1 = min(L.nz, k0 + kchunk);
+    const long long P = L.plane, hb = h ? L.B0 : 0;
+    const int pos = c * VW;
+    const int jt = min(j0 + TY, L.ny);
+    const bool lo_edge = h == 0 && c == 0, hi_edge = h == 1 && c == TH - 1, edge = lo_edge || hi_edge;
+    const int ovl = h == 0 ? -1 : na;
+    auto goff = [&](int jr, int kr) { return L.G + L.row(jr, kr) * L.P + hb; };
+    auto commit = []() { asm volatile("cp.async.commit_group;" ::: "memory"); };
+    // zz and pp_old of plane kp on row jr into tile row rr of slot sl
+    auto fill_v = [&](int sl, int rr, int jr, int kp) {
+        const long long g = goff(jr, kp);
+        cpa<VW * sizeof(TZ)>(sZ(sl, rr, h) + pos, zz + g + pos);
+        cpa<16>(sP(sl, rr, h) + pos, pp_old + g + pos);
+        if (edge) {
+            cpa<sizeof(TZ)>(sZ(sl, rr, h) + ovl, zz + g + ovl);
+            cpa<8>(sP(sl, rr, h) + ovl, pp_old + g + ovl);
+        }
+    };
+    auto fill = [&](int sl, int kp) {
+        if (valid) {
+            const long long g = goff(j, kp) + pos;
+#pragma unroll
+            for (int q = 0; q < 4; q++) cpa<16>(sO(sl, q * TY + jj, h) + pos, opr + q * P + g);
+            if (lo_edge) cpa<8>(sO(sl, TY + jj, 0) - 1, opr + P + goff(j, kp) - 1);
+            fill_v(sl, jj + 1, j, kp + 1);
+        }
+        if (jj == 0) {
+            cpa<16>(sO(sl, 4 * TY, h) + pos, opr + 2 * P + goff(j0 - 1, kp) + pos);
+            fill_v(sl, 0, j0 - 1, kp + 1);
+        }
+        if (jj == TY - 1) fill_v(sl, jt - j0 + 1, jt, kp + 1);
+    };
+    // p = zz + beta*pp_old for the tile positions this thread copied
+    auto make_p_row = [&](int sl, int slot, int rr) {
+        const TZ *z = sZ(sl, rr, h);
+        const double *po = sP(sl, rr, h);
+        double *pr = pR(slot, rr, h);
+#pragma unroll
+        for (int q = 0; q < VW; q++) pr[pos + q] = __dadd_rn((double)z[pos + q], __dmul_rn(beta, po[pos + q]));
+        if (edge) pr[ovl] = __dadd_rn((double)z[ovl], __dmul_rn(beta, po[ovl]));
+    };
+    auto make_p = [&](int sl, int slot) {
+        if (valid) make_p_row(sl, slot, jj + 1);
+        if (jj == 0) make_p_row(sl, slot, 0);
+        if (jj == TY - 1) make_p_row(sl, slot, jt - j0 + 1);
+    };
+    double acc = 0.0;
+    if (k0 < k1) {
+        double pm[VW] = {0.0, 0.0}, tm[VW] = {0.0, 0.0};
+        if (valid) {
+            const long long g = goff(j, k0 - 1) + pos;
+#pragma unroll
+            for (int q = 0; q < VW; q++) {
+                pm[q] = __dadd_rn((double)zz[g + q], __dmul_rn(beta, pp_old[g + q]));
+                tm[q] = opr[3 * P + g + q];
+            }
+        }
+        // stage(k) lives in slot (k - k0 + 1) & 1, the direction of plane k in ring slot k & 1
+        fill(0, k0 - 1);
+        commit();
+        fill(1, k0);
+        commit();
+        asm volatile("cp.async.wait_group 1;" ::: "memory");
+        __syncthreads();
+        make_p(0, k0 & 1);
+        for (int k = k0; k < k1; k++) {
+            const int scur = (k - k0 + 1) & 1, snext = (k - k0) & 1;
+            __syncthreads();  // stage(k-1) and p(k-1) are no longer read
+            if (k + 1 < k1) fill(snext, k + 1);
+            commit();
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+            __syncthreads();  // stage(k) complete for every thread
+            make_p(scur, (k + 1) & 1);
+            __syncthreads();  // p(k+1) complete
+            if (valid) {
+                double dk[VW], ek[VW], nk[VW], tk[VW], ns[VW], pc[VW], ps[VW], pn[VW], pp[VW];
+                double po[VW + 2], eo[VW + 1];
+                ldvec<double, VW>(dk, sO(scur, jj, h) + pos);
+                ldvec<double, VW>(ek, sO(scur, TY + jj, h) + pos);
+                ldvec<double, VW>(nk, sO(scur, 2 * TY + jj, h) + pos);
+                ldvec<double, VW>(tk, sO(scur, 3 * TY + jj, h) + pos);
+                ldvec<double, VW>(ns, (jj ? sO(scur, 2 * TY + jj - 1, h) : sO(scur, 4 * TY, h)) + pos);
+                const double *Eo = sO(scur, TY + jj, 1 - h);
+                ldvec<double, VW>(eo + 1, Eo + pos);
+                eo[0] = Eo[pos - 1];
+                ldvec<double, VW>(pc, pR(k & 1, jj + 1, h) + pos);
+                ldvec<double, VW>(ps, pR(k & 1, jj, h) + pos);
+                ldvec<double, VW>(pn, pR(k & 1, jj + 2, h) + pos);
+                ldvec<double, VW>(pp, pR((k + 1) & 1, jj + 1, h) + pos);
+                const double *Po = pR(k & 1, jj + 1, 1 - h);
+                ldvec<double, VW>(po + 1, Po + pos);
+                po[0] = Po[pos - 1];
+                po[VW + 1] = Po[pos + VW];
+                double out[VW];
+#pragma unroll
+                for (int q = 0; q < VW; q++) {
+                    const double wcoef = h ? eo[q] : eo[q + 1], wval = h ? po[q] : po[q + 1];
+                    const double eval = h ? po[q + 1] : po[q + 2];
+                    double s = 0.0;
+                    s = O::mac(s, tm[q], pm[q]);   // B
+                    s = O::mac(s, ns[q], ps[q]);   // S
+                    s = O::mac(s, wcoef, wval);    // W
+                    s = O::mac(s, dk[q], pc[q]);   // C
+                    s = O::mac(s, ek[q], eval);    // E
+                    s = O::mac(s, nk[q], pn[q]);   // N
+                    s = O::mac(s, tk[q], pp[q]);   // T
+                    out[q] = s;
+                    acc = __dadd_rn(acc, __dmul_rn(pc[q], s));
+                }
+                const long long g = goff(j, k) + pos;
+                *reinterpret_cast<double2 *>(pp_new + g) = make_double2(pc[0], pc[1]);
+                *reinterpret_cast<double2 *>(Ap + g) = make_double2(out[0], out[1]);
+                if (L.xper || L.yper || L.zper) {
+#pragma unroll
+                    for (int q = 0; q < VW; q++) {
+                        const int i = h ? 2 * (pos + q) : 2 * (pos + q) + 1;
+                        if (on_periodic_face(L, i, j, k)) write_images(L, pp_new, i, j, k, pc[q]);
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < VW; q++) {
+                    tm[q] = tk[q];
+                    pm[q] = pc[q];
+                }
+            }
+        }
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+    }
+    // block partial (fixed tree)
+    red[tid] = acc;
+    __syncthreads();
+    for (int s2 = NT / 2; s2 > 0; s2 >>= 1) {
+        if (tid < s2) red[tid] = red[tid] + red[tid + s2];
+        __syncthreads();
+    }
+    if (tid == 0) part[blockIdx.y * gridDim.x + blockIdx.x] = red[0];
+}
+
 // sol += alpha*pp; res -= alpha*Ap; block partial of max|res|
 // (bbmg_class.f90:688-695).  Also prepares the next preconditioner call: the
 // FP32 right-hand side (mixed precision) and a zero correction vector
@@ -1195,6 +1376,29 @@ template <typename T> struct VwMax { static constexpr int value = sizeof(T) == 4
 static bool use_staged(const Lay &L) {
     static const bool off = getenv("BBMG_NO_STAGED") != nullptr;
     return !off && !(L.nx & 1) && (L.nx >> 1) % 4 == 0;
+}
+
+// k-chunks for a k-marching kernel over `jtiles` row tiles: the count in
+// [1, min(nz, 16)] that maximises the fill of the resident slots (waves of
+// SMs x blocks per SM) times kc/(kc+1) for chunks of kc planes (each chunk
+// reads one plane more); the smallest among near-ties; 0 if no block fits.
+static int march_chunks(const void *kern, int nt, size_t smem, int jtiles, int nz) {
+    int oc = 0, nsm = 148, dev = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&oc, kern, nt, smem) != cudaSuccess || oc < 1) return 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const long long slots = (long long)nsm * oc;
+    int best = 1;
+    double beff = 0.0;
+    for (int n = 1; n <= nz && n <= 16; n++) {
+        const long long tot = (long long)jtiles * n, waves = (tot + slots - 1) / slots;
+        const int kc = (nz + n - 1) / n;
+        const double eff = (double)tot / (double)(waves * slots) * kc / (kc + 1.0);
+        if (eff > beff + 0.01) {
+            beff = eff;
+            best = n;
+        }
+    }
+    return best;
 }
 
 template <typename T, int NPT>
@@ -1343,19 +1547,8 @@ cudaError_t launch_residual(const Lay &L, const NbrOff &nb, int npt, const T *op
                     attr[sizeof(T) == 8] = true;
             }
             if (smem <= 200 * 1024 && attr[sizeof(T) == 8]) {
-                int oc = 0;
-                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&oc, k_residual_march<T>, 256, smem) != cudaSuccess ||
-                    oc < 1)
-                    oc = 1;
-                int nsm = 148;
-                {
-                    int dev = 0;
-                    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-                }
-                // about two waves of resident blocks: the second wave evens out the SMs
                 const int jtiles = (L.ny + TY - 1) / TY;
-                int nch = 2 * nsm * oc / jtiles;
-                if (nch > L.nz) nch = L.nz;
+                int nch = march_chunks((const void *)k_residual_march<T>, 256, smem, jtiles, L.nz);
                 if (nch < 1) nch = 1;
                 const int kchunk = (L.nz + nch - 1) / nch;
                 nch = (L.nz + kchunk - 1) / kchunk;
@@ -1505,8 +1698,35 @@ template <typename TZ>
 cudaError_t launch_cg_pap_fused(const Lay &L, const NbrOff &nb, int npt, const double *opr, const TZ *zz,
                                 const double *pp_old, double *pp_new, double *Ap, double *part, CgScal *sc,
                                 cudaStream_t s) {
-    const Geo g = geo_red(L);
     const CgScal *csc = sc;
+    if (npt == 4 && use_staged(L)) {
+        // symmetric 7-point level: k-column marching
+        const int na = L.nx >> 1, TH = na / 2;
+        constexpr int NT = 512;
+        if (!(L.nx & 1) && (na & 1) == 0 && TH >= 8 && 2 * TH <= NT && (TH & (TH - 1)) == 0) {
+            const int TY = NT / (2 * TH), seg = na + 8;
+            const size_t smem = (size_t)seg * 2 *
+                                (2 * ((4 * TY + 1) * sizeof(double) + (TY + 2) * sizeof(TZ) + (TY + 2) * sizeof(double)) +
+                                 2 * (TY + 2) * sizeof(double));
+            static bool attr = false;
+            if (!attr && smem <= 200 * 1024 &&
+                cudaFuncSetAttribute(k_cg_pap_march<TZ, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) ==
+                    cudaSuccess)
+                attr = true;
+            if (attr && smem <= 200 * 1024) {
+                const int jtiles = (L.ny + TY - 1) / TY;
+                const int nch = march_chunks((const void *)k_cg_pap_march<TZ, NT>, NT, smem, jtiles, L.nz);
+                if (nch > 0 && jtiles * nch <= kRedBlocks) {
+                    const int kchunk = (L.nz + nch - 1) / nch, nb2 = (L.nz + kchunk - 1) / kchunk;
+                    BB_CHECK_LAUNCH((launch_k(k_cg_pap_march<TZ, NT>, dim3(jtiles, nb2), dim3(NT), smem, s, L, opr, zz,
+                                              pp_old, pp_new, Ap, csc, part, na, kchunk)));
+                    BB_CHECK_LAUNCH((launch_k(k_cg_pap, dim3(1), dim3(256), 0, s, (const double *)part, jtiles * nb2, sc)));
+                    return cudaSuccess;
+                }
+            }
+        }
+    }
+    const Geo g = geo_red(L);
     if (npt == 4)
         BB_CHECK_LAUNCH((launch_k(k_cg_pap_fused<TZ, 4>, g.grid, g.block, 0, s, L, nb, opr, zz, pp_old, pp_new, Ap, csc, part)));
     else if (npt == 7)

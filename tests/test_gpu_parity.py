@@ -277,3 +277,23 @@ def test_staged_fp32_relax_matches_register_kernel(n, tmp_path):
     za, zb = np.load(a), np.load(b)
     for key in ("v", "r", "f2", "v2", "r2", "r64"):
         assert np.array_equal(za[key], zb[key]), key
+
+
+@pytest.mark.parametrize("precision", [FP64, MIXED], ids=["fp64", "mixed"])
+def test_pcg_solve_k_marching_64(precision):
+    """64^3 two-phase drops with walls in y: the level-1 residual and the CG
+    direction/A*p step run as k-column marching kernels (symmetric 7-point
+    level); the solve matches the oracle's pcg_bbox within the PCG tolerance."""
+    pb = P.drops_poisson(64, seed=6, ndrops=8, rmin=2.0, rmax=6.0)
+    per = (pb.xper, pb.yper, pb.zper)
+    o = OracleBBMG(64, 64, 64, *per, method=PCG_BBOX, rcvg=1e-10)
+    o.setup(pb.stc, pb.opr)
+    xo, ito, ro = o.solve(pb.rhs)
+    g = BBMG(64, 64, 64, *per, method=PCG_BBOX, precision=precision, rcvg=1e-10)
+    g.setup(pb.stc, pb.opr)
+    assert g.info["level1_stencil"] == 4
+    xg, itg, rg, st = g.solve(pb.rhs)
+    assert st == 0 and rg <= 1e-10
+    assert abs(itg - ito) <= (1 if precision == FP64 else 2)
+    d = np.abs(P.remove_mean(xg) - P.remove_mean(xo)).max() / np.abs(P.remove_mean(xo)).max()
+    assert d < (1e-8 if precision == FP64 else 1e-7), d
