@@ -1278,6 +1278,99 @@ __global__ void __launch_bounds__(NT) k_cg_pap_march(Lay L, const double *__rest
     if (tid == 0) part[blockIdx.y * gridDim.x + blockIdx.x] = red[0];
 }
 
+// Streaming kernels over the interior two positions at a time (16-byte
+// double2 accesses): thread t takes chunk t % CH of half-row (t / CH) % 2 of
+// row t / (2 CH), CH = nx/4, grid-stride over a fixed grid, so consecutive
+// threads touch consecutive 16-byte words and every block's partial is
+// accumulated in a fixed order.  Requires nx a multiple of 4.
+template <typename T>
+struct Pair;
+template <> struct Pair<double> { using V = double2; };
+template <> struct Pair<float> { using V = float2; };
+
+__device__ __forceinline__ long long pair_base(const Lay &L, long long t, int CH, int &j, int &k, int &hh, int &c) {
+    c = (int)(t % CH);
+    const long long r2 = t / CH;
+    hh = (int)(r2 & 1);
+    const long long row = r2 >> 1;
+    j = (int)(row % L.ny);
+    k = (int)(row / L.ny);
+    return L.G + L.row(j, k) * L.P + (hh ? L.B0 : 0) + 2 * c;
+}
+
+// block partials of sum a*b (the CG's rho = r . z, bbmg_class.f90:662)
+template <typename TA>
+__global__ void __launch_bounds__(256) k_dot2_part(Lay L, const TA *__restrict__ a, const double *__restrict__ b,
+                                                    double *__restrict__ part) {
+    pdl_entry();
+    __shared__ double sh[256];
+    const int CH = L.nx >> 2;
+    const long long total = (long long)L.ny * L.nz * 2 * CH;
+    double s = 0.0;
+    for (long long t = gtid(); t < total; t += gstride()) {
+        int j, k, hh, c;
+        const long long e = pair_base(L, t, CH, j, k, hh, c);
+        const typename Pair<TA>::V x = *reinterpret_cast<const typename Pair<TA>::V *>(a + e);
+        const double2 y = *reinterpret_cast<const double2 *>(b + e);
+        s = __dadd_rn(s, __dmul_rn((double)x.x, y.x));
+        s = __dadd_rn(s, __dmul_rn((double)x.y, y.y));
+    }
+    s = block_reduce<1>(s, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// k_cg_xr_fused two positions at a time (same per-point arithmetic)
+template <typename TV>
+__global__ void __launch_bounds__(256) k_cg_xr2(Lay L, double *__restrict__ sol, const double *__restrict__ pp,
+                                                 double *__restrict__ res, const double *__restrict__ Ap,
+                                                 const CgScal *__restrict__ sc, float *__restrict__ f32,
+                                                 TV *__restrict__ vzero, double *__restrict__ part) {
+    pdl_entry();
+    __shared__ double sh[256];
+    const double alpha = sc->alpha;
+    const int CH = L.nx >> 2;
+    const long long total = (long long)L.ny * L.nz * 2 * CH;
+    const bool per = L.xper || L.yper || L.zper;
+    double m = 0.0;
+    for (long long t = gtid(); t < total; t += gstride()) {
+        int j, k, hh, c;
+        const long long e = pair_base(L, t, CH, j, k, hh, c);
+        double2 x = *reinterpret_cast<const double2 *>(sol + e);
+        const double2 p = *reinterpret_cast<const double2 *>(pp + e);
+        double2 r = *reinterpret_cast<const double2 *>(res + e);
+        const double2 a = *reinterpret_cast<const double2 *>(Ap + e);
+        x.x = __dadd_rn(x.x, __dmul_rn(alpha, p.x));
+        x.y = __dadd_rn(x.y, __dmul_rn(alpha, p.y));
+        r.x = __dsub_rn(r.x, __dmul_rn(alpha, a.x));
+        r.y = __dsub_rn(r.y, __dmul_rn(alpha, a.y));
+        *reinterpret_cast<double2 *>(sol + e) = x;
+        *reinterpret_cast<double2 *>(res + e) = r;
+        m = max_nan(m, fabs(r.x));
+        m = max_nan(m, fabs(r.y));
+        if (f32) *reinterpret_cast<float2 *>(f32 + e) = make_float2((float)r.x, (float)r.y);
+        typename Pair<TV>::V z;
+        z.x = TV(0);
+        z.y = TV(0);
+        *reinterpret_cast<typename Pair<TV>::V *>(vzero + e) = z;
+        if (per) {
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                const int i = hh ? 2 * (2 * c + q) : 2 * (2 * c + q) + 1;
+                if (on_periodic_face(L, i, j, k)) write_images(L, vzero, i, j, k, TV(0));
+            }
+        }
+    }
+    m = block_reduce<0>(m, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = m;
+}
+
+static unsigned pair_grid(const Lay &L) {
+    const long long total = (long long)L.ny * L.nz * 2 * (L.nx >> 2);
+    long long b = (total + 255) / 256;
+    if (b > kRedBlocks) b = kRedBlocks;
+    return (unsigned)(b < 1 ? 1 : b);
+}
+
 // sol += alpha*pp; res -= alpha*Ap; block partial of max|res|
 // (bbmg_class.f90:688-695).  Also prepares the next preconditioner call: the
 // FP32 right-hand side (mixed precision) and a zero correction vector
@@ -1688,6 +1781,12 @@ cudaError_t launch_to_f32(const double *src, float *dst, long long n, cudaStream
 
 template <typename TZ>
 cudaError_t launch_cg_rho(const Lay &L, const TZ *zz, const double *res, double *part, CgScal *sc, cudaStream_t s) {
+    if (use_staged(L)) {  // nx a multiple of 8: two positions per thread
+        const unsigned nb2 = pair_grid(L);
+        BB_CHECK_LAUNCH((launch_k(k_dot2_part<TZ>, dim3(nb2), dim3(256), 0, s, L, zz, res, part)));
+        BB_CHECK_LAUNCH((launch_k(k_cg_rho, dim3(1), dim3(256), 0, s, (const double *)part, (int)nb2, sc)));
+        return cudaSuccess;
+    }
     const Geo g = geo_red(L);
     BB_CHECK_LAUNCH((launch_k(k_dot_part<TZ, double>, g.grid, g.block, 0, s, L, zz, res, part)));
     BB_CHECK_LAUNCH((launch_k(k_cg_rho, dim3(1), dim3(256), 0, s, (const double *)part, (int)(g.grid.x * g.grid.y), sc)));
@@ -1740,6 +1839,12 @@ cudaError_t launch_cg_pap_fused(const Lay &L, const NbrOff &nb, int npt, const d
 template <typename TV>
 cudaError_t launch_cg_xr_fused(const Lay &L, double *sol, const double *pp, double *res, const double *Ap,
                                const CgScal *sc, float *f32, TV *vzero, double *part, double *out, cudaStream_t s) {
+    if (use_staged(L)) {  // nx a multiple of 8: two positions per thread
+        const unsigned nb2 = pair_grid(L);
+        BB_CHECK_LAUNCH((launch_k(k_cg_xr2<TV>, dim3(nb2), dim3(256), 0, s, L, sol, pp, res, Ap, sc, f32, vzero, part)));
+        BB_CHECK_LAUNCH((launch_k(k_final<0>, dim3(1), dim3(256), 0, s, (const double *)part, (int)nb2, out)));
+        return cudaSuccess;
+    }
     const Geo g = geo_red(L);
     BB_CHECK_LAUNCH((launch_k(k_cg_xr_fused<TV>, g.grid, g.block, 0, s, L, sol, pp, res, Ap, sc, f32, vzero, part)));
     BB_CHECK_LAUNCH((launch_k(k_final<0>, dim3(1), dim3(256), 0, s, (const double *)part, (int)(g.grid.x * g.grid.y), out)));
