@@ -503,8 +503,8 @@ __device__ __forceinline__ void ldvec(T *dst, const T *src) {
 // HBM once per block apart from the two halo rows and one extra plane per
 // chunk: ~31 B per cell against the algorithm's 28.  Terms and order are
 // residual_point's (B, S, W, C, E, N, T): the same bits.  Requires an even
-// nx, na = nx/2 a multiple of VW and TH = na/VW a power of two in [8, 128]
-// (the block holds TY = 128/TH rows).
+// nx, na = nx/2 a multiple of VW and TH = na/VW in [4, 128]; the block of
+// 2*TH*TY threads holds TY = floor(128/TH) rows.
 template <typename T>
 __global__ void __launch_bounds__(256) k_residual_march(Lay L, const T *__restrict__ opr, const T *__restrict__ v,
                                                          const T *__restrict__ f, T *__restrict__ r, int na,
@@ -514,7 +514,7 @@ __global__ void __launch_bounds__(256) k_residual_march(Lay L, const T *__restri
     constexpr int VW = MarchVec<T>::W;
     extern __shared__ __align__(16) unsigned char smraw[];
     T *sm = reinterpret_cast<T *>(smraw);
-    const int TH = na / VW, TY = 128 / TH;
+    const int TH = na / VW, TY = blockDim.x / (2 * TH);
     const int seg = na + 8;                  // position p of a half-row at index p + 4
     const int rows = 5 * TY + 1 + TY + 2;    // C[5][TY], NH, VT[TY+2]
     const int SS = rows * 2 * seg;           // elements per stage
@@ -1099,10 +1099,11 @@ __global__ void __launch_bounds__(256) k_cg_pap_fused(Lay L, NbrOff nb, const do
 
 // pp_new = zz + beta*pp_old and Ap = A pp_new with the block partial of
 // pp_new . Ap, for the symmetric 7-point level-1 operator, by k-column
-// marching (the structure of k_residual_march): a block of NT threads owns TY
-// rows (both halves) of a chunk of k-planes, a thread VW = 2 consecutive
-// positions of one half-row.  A two-slot ring of cp.async stages holds, for
-// plane k, D, E, N, T on the block's rows and N on row j0-1, and zz and pp_old
+// marching (the structure of k_residual_march): a block of 2*TH*TY <= NT
+// threads owns TY = floor(NT/(2 TH)) rows (both halves) of a chunk of
+// k-planes, a thread VW = 2 consecutive positions of one half-row (TH = nx/4).
+// A three-slot ring of cp.async stages, filled two planes ahead, holds for
+// plane k D, E, N, T on the block's rows and N on row j0-1, and zz and pp_old
 // of plane k+1 on rows j0-1 .. j0+TY with the overlap positions; from those
 // the block forms the direction p of plane k+1 in a two-slot shared ring.
 // Ap(k) reads p(k-1) and T(k-1) from registers, p(k) and p(k+1) from the
@@ -1120,7 +1121,7 @@ __global__ void __launch_bounds__(NT) k_cg_pap_march(Lay L, const double *__rest
     using O = Ops<double, true>;
     constexpr int VW = 2;
     const double beta = sc->beta;
-    const int TH = na / VW, TY = NT / (2 * TH);
+    const int TH = na / VW, TY = blockDim.x / (2 * TH);
     const int seg = na + 8;  // position p of a half-row at index p + 4
     const int rowsO = 4 * TY + 1, rowsV = TY + 2;
     const size_t bO = (size_t)rowsO * 2 * seg * sizeof(double), bZ = (size_t)rowsV * 2 * seg * sizeof(TZ);
@@ -1135,7 +1136,7 @@ __global__ void __launch_bounds__(NT) k_cg_pap_march(Lay L, const double *__rest
         return reinterpret_cast<double *>(smraw + sl * bS + bO + bZ) + (rr * 2 + hh) * seg + 4;
     };
     auto pR = [&](int sl, int rr, int hh) {
-        return reinterpret_cast<double *>(smraw + 2 * bS + sl * bP) + (rr * 2 + hh) * seg + 4;
+        return reinterpret_cast<double *>(smraw + 3 * bS + sl * bP) + (rr * 2 + hh) * seg + 4;
     };
     const int tid = threadIdx.x, c = tid % TH, h = (tid / TH) & 1, jj = tid / (2 * TH);
     const int j0 = blockIdx.x * TY, j = j0 + jj;
@@ -1197,20 +1198,23 @@ __global__ void __launch_bounds__(NT) k_cg_pap_march(Lay L, const double *__rest
                 tm[q] = opr[3 * P + g + q];
             }
         }
-        // stage(k) lives in slot (k - k0 + 1) & 1, the direction of plane k in ring slot k & 1
+        // stage(k) lives in slot (k - k0 + 1) % 3, the direction of plane k in ring slot k & 1;
+        // stages run two planes ahead of the computation
         fill(0, k0 - 1);
         commit();
         fill(1, k0);
         commit();
-        asm volatile("cp.async.wait_group 1;" ::: "memory");
+        if (k0 + 1 < k1) fill(2, k0 + 1);
+        commit();
+        asm volatile("cp.async.wait_group 2;" ::: "memory");
         __syncthreads();
         make_p(0, k0 & 1);
         for (int k = k0; k < k1; k++) {
-            const int scur = (k - k0 + 1) & 1, snext = (k - k0) & 1;
+            const int scur = (k - k0 + 1) % 3, sfree = (k - k0) % 3;
             __syncthreads();  // stage(k-1) and p(k-1) are no longer read
-            if (k + 1 < k1) fill(snext, k + 1);
+            if (k + 2 < k1) fill(sfree, k + 2);
             commit();
-            asm volatile("cp.async.wait_group 1;" ::: "memory");
+            asm volatile("cp.async.wait_group 2;" ::: "memory");
             __syncthreads();  // stage(k) complete for every thread
             make_p(scur, (k + 1) & 1);
             __syncthreads();  // p(k+1) complete
@@ -1268,8 +1272,9 @@ __global__ void __launch_bounds__(NT) k_cg_pap_march(Lay L, const double *__rest
         }
         asm volatile("cp.async.wait_group 0;" ::: "memory");
     }
-    // block partial (fixed tree)
+    // block partial (fixed tree over NT slots; threads beyond the block add 0)
     red[tid] = acc;
+    for (int t2 = blockDim.x + tid; t2 < NT; t2 += blockDim.x) red[t2] = 0.0;
     __syncthreads();
     for (int s2 = NT / 2; s2 > 0; s2 >>= 1) {
         if (tid < s2) red[tid] = red[tid] + red[tid + s2];
@@ -1307,13 +1312,28 @@ __global__ void __launch_bounds__(256) k_dot2_part(Lay L, const TA *__restrict__
     const int CH = L.nx >> 2;
     const long long total = (long long)L.ny * L.nz * 2 * CH;
     double s = 0.0;
-    for (long long t = gtid(); t < total; t += gstride()) {
-        int j, k, hh, c;
-        const long long e = pair_base(L, t, CH, j, k, hh, c);
-        const typename Pair<TA>::V x = *reinterpret_cast<const typename Pair<TA>::V *>(a + e);
-        const double2 y = *reinterpret_cast<const double2 *>(b + e);
-        s = __dadd_rn(s, __dmul_rn((double)x.x, y.x));
-        s = __dadd_rn(s, __dmul_rn((double)x.y, y.y));
+    const long long st = gstride();
+    // four chunks' loads in flight per thread; the sum still runs in chunk order
+    for (long long t0 = gtid(); t0 < total; t0 += 4 * st) {
+        typename Pair<TA>::V x[4];
+        double2 y[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const long long t = t0 + u * st;
+            if (t < total) {
+                int j, k, hh, c;
+                const long long e = pair_base(L, t, CH, j, k, hh, c);
+                x[u] = *reinterpret_cast<const typename Pair<TA>::V *>(a + e);
+                y[u] = *reinterpret_cast<const double2 *>(b + e);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            if (t0 + u * st < total) {
+                s = __dadd_rn(s, __dmul_rn((double)x[u].x, y[u].x));
+                s = __dadd_rn(s, __dmul_rn((double)x[u].y, y[u].y));
+            }
+        }
     }
     s = block_reduce<1>(s, sh);
     if (threadIdx.x == 0) part[blockIdx.x] = s;
@@ -1630,8 +1650,8 @@ cudaError_t launch_residual(const Lay &L, const NbrOff &nb, int npt, const T *op
     if (f && npt == 4 && use_staged(L)) {
         constexpr int VW = MarchVec<T>::W;
         const int TH = na / VW;
-        if (!(L.nx & 1) && na % VW == 0 && TH >= 8 && TH <= 128 && (TH & (TH - 1)) == 0) {
-            const int TY = 128 / TH, seg = na + 8;
+        if (!(L.nx & 1) && na % VW == 0 && TH >= 4 && TH <= 128) {
+            const int TY = 128 / TH, seg = na + 8, nthr = 2 * TH * TY;
             const size_t smem = sizeof(T) * (size_t)seg * 2 * (5 * TY + 1 + TY + 2) * 3;
             static bool attr[2] = {false, false};
             if (smem <= 200 * 1024 && !attr[sizeof(T) == 8]) {
@@ -1641,12 +1661,12 @@ cudaError_t launch_residual(const Lay &L, const NbrOff &nb, int npt, const T *op
             }
             if (smem <= 200 * 1024 && attr[sizeof(T) == 8]) {
                 const int jtiles = (L.ny + TY - 1) / TY;
-                int nch = march_chunks((const void *)k_residual_march<T>, 256, smem, jtiles, L.nz);
+                int nch = march_chunks((const void *)k_residual_march<T>, nthr, smem, jtiles, L.nz);
                 if (nch < 1) nch = 1;
                 const int kchunk = (L.nz + nch - 1) / nch;
                 nch = (L.nz + kchunk - 1) / kchunk;
-                BB_CHECK_LAUNCH((launch_k(k_residual_march<T>, dim3(jtiles, nch), dim3(256), smem, s, L, opr, v, f, r,
-                                          na, kchunk)));
+                BB_CHECK_LAUNCH((launch_k(k_residual_march<T>, dim3(jtiles, nch), dim3(nthr), smem, s, L, opr, v, f,
+                                          r, na, kchunk)));
                 return cudaSuccess;
             }
         }
@@ -1802,22 +1822,23 @@ cudaError_t launch_cg_pap_fused(const Lay &L, const NbrOff &nb, int npt, const d
         // symmetric 7-point level: k-column marching
         const int na = L.nx >> 1, TH = na / 2;
         constexpr int NT = 512;
-        if (!(L.nx & 1) && (na & 1) == 0 && TH >= 8 && 2 * TH <= NT && (TH & (TH - 1)) == 0) {
-            const int TY = NT / (2 * TH), seg = na + 8;
+        if (!(L.nx & 1) && (na & 1) == 0 && TH >= 4 && 2 * TH <= NT) {
+            const int TY = NT / (2 * TH), seg = na + 8, nthr = 2 * TH * TY;
             const size_t smem = (size_t)seg * 2 *
-                                (2 * ((4 * TY + 1) * sizeof(double) + (TY + 2) * sizeof(TZ) + (TY + 2) * sizeof(double)) +
+                                (3 * ((4 * TY + 1) * sizeof(double) + (TY + 2) * sizeof(TZ) + (TY + 2) * sizeof(double)) +
                                  2 * (TY + 2) * sizeof(double));
+            constexpr size_t kMaxSmem = 220 * 1024;  // + 4 KB static: under the 227 KB a block may hold
             static bool attr = false;
-            if (!attr && smem <= 200 * 1024 &&
-                cudaFuncSetAttribute(k_cg_pap_march<TZ, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) ==
+            if (!attr && smem <= kMaxSmem &&
+                cudaFuncSetAttribute(k_cg_pap_march<TZ, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem) ==
                     cudaSuccess)
                 attr = true;
-            if (attr && smem <= 200 * 1024) {
+            if (attr && smem <= kMaxSmem) {
                 const int jtiles = (L.ny + TY - 1) / TY;
-                const int nch = march_chunks((const void *)k_cg_pap_march<TZ, NT>, NT, smem, jtiles, L.nz);
+                const int nch = march_chunks((const void *)k_cg_pap_march<TZ, NT>, nthr, smem, jtiles, L.nz);
                 if (nch > 0 && jtiles * nch <= kRedBlocks) {
                     const int kchunk = (L.nz + nch - 1) / nch, nb2 = (L.nz + kchunk - 1) / kchunk;
-                    BB_CHECK_LAUNCH((launch_k(k_cg_pap_march<TZ, NT>, dim3(jtiles, nb2), dim3(NT), smem, s, L, opr, zz,
+                    BB_CHECK_LAUNCH((launch_k(k_cg_pap_march<TZ, NT>, dim3(jtiles, nb2), dim3(nthr), smem, s, L, opr, zz,
                                               pp_old, pp_new, Ap, csc, part, na, kchunk)));
                     BB_CHECK_LAUNCH((launch_k(k_cg_pap, dim3(1), dim3(256), 0, s, (const double *)part, jtiles * nb2, sc)));
                     return cudaSuccess;

@@ -14,6 +14,13 @@ from nga2_b200.bbmg import BBMG, FP64, MIXED, PCG_BBOX
 
 n, out = int(sys.argv[1]), sys.argv[2]
 pb = P.drops_poisson(n, seed=4, ndrops=6, rmin=2.0, rmax=5.0)  # n a power of 2: exactly symmetric
+if n & (n - 1):
+    # 1/n is not exact in binary: make W, S, B the E, N, T of the neighbours
+    # exactly (periodic x and z wrap; the wall faces in y are zero both ways)
+    o = pb.opr
+    o[..., 2] = np.roll(o[..., 1], 1, axis=2)
+    o[..., 4] = np.roll(o[..., 3], 1, axis=1)
+    o[..., 6] = np.roll(o[..., 5], 1, axis=0)
 g = BBMG(n, n, n, pb.xper, pb.yper, pb.zper, method=PCG_BBOX, precision=MIXED)
 g.setup(pb.stc, pb.opr)
 assert g.info["level1_stencil"] == 4

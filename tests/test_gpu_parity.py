@@ -259,7 +259,7 @@ def test_residual_norm_rhs(method, precision):
     assert it_rhs < it_ref and it_rhs < it0, (it_rhs, it_ref, it0)
 
 
-@pytest.mark.parametrize("n", [32, 64])
+@pytest.mark.parametrize("n", [32, 48, 64])
 def test_staged_fp32_relax_matches_register_kernel(n, tmp_path):
     """The shared-memory-staged FP32 kernels (level-1 residual, restriction and
     prolongation, 27-point colours and residual on level 2) give the same bits as the
@@ -280,16 +280,25 @@ def test_staged_fp32_relax_matches_register_kernel(n, tmp_path):
 
 
 @pytest.mark.parametrize("precision", [FP64, MIXED], ids=["fp64", "mixed"])
-def test_pcg_solve_k_marching_64(precision):
-    """64^3 two-phase drops with walls in y: the level-1 residual and the CG
+@pytest.mark.parametrize("n", [48, 64])
+def test_pcg_solve_k_marching(n, precision):
+    """Two-phase drops with walls in y: the level-1 residual and the CG
     direction/A*p step run as k-column marching kernels (symmetric 7-point
-    level); the solve matches the oracle's pcg_bbox within the PCG tolerance."""
-    pb = P.drops_poisson(64, seed=6, ndrops=8, rmin=2.0, rmax=6.0)
+    level; at 48^3 the operator is symmetrised exactly and the blocks hold a
+    non-power-of-two number of rows); the solve matches the oracle's pcg_bbox
+    within the PCG tolerance."""
+    pb = P.drops_poisson(n, seed=6, ndrops=8, rmin=2.0, rmax=6.0)
+    if n & (n - 1):
+        o7 = pb.opr
+        o7[..., 2] = np.roll(o7[..., 1], 1, axis=2)
+        o7[..., 4] = np.roll(o7[..., 3], 1, axis=1)
+        o7[..., 6] = np.roll(o7[..., 5], 1, axis=0)
+        pb.rhs -= pb.rhs.mean()
     per = (pb.xper, pb.yper, pb.zper)
-    o = OracleBBMG(64, 64, 64, *per, method=PCG_BBOX, rcvg=1e-10)
+    o = OracleBBMG(n, n, n, *per, method=PCG_BBOX, rcvg=1e-10)
     o.setup(pb.stc, pb.opr)
     xo, ito, ro = o.solve(pb.rhs)
-    g = BBMG(64, 64, 64, *per, method=PCG_BBOX, precision=precision, rcvg=1e-10)
+    g = BBMG(n, n, n, *per, method=PCG_BBOX, precision=precision, rcvg=1e-10)
     g.setup(pb.stc, pb.opr)
     assert g.info["level1_stencil"] == 4
     xg, itg, rg, st = g.solve(pb.rhs)
