@@ -99,6 +99,7 @@ struct bbmg_handle {
     long long bytes = 0;
     std::string err;
     bbmg_info info{};
+    unsigned l1_planes = 0;  // planes of the level-1 27-point storage the last scatter wrote (0: none yet)
 };
 
 static thread_local std::string g_create_err;
@@ -583,15 +584,26 @@ int bbmg_setup(bbmg_handle *h, int nst, const int *stc, const double *opr) {
         if (st) return st;
     }
     CU(h, cudaMemcpyAsync(h->d_stc, stc, sizeof(int) * 3 * nst, cudaMemcpyHostToDevice, s));
-    // ils scatter + identity overlap + periodic copy (ils_class.f90:247-256, bbmg_class.f90:937-950)
-    CU(h, setup_scatter(L1, src, nst, g, h->d_stc, l1.opr27, s));
-    CU(h, wrap_planes(L1, l1.opr27, 27, s));
+    // ils scatter + identity overlap + periodic copy (ils_class.f90:247-256, bbmg_class.f90:937-950).
+    // Only the planes the stencil touches (and the centre, which carries the
+    // overlap's identity) are written; the other planes of the 27-point
+    // level-1 storage are zeroed when the set of planes changes and then stay
+    // zero, so the prolongation and A*P of level 1 skip them.
+    unsigned smask = 1u << kCentre27;
+    for (int st = 0; st < nst; st++) smask |= 1u << q27(stc[3 * st], stc[3 * st + 1], stc[3 * st + 2]);
+    if (smask != h->l1_planes) {
+        CU(h, cudaMemsetAsync(l1.opr27, 0, sizeof(double) * 27 * (size_t)L1.plane, s));
+        h->l1_planes = smask;
+    }
+    CU(h, setup_scatter(L1, src, nst, g, h->d_stc, l1.opr27, smask, s));
+    CU(h, wrap_planes_mask(L1, l1.opr27, smask, s));
     // hierarchy (bbmg_class.f90:952-959)
     for (int n = 2; n <= h->nlvl; n++) {
         Level &F = h->lv[n - 1], &C = h->lv[n];
-        CU(h, setup_prolongation(F.L, F.opr27, F.c2f, s));
+        const unsigned fmask = n == 2 ? smask : 0x7FFFFFFu;
+        CU(h, setup_prolongation(F.L, F.opr27, F.c2f, fmask, s));
         CU(h, setup_restriction(F.L, C.L, F.c2f, C.f2c, s));
-        CU(h, setup_operator(F.L, C.L, F.opr27, F.c2f, C.f2c, F.oprc2f, C.opr27, s));
+        CU(h, setup_operator(F.L, C.L, F.opr27, F.c2f, C.f2c, F.oprc2f, C.opr27, fmask, s));
     }
     // dense coarsest problem (bbmg_class.f90:961, 1307-1385)
     CU(h, setup_direct(h->lv[h->nlvl].L, h->lv[h->nlvl].opr27, h->OP, h->LU, h->piv, h->pinned, h->d_info, s));

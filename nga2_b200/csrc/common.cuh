@@ -119,6 +119,38 @@ BB_HD void any_cell(const Lay &L, long long t, int &i, int &j, int &k) {
     i = ti < nodd ? 2 * ti - 1 : 2 * (ti - nodd);
 }
 
+// Enumeration of the overlap shell only: the planes k = -1 and k = nz, then
+// the rows j = -1 and j = ny of the interior planes, then the cells i = -1
+// and i = nx of the interior rows.
+BB_HD long long shell_cells(const Lay &L) {
+    return 2LL * (L.nx + 2) * (L.ny + 2) + 2LL * (L.nx + 2) * L.nz + 2LL * L.ny * L.nz;
+}
+BB_HD void shell_cell(const Lay &L, long long t, int &i, int &j, int &k) {
+    const long long A = (long long)(L.nx + 2) * (L.ny + 2);
+    if (t < 2 * A) {
+        k = t < A ? -1 : L.nz;
+        const long long r = t % A;
+        i = (int)(r % (L.nx + 2)) - 1;
+        j = (int)(r / (L.nx + 2)) - 1;
+        return;
+    }
+    t -= 2 * A;
+    const long long B = (long long)(L.nx + 2) * L.nz;
+    if (t < 2 * B) {
+        j = t < B ? -1 : L.ny;
+        const long long r = t % B;
+        i = (int)(r % (L.nx + 2)) - 1;
+        k = (int)(r / (L.nx + 2));
+        return;
+    }
+    t -= 2 * B;
+    const long long C = (long long)L.ny * L.nz;
+    i = t < C ? -1 : L.nx;
+    const long long r = t % C;
+    j = (int)(r % L.ny);
+    k = (int)(r / L.ny);
+}
+
 // Write `val` into every periodic image of interior cell (i,j,k) held in the
 // overlap, reproducing the reference's vsync after a write of the interior
 // (bbmg_class.f90:1388-1554 on one rank).

@@ -15,7 +15,7 @@ namespace bbmg {
 // 27-point layout (ils_class.f90:247-256), identity in the overlap
 // (bbmg_class.f90:937-949).  src is (nst, nx+2g, ny+2g, nz+2g) Fortran order.
 __global__ void k_scatter_operator(Lay L, const double *__restrict__ src, int nst, int g,
-                                   const int *__restrict__ stc, double *__restrict__ opr) {
+                                   const int *__restrict__ stc, double *__restrict__ opr, unsigned wmask) {
     long long total = (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
     const long long sx = nst, sy = sx * (L.nx + 2 * g), sz = sy * (L.ny + 2 * g);
     for (long long t = gtid(); t < total; t += gstride()) {
@@ -37,7 +37,8 @@ __global__ void k_scatter_operator(Lay L, const double *__restrict__ src, int ns
             o[kCentre27] = 1.0;
         }
 #pragma unroll
-        for (int q = 0; q < 27; q++) opr[q * L.plane + id] = o[q];
+        for (int q = 0; q < 27; q++)
+            if ((wmask >> q) & 1u) opr[q * L.plane + id] = o[q];
     }
 }
 
@@ -48,26 +49,39 @@ __global__ void k_scatter_operator(Lay L, const double *__restrict__ src, int ns
 // with a coordinate outside the interior of a periodic direction holds the
 // value of the cell obtained by wrapping those coordinates.  The sources are
 // never themselves periodic images, so one gather pass reproduces it.
-__global__ void k_wrap(Lay L, double *__restrict__ a, int nplanes) {
-    long long total = (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
+// Only the overlap shell is visited (2 ((nx+2)(ny+2) + (nx+2) nz + ny nz)
+// cells), and only the planes in `mask`.
+__global__ void k_wrap(Lay L, double *__restrict__ a, unsigned mask) {
+    const long long total = shell_cells(L);
     for (long long t = gtid(); t < total; t += gstride()) {
         int i, j, k;
-        any_cell(L, t, i, j, k);
+        shell_cell(L, t, i, j, k);
+        int si = wrap(L.xper, i, L.nx), sj = wrap(L.yper, j, L.ny), sk = wrap(L.zper, k, L.nz);
+        if (si == i && sj == j && sk == k) continue;
+        long long d = L.idx(i, j, k), s = L.idx(si, sj, sk);
+        for (int q = 0; q < 27; q++)
+            if ((mask >> q) & 1u) a[q * L.plane + d] = a[q * L.plane + s];
+    }
+}
+__global__ void k_wrap_f(Lay L, float *__restrict__ a, int nplanes) {
+    const long long total = shell_cells(L);
+    for (long long t = gtid(); t < total; t += gstride()) {
+        int i, j, k;
+        shell_cell(L, t, i, j, k);
         int si = wrap(L.xper, i, L.nx), sj = wrap(L.yper, j, L.ny), sk = wrap(L.zper, k, L.nz);
         if (si == i && sj == j && sk == k) continue;
         long long d = L.idx(i, j, k), s = L.idx(si, sj, sk);
         for (int q = 0; q < nplanes; q++) a[q * L.plane + d] = a[q * L.plane + s];
     }
 }
-__global__ void k_wrap_f(Lay L, float *__restrict__ a, int nplanes) {
-    long long total = (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
+// zero every plane of the overlap shell (the interior is written by the caller's kernel)
+__global__ void k_zero_shell(Lay L, double *__restrict__ a, int nplanes) {
+    const long long total = shell_cells(L);
     for (long long t = gtid(); t < total; t += gstride()) {
         int i, j, k;
-        any_cell(L, t, i, j, k);
-        int si = wrap(L.xper, i, L.nx), sj = wrap(L.yper, j, L.ny), sk = wrap(L.zper, k, L.nz);
-        if (si == i && sj == j && sk == k) continue;
-        long long d = L.idx(i, j, k), s = L.idx(si, sj, sk);
-        for (int q = 0; q < nplanes; q++) a[q * L.plane + d] = a[q * L.plane + s];
+        shell_cell(L, t, i, j, k);
+        const long long d = L.idx(i, j, k);
+        for (int q = 0; q < nplanes; q++) a[q * L.plane + d] = 0.0;
     }
 }
 
@@ -79,7 +93,7 @@ __device__ __forceinline__ double sgn_clamp(double a) {
 // ---------------------------------------------------------------------------
 // Prolongation, sweep 1: identity and 1-D lines with Shapira lumping
 // (bbmg_class.f90:978-1051).  Every cell including the overlap.
-__global__ void k_prolong_sweep1(Lay L, const double *__restrict__ opr, double *__restrict__ c2f) {
+__global__ void k_prolong_sweep1(Lay L, const double *__restrict__ opr, double *__restrict__ c2f, unsigned mask) {
     const double ratio = 10.0;
     long long total = (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
     for (long long t = gtid(); t < total; t += gstride()) {
@@ -97,6 +111,7 @@ __global__ void k_prolong_sweep1(Lay L, const double *__restrict__ opr, double *
             double m = 0.0, z = 0.0, p = 0.0;  // opr1d(-1), opr1d(0), opr1d(+1)
 #pragma unroll 1
             for (int q = 0; q < 27; q++) {
+                if (!((mask >> q) & 1u)) continue;  // an all-zero plane adds only zeros
                 int li = q % 3 - 1, lj = (q / 3) % 3 - 1, lk = q / 9 - 1;
                 int l = n1 ? li : (n2 ? lj : lk);
                 int ax = n1 ? q27(li, 0, 0) : (n2 ? q27(0, lj, 0) : q27(0, 0, lk));
@@ -124,7 +139,7 @@ __global__ void k_prolong_sweep1(Lay L, const double *__restrict__ opr, double *
 // axis of the reference's inner loop, PB that of its outer loop.
 template <int AXN>
 __device__ __forceinline__ void face_weights(const Lay &L, const double *__restrict__ opr, double *__restrict__ c2f,
-                                             int i, int j, int k) {
+                                             int i, int j, int k, unsigned mask) {
     constexpr int PA = AXN == 0 ? 1 : 0;
     constexpr int PB = AXN == 2 ? 1 : 2;
     const double ratio = 10.0;
@@ -137,6 +152,7 @@ __device__ __forceinline__ void face_weights(const Lay &L, const double *__restr
     for (int e = 0; e < 9; e++) o2[e] = 0.0;
 #pragma unroll 1
     for (int q = 0; q < 27; q++) {
+        if (!((mask >> q) & 1u)) continue;  // an all-zero plane adds only zeros
         int l[3] = {q % 3 - 1, (q / 3) % 3 - 1, q / 9 - 1};
         int la = l[PA], lb = l[PB];
         int lr[3] = {l[0], l[1], l[2]};
@@ -174,21 +190,21 @@ __device__ __forceinline__ void face_weights(const Lay &L, const double *__restr
     for (int t = 0; t < 8; t++) c2f[t * L.plane + id] = c[t];
 }
 
-__global__ void k_prolong_sweep2(Lay L, const double *__restrict__ opr, double *__restrict__ c2f) {
+__global__ void k_prolong_sweep2(Lay L, const double *__restrict__ opr, double *__restrict__ c2f, unsigned mask) {
     long long total = (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
     for (long long t = gtid(); t < total; t += gstride()) {
         int i, j, k;
         any_cell(L, t, i, j, k);
         int n1 = pmod(L.xper, i, L.nx), n2 = pmod(L.yper, j, L.ny), n3 = pmod(L.zper, k, L.nz);
         if (n1 + n2 + n3 != 2) continue;
-        if (n1 == 0) face_weights<0>(L, opr, c2f, i, j, k);
-        else if (n2 == 0) face_weights<1>(L, opr, c2f, i, j, k);
-        else face_weights<2>(L, opr, c2f, i, j, k);
+        if (n1 == 0) face_weights<0>(L, opr, c2f, i, j, k, mask);
+        else if (n2 == 0) face_weights<1>(L, opr, c2f, i, j, k, mask);
+        else face_weights<2>(L, opr, c2f, i, j, k, mask);
     }
 }
 
 // Prolongation, sweep 3: cube centres, interior only (bbmg_class.f90:1161-1194).
-__global__ void k_prolong_sweep3(Lay L, const double *__restrict__ opr, double *__restrict__ c2f) {
+__global__ void k_prolong_sweep3(Lay L, const double *__restrict__ opr, double *__restrict__ c2f, unsigned mask) {
     long long total = (long long)L.nx * L.ny * L.nz;
     for (long long t = gtid(); t < total; t += gstride()) {
         int i, j, k;
@@ -202,7 +218,7 @@ __global__ void k_prolong_sweep3(Lay L, const double *__restrict__ opr, double *
         for (int s = 0; s < 8; s++) c[s] = c2f[s * L.plane + id];
 #pragma unroll 1
         for (int q = 0; q < 27; q++) {
-            if (q == kCentre27) continue;
+            if (q == kCentre27 || !((mask >> q) & 1u)) continue;  // an all-zero plane subtracts only zeros
             int li = q % 3 - 1, lj = (q / 3) % 3 - 1, lk = q / 9 - 1;
             long long nid = L.idx(i + li, j + lj, k + lk);
             double w = opr[q * L.plane + id] / d;
@@ -246,7 +262,7 @@ __global__ void k_restriction_weights(Lay F, Lay C, const double *__restrict__ c
 // Galerkin operator, part 1: oprc2f = A P on the fine interior
 // (bbmg_class.f90:1245-1271).
 __global__ void k_rap_ap(Lay F, const double *__restrict__ opr, const double *__restrict__ c2f,
-                         double *__restrict__ oprc2f) {
+                         double *__restrict__ oprc2f, unsigned mask) {
     long long total = (long long)F.nx * F.ny * F.nz;
     for (long long t = gtid(); t < total; t += gstride()) {
         int fi, fj, fk;
@@ -258,6 +274,7 @@ __global__ void k_rap_ap(Lay F, const double *__restrict__ opr, const double *__
         for (int q = 0; q < 27; q++) acc[q] = 0.0;
 #pragma unroll 1
         for (int q = 0; q < 27; q++) {
+            if (!((mask >> q) & 1u)) continue;  // an all-zero plane adds only zeros
             int li = q % 3 - 1, lj = (q / 3) % 3 - 1, lk = q / 9 - 1;
             int pxl = pmod(F.xper, fi + li, F.nx), pyl = pmod(F.yper, fj + lj, F.ny), pzl = pmod(F.zper, fk + lk, F.nz);
             double o = opr[q * F.plane + id];
@@ -448,37 +465,40 @@ __global__ void k_check_sym7(Lay L, const double *__restrict__ opr, int *flag) {
 // host launchers
 #define BB_LAUNCH_CHECK() do { cudaError_t e_ = cudaGetLastError(); if (e_ != cudaSuccess) return e_; } while (0)
 
-cudaError_t setup_scatter(const Lay &L, const double *src, int nst, int g, const int *stc, double *opr, cudaStream_t s) {
+cudaError_t setup_scatter(const Lay &L, const double *src, int nst, int g, const int *stc, double *opr, unsigned wmask,
+                          cudaStream_t s) {
     long long n = (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
-    k_scatter_operator<<<grid_for(n, 128), 128, 0, s>>>(L, src, nst, g, stc, opr);
+    k_scatter_operator<<<grid_for(n, 128), 128, 0, s>>>(L, src, nst, g, stc, opr, wmask);
+    BB_LAUNCH_CHECK();
+    return cudaSuccess;
+}
+
+cudaError_t wrap_planes_mask(const Lay &L, double *a, unsigned mask, cudaStream_t s) {
+    if (!(L.xper || L.yper || L.zper)) return cudaSuccess;
+    k_wrap<<<grid_for(shell_cells(L), 256), 256, 0, s>>>(L, a, mask);
     BB_LAUNCH_CHECK();
     return cudaSuccess;
 }
 
 cudaError_t wrap_planes(const Lay &L, double *a, int nplanes, cudaStream_t s) {
-    if (!(L.xper || L.yper || L.zper)) return cudaSuccess;
-    long long n = (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
-    k_wrap<<<grid_for(n, 256), 256, 0, s>>>(L, a, nplanes);
-    BB_LAUNCH_CHECK();
-    return cudaSuccess;
+    return wrap_planes_mask(L, a, nplanes >= 32 ? ~0u : ((1u << nplanes) - 1u), s);
 }
 
 cudaError_t wrap_planes(const Lay &L, float *a, int nplanes, cudaStream_t s) {
     if (!(L.xper || L.yper || L.zper)) return cudaSuccess;
-    long long n = (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
-    k_wrap_f<<<grid_for(n, 256), 256, 0, s>>>(L, a, nplanes);
+    k_wrap_f<<<grid_for(shell_cells(L), 256), 256, 0, s>>>(L, a, nplanes);
     BB_LAUNCH_CHECK();
     return cudaSuccess;
 }
 
-cudaError_t setup_prolongation(const Lay &L, const double *opr, double *c2f, cudaStream_t s) {
+cudaError_t setup_prolongation(const Lay &L, const double *opr, double *c2f, unsigned mask, cudaStream_t s) {
     long long na = (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
     long long ni = (long long)L.nx * L.ny * L.nz;
-    k_prolong_sweep1<<<grid_for(na, 128), 128, 0, s>>>(L, opr, c2f);
+    k_prolong_sweep1<<<grid_for(na, 128), 128, 0, s>>>(L, opr, c2f, mask);
     BB_LAUNCH_CHECK();
-    k_prolong_sweep2<<<grid_for(na, 128), 128, 0, s>>>(L, opr, c2f);
+    k_prolong_sweep2<<<grid_for(na, 128), 128, 0, s>>>(L, opr, c2f, mask);
     BB_LAUNCH_CHECK();
-    k_prolong_sweep3<<<grid_for(ni, 128), 128, 0, s>>>(L, opr, c2f);
+    k_prolong_sweep3<<<grid_for(ni, 128), 128, 0, s>>>(L, opr, c2f, mask);
     BB_LAUNCH_CHECK();
     return wrap_planes(L, c2f, 8, s);
 }
@@ -493,14 +513,18 @@ cudaError_t setup_restriction(const Lay &F, const Lay &C, const double *c2f, dou
 }
 
 cudaError_t setup_operator(const Lay &F, const Lay &C, const double *oprF, const double *c2f, const double *f2c,
-                           double *oprc2f, double *oprC, cudaStream_t s) {
-    cudaError_t e = cudaMemsetAsync(oprc2f, 0, sizeof(double) * 27 * F.plane, s);
-    if (e != cudaSuccess) return e;
+                           double *oprc2f, double *oprC, unsigned mask, cudaStream_t s) {
+    cudaError_t e;
+    // the products are written on every interior cell; the overlap is zero
+    // (non-periodic) or the periodic image
+    k_zero_shell<<<grid_for(shell_cells(F), 256), 256, 0, s>>>(F, oprc2f, 27);
+    BB_LAUNCH_CHECK();
     long long nf = (long long)F.nx * F.ny * F.nz;
-    k_rap_ap<<<grid_for(nf, 128), 128, 0, s>>>(F, oprF, c2f, oprc2f);
+    k_rap_ap<<<grid_for(nf, 128), 128, 0, s>>>(F, oprF, c2f, oprc2f, mask);
     BB_LAUNCH_CHECK();
     if ((e = wrap_planes(F, oprc2f, 27, s)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(oprC, 0, sizeof(double) * 27 * C.plane, s)) != cudaSuccess) return e;
+    k_zero_shell<<<grid_for(shell_cells(C), 256), 256, 0, s>>>(C, oprC, 27);
+    BB_LAUNCH_CHECK();
     long long nc = (long long)C.nx * C.ny * C.nz;
     k_rap_rap<<<grid_for(nc, 128), 128, 0, s>>>(F, C, f2c, oprc2f, oprC);
     BB_LAUNCH_CHECK();

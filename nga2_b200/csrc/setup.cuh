@@ -7,13 +7,18 @@
 namespace bbmg {
 
 // setup.cu (FP64)
-cudaError_t setup_scatter(const Lay &L, const double *src, int nst, int g, const int *stc, double *opr, cudaStream_t s);
+// `wmask`/`mask`: 27-bit sets of operator planes (q27 slots); the scatter
+// writes only the planes in wmask (the others hold zeros already), the
+// prolongation and A*P skip planes outside mask (known to be all zero)
+cudaError_t setup_scatter(const Lay &L, const double *src, int nst, int g, const int *stc, double *opr, unsigned wmask,
+                          cudaStream_t s);
 cudaError_t wrap_planes(const Lay &L, double *a, int nplanes, cudaStream_t s);
+cudaError_t wrap_planes_mask(const Lay &L, double *a, unsigned mask, cudaStream_t s);
 cudaError_t wrap_planes(const Lay &L, float *a, int nplanes, cudaStream_t s);
-cudaError_t setup_prolongation(const Lay &L, const double *opr, double *c2f, cudaStream_t s);
+cudaError_t setup_prolongation(const Lay &L, const double *opr, double *c2f, unsigned mask, cudaStream_t s);
 cudaError_t setup_restriction(const Lay &F, const Lay &C, const double *c2f, double *f2c, cudaStream_t s);
 cudaError_t setup_operator(const Lay &F, const Lay &C, const double *oprF, const double *c2f, const double *f2c,
-                           double *oprc2f, double *oprC, cudaStream_t s);
+                           double *oprc2f, double *oprC, unsigned mask, cudaStream_t s);
 cudaError_t check_symmetric7(const Lay &L, const double *opr, int *flag, cudaStream_t s);
 cudaError_t setup_direct(const Lay &L, const double *opr, double *OP, double *LU, int *piv, int *pinned, int *info,
                          cudaStream_t s);

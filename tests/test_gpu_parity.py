@@ -306,3 +306,23 @@ def test_pcg_solve_k_marching(n, precision):
     assert abs(itg - ito) <= (1 if precision == FP64 else 2)
     d = np.abs(P.remove_mean(xg) - P.remove_mean(xo)).max() / np.abs(P.remove_mean(xo)).max()
     assert d < (1e-8 if precision == FP64 else 1e-7), d
+
+
+def test_setup_reuse_across_stencils_bitexact():
+    """One handle set up with a 27-point operator, then a 7-point one, then
+    another 7-point one: the level-1 storage keeps only the planes the stencil
+    writes (the rest is zeroed when the stencil changes), and every setup
+    array still equals a fresh oracle's bit for bit."""
+    dims, per = (16, 12, 10), (True, False, True)
+    stc27, opr27 = P.random_operator(*dims, per, seed=11, full27=True)
+    stc7a, opr7a = P.random_operator(*dims, per, seed=12)
+    stc7b, opr7b = P.random_operator(*dims, per, seed=13)
+    g = BBMG(*dims, *per, method=BBOX)
+    for stc, opr in ((stc27, opr27), (stc7a, opr7a), (stc7b, opr7b)):
+        g.setup(stc, opr)
+        o = OracleBBMG(*dims, *per, method=BBOX)
+        o.setup(stc, opr)
+        for n in range(1, o.nlvl + 1):
+            names = ["opr"] + (["c2f", "oprc2f"] if n < o.nlvl else []) + (["f2c"] if n > 1 else [])
+            for w in names:
+                assert np.array_equal(g.get(n, w), o.get(n, w)), (n, w)
