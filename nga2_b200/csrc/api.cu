@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "../../include/bbmg_b200.h"
+#include "hostcopy.cuh"
 #include "setup.cuh"
 
 using namespace bbmg;
@@ -100,6 +101,7 @@ struct bbmg_handle {
     std::string err;
     bbmg_info info{};
     unsigned l1_planes = 0;  // planes of the level-1 27-point storage the last scatter wrote (0: none yet)
+    HostCopier copier;       // caller host arrays <-> device
 };
 
 static thread_local std::string g_create_err;
@@ -377,6 +379,7 @@ int bbmg_destroy(bbmg_handle *h) {
     dfree(h->sol); dfree(h->pp); dfree(h->pp2); dfree(h->Ap); dfree(h->x2); dfree(h->sc); dfree(h->part); dfree(h->dscal);
     dfree(h->d_opr_in); dfree(h->d_stc); dfree(h->d_io);
     if (h->h_scal) cudaFreeHost(h->h_scal);
+    h->copier.release();
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
@@ -576,7 +579,7 @@ int bbmg_setup(bbmg_handle *h, int nst, const int *stc, const double *opr) {
             if (st) return st;
             h->d_opr_in_n = ncaller * nst;
         }
-        CU(h, cudaMemcpyAsync(h->d_opr_in, opr, sizeof(double) * ncaller * nst, cudaMemcpyHostToDevice, s));
+        CU(h, h->copier.h2d(h->d_opr_in, opr, sizeof(double) * ncaller * nst, s));
         src = h->d_opr_in;
     }
     if (!h->d_stc) {
@@ -718,13 +721,13 @@ int bbmg_solve(bbmg_handle *h, const double *rhs, double *sol, int *it_out, doub
     CU(h, cudaMemsetAsync(l1.v, 0, sizeof(double) * L.plane, s));
     const double *rsrc = rhs;
     if (!rhs_dev) {
-        CU(h, cudaMemcpyAsync(h->d_io, rhs, sizeof(double) * ncaller, cudaMemcpyHostToDevice, s));
+        CU(h, h->copier.h2d(h->d_io, rhs, sizeof(double) * ncaller, s));
         rsrc = h->d_io;
     }
     CU(h, launch_from_caller<double>(L, rsrc, g, l1.f, s));
     const double *xsrc = sol;
     if (!sol_dev) {
-        CU(h, cudaMemcpyAsync(h->d_io, sol, sizeof(double) * ncaller, cudaMemcpyHostToDevice, s));
+        CU(h, h->copier.h2d(h->d_io, sol, sizeof(double) * ncaller, s));
         xsrc = h->d_io;
     }
     CU(h, launch_from_caller<double>(L, xsrc, g, l1.v, s));
@@ -829,7 +832,7 @@ int bbmg_solve(bbmg_handle *h, const double *rhs, double *sol, int *it_out, doub
         // d_io still holds the caller's sol (copied in last), so its overlap
         // layers go back unchanged
         CU(h, launch_to_caller(L, xout, g, h->d_io, s));
-        CU(h, cudaMemcpyAsync(sol, h->d_io, sizeof(double) * ncaller, cudaMemcpyDeviceToHost, s));
+        CU(h, h->copier.d2h(sol, h->d_io, sizeof(double) * ncaller, s));
     }
     if (krylov && status != BBMG_NONFINITE)  // the reference puts the solution back into lvl(1)%v (702)
         CU(h, cudaMemcpyAsync(l1.v, h->sol, sizeof(double) * L.plane, cudaMemcpyDeviceToDevice, s));

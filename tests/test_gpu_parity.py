@@ -326,3 +326,22 @@ def test_setup_reuse_across_stencils_bitexact():
             names = ["opr"] + (["c2f", "oprc2f"] if n < o.nlvl else []) + (["f2c"] if n > 1 else [])
             for w in names:
                 assert np.array_equal(g.get(n, w), o.get(n, w)), (n, w)
+
+
+def test_pageable_host_arrays_match_device():
+    """Arrays larger than one 32 MB staging chunk: the operator, rhs and
+    solution given as pageable numpy arrays (copied through the pinned staging
+    ring by several host threads) give the same bits as device tensors."""
+    import torch
+    n = 176  # 43 MB per vector, 0.3 GB operator
+    pb = P.drops_poisson(n, seed=3, ndrops=8, rmin=3.0, rmax=8.0)
+    per = (pb.xper, pb.yper, pb.zper)
+    g = BBMG(n, n, n, *per, method=PCG_BBOX, precision=MIXED, rcvg=1e-10)
+    g.setup(pb.stc, np.array(pb.opr))
+    xh, ith, rh, sth = g.solve(np.array(pb.rhs), np.zeros(pb.rhs.shape))
+    g.setup(pb.stc, torch.from_numpy(pb.opr).cuda())
+    xd = torch.zeros(pb.rhs.shape, dtype=torch.float64, device="cuda")
+    _, itd, rd, std = g.solve(torch.from_numpy(pb.rhs).cuda(), xd)
+    assert sth == std == 0 and ith == itd and rh == rd
+    assert np.array_equal(xh, xd.cpu().numpy())
+    g.close()
