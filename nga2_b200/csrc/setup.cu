@@ -16,6 +16,12 @@ namespace bbmg {
 // (bbmg_class.f90:937-949).  src is (nst, nx+2g, ny+2g, nz+2g) Fortran order.
 __global__ void k_scatter_operator(Lay L, const double *__restrict__ src, int nst, int g,
                                    const int *__restrict__ stc, double *__restrict__ opr, unsigned wmask) {
+    // slot of every caller stencil entry; each slot's value is the sum of its
+    // entries in stencil order, built one slot at a time so the sums stay in
+    // registers
+    __shared__ int qst[27];
+    for (int st = threadIdx.x; st < nst; st += blockDim.x) qst[st] = q27(stc[3 * st], stc[3 * st + 1], stc[3 * st + 2]);
+    __syncthreads();
     long long total = (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
     const long long sx = nst, sy = sx * (L.nx + 2 * g), sz = sy * (L.ny + 2 * g);
     for (long long t = gtid(); t < total; t += gstride()) {
@@ -23,22 +29,20 @@ __global__ void k_scatter_operator(Lay L, const double *__restrict__ src, int ns
         any_cell(L, t, i, j, k);
         long long id = L.idx(i, j, k);
         bool interior = i >= 0 && i < L.nx && j >= 0 && j < L.ny && k >= 0 && k < L.nz;
-        double o[27];
+        const double *s = src + (long long)(k + g) * sz + (long long)(j + g) * sy + (long long)(i + g) * sx;
 #pragma unroll
-        for (int q = 0; q < 27; q++) o[q] = 0.0;
-        if (interior) {
-            const double *s = src + (long long)(k + g) * sz + (long long)(j + g) * sy + (long long)(i + g) * sx;
+        for (int q = 0; q < 27; q++) {
+            if (!((wmask >> q) & 1u)) continue;
+            double o = 0.0;
+            if (interior) {
 #pragma unroll 1
-            for (int st = 0; st < nst; st++) {
-                int q = q27(stc[3 * st], stc[3 * st + 1], stc[3 * st + 2]);
-                o[q] = __dadd_rn(o[q], s[st]);
+                for (int st = 0; st < nst; st++)
+                    if (qst[st] == q) o = __dadd_rn(o, s[st]);
+            } else if (q == kCentre27) {
+                o = 1.0;
             }
-        } else {
-            o[kCentre27] = 1.0;
+            opr[q * L.plane + id] = o;
         }
-#pragma unroll
-        for (int q = 0; q < 27; q++)
-            if ((wmask >> q) & 1u) opr[q * L.plane + id] = o[q];
     }
 }
 
