@@ -6,7 +6,7 @@
  * a small 3-D U-Net that predicts the pressure increment from the right-hand
  * side and the previous pressure; the network is orchestrated from the host
  * (nga2_b200/learned.py) and always followed by the multigrid solve, which
- * remains the judge of convergence.
+ * still decides convergence.
  *
  * Activations are BF16, channels-last: element (voxel v, channel c) of a view
  * lives at data[v * ld + c]; voxels are ordered (n, d, h, w) with w fastest and

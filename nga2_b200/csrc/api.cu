@@ -1,7 +1,7 @@
 // api.cu -- the C ABI (include/bbmg_b200.h): handle, level hierarchy, setup
 // and the solve drivers (stationary V-cycles, PCG, mixed precision).
 //
-// The drivers follow src/solver/bbmg_class.f90: solve 604-639, cgsolve
+// The solve routines follow src/solver/bbmg_class.f90: solve 604-639, cgsolve
 // 643-703, mgsolve 707-728, cycle 732-776; the ILS wrapper around them follows
 // src/solver/ils_class.f90:162-226 (init), 230-376 (setup), 674-822 (solve).
 // One iteration of a solve is captured once into a CUDA graph and replayed;

@@ -1,7 +1,7 @@
 // hostcopy.cuh -- copies between caller host arrays and device memory.
 //
 // Page-locked host memory is copied by DMA directly.  Pageable memory (the
-// usual case for a Fortran or numpy caller) would go through the driver's
+// usual case for a Fortran or numpy caller) would go through the CUDA driver's
 // single bounce buffer at ~11 GB/s; here it goes through a ring of pinned
 // staging buffers instead: several host threads fill (or drain) one chunk
 // while the copy engine moves the previous one, so the host-side memcpy and
@@ -120,7 +120,7 @@ class HostCopier {
     }
 
     // host src -> device dst, ordered on stream s; src may be reused on return
-    // (pageable chunks are in the staging ring by then, and the driver stages
+    // (pageable chunks are in the staging ring by then, and the CUDA driver stages
     // small pageable copies before returning)
     cudaError_t h2d(void *dst, const void *src, size_t bytes, cudaStream_t s) {
         if (bytes < kChunk || pinned(src)) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);

@@ -1,7 +1,7 @@
 """ctypes front end of the CPU oracle (bbmg_oracle.c).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, ``__graft_entry__.smoke()`` and
-bench.py's CPU-baseline legs as the checker; the product never imports it.
+bench.py's CPU-baseline legs, to check the GPU solver; the product never imports it.
 
 ``OracleBBMG`` mirrors NGA2's ILS bbmg branch (src/solver/ils_class.f90:162-226
 init, 230-376 setup, 674-822 solve): methods ``bbox`` (stationary V-cycles) and

@@ -1,4 +1,4 @@
-"""Pins the CPU oracle (oracle/bbmg_oracle.c) before it is trusted as the checker.
+"""Pins the CPU oracle (oracle/bbmg_oracle.c) before the GPU solver is checked against it.
 
 The reference ships no tests or golden vectors for bbmg and cannot be compiled
 here (Fortran 2008 + MPI + LAPACK), so the restatement is pinned by:
