@@ -92,6 +92,45 @@ int nga_proj_pgrad(nga_proj *p, const double *P, double *Pgradx, double *Pgrady,
 int nga_proj_correct(nga_proj *p, const double *sol, double dt, const double *rho_U, const double *rho_V,
                      const double *rho_W, double *P, double *U, double *V, double *W);
 
+/* get_dmomdt (incomp_class.f90:1021-1159): the time derivatives of rho U,
+ * rho V, rho W on the faces from the convective, viscous and pressure fluxes
+ * (constant density rho; cell-centred viscosity visc, or visc0 everywhere
+ * when visc is NULL), synchronised.  Triply periodic grids only: walls need
+ * the metric adjustments of adjust_metrics (incomp_class.f90:449-700), which
+ * are not implemented (BBMG_BAD_ARGS).  The overlap of U, V, W, P and visc
+ * must hold the periodic images. */
+int nga_proj_dmomdt(nga_proj *p, const double *U, const double *V, const double *W, const double *P, double rho,
+                    const double *visc, double visc0, double *drhoUdt, double *drhoVdt, double *drhoWdt);
+
+/* The mid-time velocity of a sub-iteration (examples/hit simulation.f90:
+ * 282-285): U = 0.5*(U+Uold), V and W likewise, over the whole padded arrays
+ * (so periodic images stay images). */
+int nga_proj_midpoint(nga_proj *p, double *U, double *V, double *W, const double *Uold, const double *Vold,
+                      const double *Wold);
+
+/* The explicit update of a sub-iteration (examples/hit simulation.f90:
+ * 290-325): resU = -2*(rho*U - rho*Uold) + dt*drhoUdt, plus the linear
+ * forcing (force_a*(U - mean[0]))/force_b when force_a != 0 (hit: force_a =
+ * dt*KE0/KE, force_b = 2*tau_eddy), then U = 2*U - Uold + resU/rho; V and W
+ * likewise, over the whole padded arrays.  mean is a host array of 3 and may
+ * be NULL when force_a == 0. */
+int nga_proj_advance(nga_proj *p, double dt, double rho, double *U, double *V, double *W, const double *Uold,
+                     const double *Vold, const double *Wold, const double *drhoUdt, const double *drhoVdt,
+                     const double *drhoWdt, double force_a, double force_b, const double *mean);
+
+/* Flow statistics in one pass over the interior, into the host array
+ * out[10]: out[0..2] the convective CFLs max|U|*dxmi*dt, max|V|*dymi*dt,
+ * max|W|*dzmi*dt and out[3..5] the viscous CFLs max(4*visc*dxi**2/rho)*dt ...
+ * (get_cfl, incomp_class.f90:1497-1540); out[6] the kinetic energy
+ * sum 0.5*(Ui**2+Vi**2+Wi**2) of interp_vel's cell velocities
+ * (incomp_class.f90:1188-1225; hit simulation.f90:299-311); out[7..9] the
+ * volume means of U, V, W (config_class.f90:196-214 / fluid_vol).  visc may
+ * be NULL for visc0 everywhere.  The sums are fixed-order parallel
+ * reductions (round-off from the reference's sequential loops; the maxima
+ * are exact).  Triply periodic grids only. */
+int nga_proj_flow_stats(nga_proj *p, const double *U, const double *V, const double *W, const double *visc,
+                        double visc0, double rho, double dt, double *out);
+
 #ifdef __cplusplus
 }
 #endif

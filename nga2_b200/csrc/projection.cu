@@ -39,6 +39,12 @@ struct nga_proj {
     double *metrics = nullptr;  // one allocation holding all of the above
     double *part = nullptr;     // reduction partials + the mean
     double vol_total = 0.0;
+    // momentum metrics per direction (two layers of the naive extension):
+    // dxi on cells -1..n (index c+1), dxmi and the edge weights itm (of the
+    // value at f-1) and itz (of the value at f) on faces 0..n
+    double *mdi[3] = {nullptr, nullptr, nullptr}, *mdmi[3] = {nullptr, nullptr, nullptr};
+    double *mitm[3] = {nullptr, nullptr, nullptr}, *mitz[3] = {nullptr, nullptr, nullptr};
+    double *mmetrics = nullptr;
 };
 
 namespace {
@@ -333,6 +339,267 @@ void axis_metrics(const double *x, int n, bool per, std::vector<double> &dp0, st
     }
 }
 
+// Momentum metrics of one direction (incomp_class.f90:250-446 with the mesh of
+// sgrid_class.f90:160-254 extended naively by two layers).
+void momentum_metrics(const double *x, int n, std::vector<double> &di, std::vector<double> &dmi,
+                      std::vector<double> &itm, std::vector<double> &itz) {
+    std::vector<double> xe(n + 5), xm(n + 4);  // nodes -2..n+2, cells -2..n+1 at index +2
+    for (int i = 0; i <= n; i++) xe[i + 2] = x[i];
+    for (int m = 1; m >= 0; m--) xe[m] = xe[m + 1] - (xe[3] - xe[2]);
+    for (int m = n + 3; m <= n + 4; m++) xe[m] = xe[m - 1] + (xe[n + 2] - xe[n + 1]);
+    for (int m = 0; m < n + 4; m++) xm[m] = 0.5 * (xe[m] + xe[m + 1]);
+    di.assign(n + 2, 0.0);
+    for (int c = -1; c <= n; c++) di[c + 1] = 1.0 / (xe[c + 3] - xe[c + 2]);
+    dmi.assign(n + 1, 0.0); itm.assign(n + 1, 0.0); itz.assign(n + 1, 0.0);
+    for (int f = 0; f <= n; f++) {
+        dmi[f] = 1.0 / (xm[f + 2] - xm[f + 1]);
+        itm[f] = dmi[f] * (xm[f + 2] - xe[f + 2]);
+        itz[f] = dmi[f] * (xe[f + 2] - xm[f + 1]);
+    }
+}
+
+struct MomM {
+    const double *di[3], *dmi[3], *itm[3], *itz[3];
+};
+
+__device__ __forceinline__ double pa(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double pm(double a, double b) { return __dmul_rn(a, b); }
+// sum(a(:)*b(:)) over two entries, in order
+__device__ __forceinline__ double two(double a0, double b0, double a1, double b1) { return pa(pm(a0, b0), pm(a1, b1)); }
+// sum(itp2d(:,:)*visc(..)) with the lower index (l) fastest
+__device__ __forceinline__ double visc_edge(double lm, double lz, double hm, double hz, double v_mm, double v_zm,
+                                            double v_mz, double v_zz) {
+    double t = pm(pm(lm, hm), v_mm);
+    t = pa(t, pm(pm(lz, hm), v_zm));
+    t = pa(t, pm(pm(lm, hz), v_mz));
+    return pa(t, pm(pm(lz, hz), v_zz));
+}
+// -rho (itp_a Qa) (itp_b Qb) + vi (grd_a Qa + grd_b Qb)
+__device__ __forceinline__ double edge_flux(double rho, double am, double az, double qam, double qa0, double bm,
+                                            double bz, double qbm, double qb0, double dma, double dmb, double vi) {
+    const double a = two(am, qam, az, qa0), b = two(bm, qbm, bz, qb0);
+    const double g = pa(two(-dma, qam, dma, qa0), two(-dmb, qbm, dmb, qb0));
+    return pa(-pm(pm(rho, a), b), pm(vi, g));
+}
+
+// get_dmomdt (incomp_class.f90:1021-1159) on a triply periodic grid, one
+// thread per cell computing the three face derivatives there; every flux is
+// recomputed by the threads that need it (the same bits each time) instead of
+// being stored.  Terms and order follow the reference expression by expression.
+__global__ void __launch_bounds__(kThreads) k_dmomdt(Pad P, MomM M, const double *__restrict__ U,
+                                                      const double *__restrict__ V, const double *__restrict__ W,
+                                                      const double *__restrict__ Pr, double rho,
+                                                      const double *__restrict__ visc, double visc0,
+                                                      double *__restrict__ dU, double *__restrict__ dV,
+                                                      double *__restrict__ dW) {
+    const long long n = (long long)P.nx * P.ny * P.nz;
+    const double c23 = 2.0 / 3.0;
+    const long long sx = 1, sy = P.sy, sz = P.sz;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        cell_of(P, t, i, j, k);
+        const long long e = P.at(i, j, k);
+        auto vs = [&](long long o) { return visc ? visc[o] : visc0; };
+        // divergence at the cell at element o with cell indices (ci, cj, ck)
+        auto divc = [&](long long o, int ci, int cj, int ck) {
+            const double dx = M.di[0][ci + 1], dy = M.di[1][cj + 1], dz = M.di[2][ck + 1];
+            const double a = two(-dx, U[o], dx, U[o + sx]);
+            const double b = two(-dy, V[o], dy, V[o + sy]);
+            const double c = two(-dz, W[o], dz, W[o + sz]);
+            return pa(pa(a, b), c);
+        };
+        // normal flux of component Q along direction d at the cell at element o
+        auto normal = [&](const double *Q, long long st, double dci, long long o, int ci, int cj, int ck) {
+            const double q0 = Q[o], q1 = Q[o + st];
+            const double s1 = two(0.5, q0, 0.5, q1);
+            const double g = two(-dci, q0, dci, q1);
+            const double vt = pm(vs(o), __dsub_rn(pa(g, g), pm(c23, divc(o, ci, cj, ck))));
+            return __dsub_rn(pa(-pm(pm(rho, s1), s1), vt), Pr[o]);
+        };
+        // ---- rho U at x-face i
+        {
+            const double fxm = normal(U, sx, M.di[0][i], e - sx, i - 1, j, k);
+            const double fx0 = normal(U, sx, M.di[0][i + 1], e, i, j, k);
+            double fy[2], fz[2];
+#pragma unroll
+            for (int oy = 0; oy < 2; oy++) {  // xy edge (x-face i, y-face j+oy)
+                const int f = j + oy;
+                const long long o = e + oy * sy;
+                const double vi = visc_edge(M.itm[0][i], M.itz[0][i], M.itm[1][f], M.itz[1][f], vs(o - sx - sy),
+                                            vs(o - sy), vs(o - sx), vs(o));
+                fy[oy] = edge_flux(rho, M.itm[1][f], M.itz[1][f], U[o - sy], U[o], M.itm[0][i], M.itz[0][i], V[o - sx],
+                                   V[o], M.dmi[1][f], M.dmi[0][i], vi);
+            }
+#pragma unroll
+            for (int oz = 0; oz < 2; oz++) {  // xz edge (x-face i, z-face k+oz)
+                const int f = k + oz;
+                const long long o = e + oz * sz;
+                const double vi = visc_edge(M.itm[0][i], M.itz[0][i], M.itm[2][f], M.itz[2][f], vs(o - sx - sz),
+                                            vs(o - sz), vs(o - sx), vs(o));
+                fz[oz] = edge_flux(rho, M.itm[2][f], M.itz[2][f], U[o - sz], U[o], M.itm[0][i], M.itz[0][i], W[o - sx],
+                                   W[o], M.dmi[2][f], M.dmi[0][i], vi);
+            }
+            const double dmx = M.dmi[0][i], dy = M.di[1][j + 1], dz = M.di[2][k + 1];
+            dU[e] = pa(pa(two(-dmx, fxm, dmx, fx0), two(-dy, fy[0], dy, fy[1])), two(-dz, fz[0], dz, fz[1]));
+        }
+        // ---- rho V at y-face j
+        {
+            double fx[2], fz[2];
+#pragma unroll
+            for (int ox = 0; ox < 2; ox++) {  // xy edge (x-face i+ox, y-face j)
+                const int f = i + ox;
+                const long long o = e + ox * sx;
+                const double vi = visc_edge(M.itm[0][f], M.itz[0][f], M.itm[1][j], M.itz[1][j], vs(o - sx - sy),
+                                            vs(o - sy), vs(o - sx), vs(o));
+                fx[ox] = edge_flux(rho, M.itm[0][f], M.itz[0][f], V[o - sx], V[o], M.itm[1][j], M.itz[1][j], U[o - sy],
+                                   U[o], M.dmi[0][f], M.dmi[1][j], vi);
+            }
+            const double fym = normal(V, sy, M.di[1][j], e - sy, i, j - 1, k);
+            const double fy0 = normal(V, sy, M.di[1][j + 1], e, i, j, k);
+#pragma unroll
+            for (int oz = 0; oz < 2; oz++) {  // yz edge (y-face j, z-face k+oz)
+                const int f = k + oz;
+                const long long o = e + oz * sz;
+                const double vi = visc_edge(M.itm[1][j], M.itz[1][j], M.itm[2][f], M.itz[2][f], vs(o - sy - sz),
+                                            vs(o - sz), vs(o - sy), vs(o));
+                fz[oz] = edge_flux(rho, M.itm[2][f], M.itz[2][f], V[o - sz], V[o], M.itm[1][j], M.itz[1][j], W[o - sy],
+                                   W[o], M.dmi[2][f], M.dmi[1][j], vi);
+            }
+            const double dx = M.di[0][i + 1], dmy = M.dmi[1][j], dz = M.di[2][k + 1];
+            dV[e] = pa(pa(two(-dx, fx[0], dx, fx[1]), two(-dmy, fym, dmy, fy0)), two(-dz, fz[0], dz, fz[1]));
+        }
+        // ---- rho W at z-face k
+        {
+            double fx[2], fy[2];
+#pragma unroll
+            for (int ox = 0; ox < 2; ox++) {  // xz edge (x-face i+ox, z-face k)
+                const int f = i + ox;
+                const long long o = e + ox * sx;
+                const double vi = visc_edge(M.itm[0][f], M.itz[0][f], M.itm[2][k], M.itz[2][k], vs(o - sx - sz),
+                                            vs(o - sz), vs(o - sx), vs(o));
+                fx[ox] = edge_flux(rho, M.itm[0][f], M.itz[0][f], W[o - sx], W[o], M.itm[2][k], M.itz[2][k], U[o - sz],
+                                   U[o], M.dmi[0][f], M.dmi[2][k], vi);
+            }
+#pragma unroll
+            for (int oy = 0; oy < 2; oy++) {  // yz edge (y-face j+oy, z-face k)
+                const int f = j + oy;
+                const long long o = e + oy * sy;
+                const double vi = visc_edge(M.itm[1][f], M.itz[1][f], M.itm[2][k], M.itz[2][k], vs(o - sy - sz),
+                                            vs(o - sz), vs(o - sy), vs(o));
+                fy[oy] = edge_flux(rho, M.itm[1][f], M.itz[1][f], W[o - sy], W[o], M.itm[2][k], M.itz[2][k], V[o - sz],
+                                   V[o], M.dmi[1][f], M.dmi[2][k], vi);
+            }
+            const double fzm = normal(W, sz, M.di[2][k], e - sz, i, j, k - 1);
+            const double fz0 = normal(W, sz, M.di[2][k + 1], e, i, j, k);
+            const double dx = M.di[0][i + 1], dy = M.di[1][j + 1], dmz = M.dmi[2][k];
+            dW[e] = pa(pa(two(-dx, fx[0], dx, fx[1]), two(-dy, fy[0], dy, fy[1])), two(-dmz, fzm, dmz, fz0));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The whole-array updates of a sub-iteration of the time loop (the hit
+// example, simulation.f90:283-341): elementwise over the padded arrays, like
+// the reference's array statements, so the overlap stays the periodic image.
+
+struct Vel3 {
+    double *a[3];
+};
+struct CVel3 {
+    const double *a[3];
+};
+
+// U = 0.5*(U + Uold)
+__global__ void __launch_bounds__(kThreads) k_midpoint(long long n, Vel3 U, CVel3 Uo) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) U.a[c][t] = pm(0.5, pa(U.a[c][t], Uo.a[c][t]));
+    }
+}
+
+// res = -2*(rho*U - rho*Uold) + dt*drhoUdt [+ (fa*(U - mean))/fb];
+// U = 2*U - Uold + res/rho
+__global__ void __launch_bounds__(kThreads) k_advance(long long n, double dt, double rho, Vel3 U, CVel3 Uo,
+                                                      CVel3 dU, double fa, double fb, double m0, double m1,
+                                                      double m2) {
+    const double mean[3] = {m0, m1, m2};
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const double u = U.a[c][t], uo = Uo.a[c][t];
+            double r = pa(pm(-2.0, __dsub_rn(pm(rho, u), pm(rho, uo))), pm(dt, dU.a[c][t]));
+            if (fa != 0.0) r = pa(r, __ddiv_rn(pm(fa, __dsub_rn(u, mean[c])), fb));
+            U.a[c][t] = pa(__dsub_rn(pm(2.0, u), uo), __ddiv_rn(r, rho));
+        }
+    }
+}
+
+// Flow statistics, block partials over the interior cells (fixed grid, fixed
+// per-thread order): q 0-2 max|U|*dxmi (get_cfl, incomp_class.f90:1497-1540),
+// 3-5 max 4*visc*dxi**2/rho, 6 sum 0.5*(Ui**2+Vi**2+Wi**2) with the
+// interp_vel midpoints (incomp_class.f90:1188-1225), 7-9 sum vol*U
+// (config_class.f90:196-214 with VF = 1).
+constexpr int kStat = 10;
+
+__global__ void __launch_bounds__(kThreads) k_stats(Pad P, Metrics Mp, MomM M, const double *__restrict__ U,
+                                                    const double *__restrict__ V, const double *__restrict__ W,
+                                                    const double *__restrict__ visc, double visc0, double rho,
+                                                    double *__restrict__ part) {
+    __shared__ double sh[kStat][kThreads];
+    double acc[kStat];
+#pragma unroll
+    for (int q = 0; q < kStat; q++) acc[q] = 0.0;
+    const long long n = (long long)P.nx * P.ny * P.nz;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        cell_of(P, t, i, j, k);
+        const long long e = P.at(i, j, k);
+        const double u = U[e], v = V[e], w = W[e];
+        acc[0] = fmax(acc[0], pm(fabs(u), M.dmi[0][i]));
+        acc[1] = fmax(acc[1], pm(fabs(v), M.dmi[1][j]));
+        acc[2] = fmax(acc[2], pm(fabs(w), M.dmi[2][k]));
+        const double vis = visc ? visc[e] : visc0;
+        const double dxi = M.di[0][i + 1], dyi = M.di[1][j + 1], dzi = M.di[2][k + 1];
+        acc[3] = fmax(acc[3], __ddiv_rn(pm(pm(4.0, vis), pm(dxi, dxi)), rho));
+        acc[4] = fmax(acc[4], __ddiv_rn(pm(pm(4.0, vis), pm(dyi, dyi)), rho));
+        acc[5] = fmax(acc[5], __ddiv_rn(pm(pm(4.0, vis), pm(dzi, dzi)), rho));
+        const double ui = pa(pm(0.5, u), pm(0.5, U[e + 1]));
+        const double vi = pa(pm(0.5, v), pm(0.5, V[e + P.sy]));
+        const double wi = pa(pm(0.5, w), pm(0.5, W[e + P.sz]));
+        acc[6] = pa(acc[6], pm(0.5, pa(pa(pm(ui, ui), pm(vi, vi)), pm(wi, wi))));
+        const double vol = pm(pm(Mp.dx[i], Mp.dy[j]), Mp.dz[k]);
+        acc[7] = pa(acc[7], pm(vol, u));
+        acc[8] = pa(acc[8], pm(vol, v));
+        acc[9] = pa(acc[9], pm(vol, w));
+    }
+#pragma unroll
+    for (int q = 0; q < kStat; q++) sh[q][threadIdx.x] = acc[q];
+    __syncthreads();
+    for (int h = kThreads / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) {
+#pragma unroll
+            for (int q = 0; q < kStat; q++)
+                sh[q][threadIdx.x] = q < 6 ? fmax(sh[q][threadIdx.x], sh[q][threadIdx.x + h])
+                                           : pa(sh[q][threadIdx.x], sh[q][threadIdx.x + h]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < kStat) part[threadIdx.x * kRedBlocks + blockIdx.x] = sh[threadIdx.x][0];
+}
+
+// final: maxima times dt, the kinetic energy, sums / fluid_vol, into
+// part[kStat*kRedBlocks + q]; one warp per statistic
+__global__ void __launch_bounds__(kStat * 32) k_stats_final(double *__restrict__ part, double dt, double fluid_vol) {
+    const int q = threadIdx.x / 32, l = threadIdx.x % 32;
+    double s = 0.0;
+    for (int b = l; b < kRedBlocks; b += 32) s = q < 6 ? fmax(s, part[q * kRedBlocks + b]) : pa(s, part[q * kRedBlocks + b]);
+    for (int o = 16; o > 0; o >>= 1) {
+        const double x = __shfl_down_sync(0xffffffffu, s, o);
+        s = q < 6 ? fmax(s, x) : pa(s, x);
+    }
+    if (l == 0) part[kStat * kRedBlocks + q] = q < 6 ? pm(s, dt) : (q == 6 ? s : __ddiv_rn(s, fluid_vol));
+}
+
 int check_dev(const void *a, const char *name) {
     if (!a) return pfail(BBMG_BAD_ARGS, "%s is NULL", name);
     if (!on_device(a)) return pfail(BBMG_BAD_ARGS, "%s is not a device pointer", name);
@@ -381,7 +648,7 @@ extern "C" int nga_proj_create(const bbmg_grid *grid, const double *x, const dou
         }
     }
     cudaError_t e = cudaMalloc((void **)&p->metrics, host.size() * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc((void **)&p->part, (kRedBlocks + 1) * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&p->part, (kStat * kRedBlocks + kStat) * sizeof(double));
     if (e == cudaSuccess) e = cudaMemcpy(p->metrics, host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -396,6 +663,33 @@ extern "C" int nga_proj_create(const bbmg_grid *grid, const double *x, const dou
         p->du1[a] = p->metrics + off[a][3];
         p->d[a] = p->metrics + off[a][4];
     }
+    {
+        std::vector<double> mh;
+        size_t mo[3][4];
+        for (int a = 0; a < 3; a++) {
+            std::vector<double> di, dmi, itm, itz;
+            momentum_metrics(xs[a], ns[a], di, dmi, itm, itz);
+            const std::vector<double> *parts[4] = {&di, &dmi, &itm, &itz};
+            for (int q = 0; q < 4; q++) {
+                mo[a][q] = mh.size();
+                mh.insert(mh.end(), parts[q]->begin(), parts[q]->end());
+            }
+        }
+        cudaError_t e2 = cudaMalloc((void **)&p->mmetrics, mh.size() * sizeof(double));
+        if (e2 == cudaSuccess) e2 = cudaMemcpy(p->mmetrics, mh.data(), mh.size() * sizeof(double), cudaMemcpyHostToDevice);
+        if (e2 != cudaSuccess) {
+            cudaGetLastError();
+            nga_proj_destroy(p);
+            return pfail(e2 == cudaErrorMemoryAllocation ? BBMG_NO_MEMORY : BBMG_CUDA, "momentum metrics: %s",
+                         cudaGetErrorString(e2));
+        }
+        for (int a = 0; a < 3; a++) {
+            p->mdi[a] = p->mmetrics + mo[a][0];
+            p->mdmi[a] = p->mmetrics + mo[a][1];
+            p->mitm[a] = p->mmetrics + mo[a][2];
+            p->mitz[a] = p->mmetrics + mo[a][3];
+        }
+    }
     // fluid_vol = vol_total = xL*yL*zL (sgrid_class.f90:260-263; config_class.f90:129)
     const double xL = x[g.nx] - x[0], yL = y[g.ny] - y[0], zL = z[g.nz] - z[0];
     p->vol_total = xL * yL * zL;
@@ -408,6 +702,7 @@ extern "C" int nga_proj_destroy(nga_proj *p) {
     cudaSetDevice(p->device);
     if (p->metrics) cudaFree(p->metrics);
     if (p->part) cudaFree(p->part);
+    if (p->mmetrics) cudaFree(p->mmetrics);
     delete p;
     return BBMG_OK;
 }
@@ -505,4 +800,116 @@ extern "C" int nga_proj_correct(nga_proj *p, const double *sol, double dt, const
                                                          W);
     PCU(cudaGetLastError());
     return sync_arrays(p, U, V, W, pres);
+}
+
+extern "C" int nga_proj_dmomdt(nga_proj *p, const double *U, const double *V, const double *W, const double *P_,
+                               double rho, const double *visc, double visc0, double *dU, double *dV, double *dW) {
+    if (!p) return pfail(BBMG_BAD_ARGS, "null projection handle");
+    if (!(p->g.xper && p->g.yper && p->g.zper))
+        return pfail(BBMG_BAD_ARGS, "nga_proj_dmomdt needs a triply periodic grid (walls need the metric "
+                                    "adjustments of adjust_metrics, which are not implemented)");
+    PCHK(check_dev(U, "U"));
+    PCHK(check_dev(V, "V"));
+    PCHK(check_dev(W, "W"));
+    PCHK(check_dev(P_, "P"));
+    PCHK(check_opt(visc, "visc"));
+    PCHK(check_dev(dU, "drhoUdt"));
+    PCHK(check_dev(dV, "drhoVdt"));
+    PCHK(check_dev(dW, "drhoWdt"));
+    PCU(cudaSetDevice(p->device));
+    const Pad P = pad_of(p->g);
+    MomM M;
+    for (int a = 0; a < 3; a++) {
+        M.di[a] = p->mdi[a];
+        M.dmi[a] = p->mdmi[a];
+        M.itm[a] = p->mitm[a];
+        M.itz[a] = p->mitz[a];
+    }
+    const long long n = (long long)P.nx * P.ny * P.nz;
+    k_dmomdt<<<grid_cells(n), kThreads, 0, p->stream>>>(P, M, U, V, W, P_, rho, visc, visc0, dU, dV, dW);
+    PCU(cudaGetLastError());
+    return sync_arrays(p, dU, dV, dW, nullptr);
+}
+
+namespace {
+MomM momentum_of(const nga_proj *p) {
+    MomM M;
+    for (int a = 0; a < 3; a++) {
+        M.di[a] = p->mdi[a];
+        M.dmi[a] = p->mdmi[a];
+        M.itm[a] = p->mitm[a];
+        M.itz[a] = p->mitz[a];
+    }
+    return M;
+}
+long long padded_size(const bbmg_grid &g) {
+    return (g.nx + 2LL * g.ghost) * (g.ny + 2LL * g.ghost) * (g.nz + 2LL * g.ghost);
+}
+}  // namespace
+
+extern "C" int nga_proj_midpoint(nga_proj *p, double *U, double *V, double *W, const double *Uold,
+                                 const double *Vold, const double *Wold) {
+    if (!p) return pfail(BBMG_BAD_ARGS, "null projection handle");
+    PCHK(check_dev(U, "U"));
+    PCHK(check_dev(V, "V"));
+    PCHK(check_dev(W, "W"));
+    PCHK(check_dev(Uold, "Uold"));
+    PCHK(check_dev(Vold, "Vold"));
+    PCHK(check_dev(Wold, "Wold"));
+    PCU(cudaSetDevice(p->device));
+    const long long n = padded_size(p->g);
+    k_midpoint<<<grid_cells(n), kThreads, 0, p->stream>>>(n, Vel3{{U, V, W}}, CVel3{{Uold, Vold, Wold}});
+    PCU(cudaGetLastError());
+    return BBMG_OK;
+}
+
+extern "C" int nga_proj_advance(nga_proj *p, double dt, double rho, double *U, double *V, double *W,
+                                const double *Uold, const double *Vold, const double *Wold, const double *drhoUdt,
+                                const double *drhoVdt, const double *drhoWdt, double force_a, double force_b,
+                                const double *mean) {
+    if (!p) return pfail(BBMG_BAD_ARGS, "null projection handle");
+    PCHK(check_dev(U, "U"));
+    PCHK(check_dev(V, "V"));
+    PCHK(check_dev(W, "W"));
+    PCHK(check_dev(Uold, "Uold"));
+    PCHK(check_dev(Vold, "Vold"));
+    PCHK(check_dev(Wold, "Wold"));
+    PCHK(check_dev(drhoUdt, "drhoUdt"));
+    PCHK(check_dev(drhoVdt, "drhoVdt"));
+    PCHK(check_dev(drhoWdt, "drhoWdt"));
+    if (!(rho != 0.0)) return pfail(BBMG_BAD_ARGS, "rho must be non-zero");
+    if (force_a != 0.0 && (!mean || !(force_b != 0.0)))
+        return pfail(BBMG_BAD_ARGS, "forcing needs the mean velocity and a non-zero force_b");
+    PCU(cudaSetDevice(p->device));
+    const long long n = padded_size(p->g);
+    const double m0 = force_a != 0.0 ? mean[0] : 0.0, m1 = force_a != 0.0 ? mean[1] : 0.0,
+                 m2 = force_a != 0.0 ? mean[2] : 0.0;
+    k_advance<<<grid_cells(n), kThreads, 0, p->stream>>>(n, dt, rho, Vel3{{U, V, W}}, CVel3{{Uold, Vold, Wold}},
+                                                         CVel3{{drhoUdt, drhoVdt, drhoWdt}}, force_a, force_b, m0, m1,
+                                                         m2);
+    PCU(cudaGetLastError());
+    return BBMG_OK;
+}
+
+extern "C" int nga_proj_flow_stats(nga_proj *p, const double *U, const double *V, const double *W,
+                                   const double *visc, double visc0, double rho, double dt, double *out) {
+    if (!p) return pfail(BBMG_BAD_ARGS, "null projection handle");
+    if (!(p->g.xper && p->g.yper && p->g.zper))
+        return pfail(BBMG_BAD_ARGS, "nga_proj_flow_stats needs a triply periodic grid");
+    if (!out) return pfail(BBMG_BAD_ARGS, "out is NULL");
+    PCHK(check_dev(U, "U"));
+    PCHK(check_dev(V, "V"));
+    PCHK(check_dev(W, "W"));
+    PCHK(check_opt(visc, "visc"));
+    if (!(rho != 0.0)) return pfail(BBMG_BAD_ARGS, "rho must be non-zero");
+    PCU(cudaSetDevice(p->device));
+    const Pad P = pad_of(p->g);
+    k_stats<<<kRedBlocks, kThreads, 0, p->stream>>>(P, metrics_of(p), momentum_of(p), U, V, W, visc, visc0, rho,
+                                                    p->part);
+    PCU(cudaGetLastError());
+    k_stats_final<<<1, kStat * 32, 0, p->stream>>>(p->part, dt, p->vol_total);
+    PCU(cudaGetLastError());
+    PCU(cudaMemcpyAsync(out, p->part + kStat * kRedBlocks, kStat * sizeof(double), cudaMemcpyDefault, p->stream));
+    PCU(cudaStreamSynchronize(p->stream));
+    return BBMG_OK;
 }

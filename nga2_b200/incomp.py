@@ -1,0 +1,210 @@
+"""Constant-density incompressible flow on the GPU, triply periodic pgrids.
+
+The device counterpart of NGA2's ``incomp`` solver
+(src/constant_density/incomp_class.f90) for the calls that the homogeneous
+isotropic turbulence example makes in its time loop
+(examples/hit/src/simulation.f90:256-352), with the pressure Poisson equation
+solved by this package's bbmg (pcg_bbox) in place of the example's FFT
+solver.  Every field operation runs as a kernel of the projection library
+(include/nga_projection.h):
+
+* ``get_dmomdt``                           -> nga_proj_dmomdt
+* ``U = 0.5*(U + Uold)``                   -> nga_proj_midpoint
+* residual, linear forcing, ``U = 2U - Uold + res/rho`` -> nga_proj_advance
+* ``get_cfl``, interp_vel's kinetic energy, ``cfg%integrate`` means
+                                           -> nga_proj_flow_stats
+* ``get_div`` and ``rhs = -vol*div*rho/dt`` -> nga_proj_divergence
+* ``shift_p``                              -> nga_proj_shift_p
+* ``get_pgrad``, ``P += sol``, ``U -= dt*grad/rho`` -> nga_proj_correct
+
+Fields are CUDA float64 tensors in NGA2's padded layout [k, j, i] with
+``ghost`` overlap layers holding the periodic images.  There is no CPU path.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import bbmg as B
+from .problems import STC7
+from .projection import Projection
+
+ALPHA = 0.7  # timetracker_class.f90:12, damping of dt increases
+
+
+class TimeTracker:
+    """NGA2's timetracker (src/libraries/timetracker_class.f90): dt from the
+    CFL (``adjust_dt``, lines 88-97), time and step counters (``increment``,
+    lines 68-84) and the sub-iteration counter."""
+
+    def __init__(self, dtmax, cflmax, itmax=2, tmax=float("inf"), nmax=2 ** 62):
+        self.dtmax, self.cflmax, self.itmax = float(dtmax), float(cflmax), int(itmax)
+        self.tmax, self.nmax = tmax, nmax
+        self.dt = self.dtmax
+        self.dtold = self.dt
+        self.cfl = 0.0
+        self.t = 0.0
+        self.n = 0
+        self.it = 1
+
+    def adjust_dt(self):
+        self.dtold = self.dt
+        if self.cfl > 0.0:
+            self.dt = min(self.dtold * self.cflmax / self.cfl, self.dtmax)
+        if self.dt > self.dtold:
+            self.dt = ALPHA * self.dt + (1.0 - ALPHA) * self.dtold
+
+    def increment(self):
+        self.it = 1
+        self.t = self.t + self.dt
+        self.n += 1
+
+    def done(self):
+        return self.n >= self.nmax or self.t >= self.tmax
+
+
+class Incomp:
+    """The incompressible solver's state and operations on one triply
+    periodic pgrid (node coordinates xn, yn, zn): U, V, W, P, Uold, Vold,
+    Wold, the cell-centred viscosity, the constant density, and the pressure
+    solver ``psolv`` set up once on ``-vol div(grad)`` (update_laplacian
+    with rho = 1, incomp_class.f90:766-785)."""
+
+    def __init__(self, xn, yn, zn, rho=1.0, visc=0.0, ghost=1, precision=B.FP64, rcvg=1e-10, maxit=100,
+                 device=0):
+        import torch
+        self.torch = torch
+        self.proj = Projection(xn, yn, zn, True, True, True, ghost=ghost, device=device)
+        g = self.proj.grid
+        self.nx, self.ny, self.nz, self.g = g.nx, g.ny, g.nz, ghost
+        self.shape = self.proj.shape
+        z = lambda: torch.zeros(self.shape, dtype=torch.float64, device="cuda")
+        self.U, self.V, self.W, self.P = z(), z(), z(), z()
+        self.Uold, self.Vold, self.Wold = z(), z(), z()
+        self.resU, self.resV, self.resW = z(), z(), z()
+        self.div, self.rhs, self.sol = z(), z(), z()
+        self.rho = float(rho)
+        self.visc = torch.full(self.shape, float(visc), dtype=torch.float64, device="cuda")
+        self.rho_face = torch.full(self.shape, self.rho, dtype=torch.float64, device="cuda")
+        self.opr = self.proj.update_laplacian()
+        self.psolv = B.BBMG(self.nx, self.ny, self.nz, True, True, True, ghost=ghost, method=B.PCG_BBOX,
+                            precision=precision, rcvg=rcvg, maxit=maxit, device=device)
+        self.psolv.setup(STC7, self.opr)
+        self.psolv_it, self.psolv_rerr = 0, 0.0
+        self.solve_ms = 0.0  # device time of the pressure solves, accumulated
+
+    # ------------------------------------------------------------ operations
+    def sync(self, a):
+        """cfg%sync: the overlap of a padded field takes the periodic images."""
+        torch = self.torch
+        g = self.g
+        if g == 0:
+            return a
+        i = a[g:-g, g:-g, g:-g]
+        a.copy_(torch.nn.functional.pad(i[None], (g, g, g, g, g, g), mode="circular")[0])
+        return a
+
+    def get_dmomdt(self):
+        return self.proj.get_dmomdt(self.U, self.V, self.W, self.P, rho=self.rho, visc=self.visc,
+                                    out=(self.resU, self.resV, self.resW))
+
+    def get_div(self, dt=None):
+        """div of the velocity; with dt also the pressure right-hand side
+        rhs = -vol*div*rho/dt."""
+        self.proj.get_div(self.U, self.V, self.W, rho=self.rho, dt=dt, div=self.div,
+                          rhs=self.rhs if dt is not None else None)
+        return self.div
+
+    def stats(self, dt=1.0):
+        return self.proj.flow_stats(self.U, self.V, self.W, visc=self.visc, rho=self.rho, dt=dt)
+
+    def get_cfl(self, dt):
+        """(cflc, cfl): the largest convective CFL and the largest overall."""
+        s = self.stats(dt)
+        cflc = max(s["cflc_x"], s["cflc_y"], s["cflc_z"])
+        return cflc, max(cflc, s["cflv_x"], s["cflv_y"], s["cflv_z"])
+
+    def pressure_projection(self, dt):
+        """get_div, rhs = -vol*div*rho/dt, sol = 0, psolv%solve, shift_p,
+        get_pgrad, P += sol, U -= dt*grad(sol)/rho (simulation.f90:332-343)."""
+        self.get_div(dt)
+        self.sol.zero_()
+        _, it, rerr, st = self.psolv.solve(self.rhs, self.sol)
+        self.psolv_it, self.psolv_rerr = it, rerr
+        self.solve_ms += self.psolv.info["solve_ms"]
+        self.proj.shift_p(self.sol)
+        self.proj.correct(self.sol, dt, self.U, self.V, self.W, self.P, self.rho_face, self.rho_face, self.rho_face)
+        return it, rerr, st
+
+    def close(self):
+        self.psolv.close()
+        self.proj.close()
+
+
+class HIT:
+    """The forced homogeneous isotropic turbulence example
+    (examples/hit/src/simulation.f90) on the GPU: a (Lx)^3 triply periodic
+    box of n^3 cells, Gaussian initial velocity of rms ``urms0`` projected to
+    be divergence-free (lines 100-135), then the time loop (lines 256-352):
+    dt from the CFL, ``itmax`` sub-iterations of a mid-point (Crank-Nicolson
+    like) explicit update with linear forcing towards the initial kinetic
+    energy, each closed by a pressure projection.  Defaults are the
+    example's input file (examples/hit/input) without particles."""
+
+    def __init__(self, n=64, Lx=1.0, visc=0.01, rho=1.0, urms0=5.0, tau_eddy=0.1, dtmax=1e-3, cflmax=0.9,
+                 itmax=2, seed=0, ghost=1, precision=B.FP64, rcvg=1e-10, maxit=100, forcing=True, device=0):
+        import torch
+        self.torch = torch
+        x = np.arange(n + 1, dtype=np.float64) / float(n) * Lx
+        self.fs = Incomp(x, x, x, rho=rho, visc=visc, ghost=ghost, precision=precision, rcvg=rcvg, maxit=maxit,
+                         device=device)
+        self.time = TimeTracker(dtmax, cflmax, itmax)
+        self.tau_eddy, self.forcing = float(tau_eddy), bool(forcing)
+        self.records = []
+        fs, g = self.fs, ghost
+        rng = np.random.default_rng(seed)
+        for a in (fs.U, fs.V, fs.W):  # random_normal(m=0, sd=Urms0) on the interior, then sync
+            a[g:g + n, g:g + n, g:g + n] = torch.from_numpy(rng.normal(0.0, urms0, size=(n, n, n))).cuda()
+            fs.sync(a)
+        fs.pressure_projection(self.time.dt)
+        self.KE0 = fs.stats()["KE"]
+        self.KE = self.KE0
+
+    def step(self, keep=False):
+        """One time step; returns the number of PCG iterations of each
+        sub-iteration's pressure solve.  With keep, each solve's (rhs,
+        previous solution, solution) is appended to ``records``."""
+        fs, time = self.fs, self.time
+        _, time.cfl = fs.get_cfl(time.dt)
+        time.adjust_dt()
+        time.increment()
+        for a, b in ((fs.Uold, fs.U), (fs.Vold, fs.V), (fs.Wold, fs.W)):
+            a.copy_(b)
+        its = []
+        while time.it <= time.itmax:
+            fs.proj.midpoint(fs.U, fs.V, fs.W, fs.Uold, fs.Vold, fs.Wold)
+            fs.get_dmomdt()
+            fa, mean = 0.0, None
+            if self.forcing:
+                s = fs.stats()
+                self.KE = s["KE"]
+                fa, mean = time.dt * self.KE0 / self.KE, (s["meanU"], s["meanV"], s["meanW"])
+            fs.proj.advance(time.dt, fs.rho, fs.U, fs.V, fs.W, fs.Uold, fs.Vold, fs.Wold, fs.resU, fs.resV, fs.resW,
+                            force_a=fa, force_b=2.0 * self.tau_eddy, mean=mean)
+            prev = fs.sol.clone() if keep else None
+            it, rerr, st = fs.pressure_projection(time.dt)
+            its.append(it)
+            if keep:
+                self.records.append(self._record(prev))
+            time.it += 1
+        fs.get_div()
+        return its
+
+    def _record(self, prev):
+        fs, g = self.fs, self.fs.g
+        n = fs.nx
+        inner = lambda a: a[g:g + n, g:g + n, g:g + n].contiguous()
+        return {"rhs": inner(fs.rhs), "p_prev": inner(prev), "dp": inner(fs.sol), "dt": self.time.dt,
+                "step": self.time.n, "it": fs.psolv_it}
+
+    def close(self):
+        self.fs.close()

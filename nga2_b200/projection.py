@@ -13,7 +13,8 @@ import ctypes as C
 from . import bbmg as B
 
 EXPORTS = ["nga_proj_create", "nga_proj_destroy", "nga_proj_set_stream", "nga_proj_laplacian",
-           "nga_proj_divergence", "nga_proj_shift_p", "nga_proj_pgrad", "nga_proj_correct"]
+           "nga_proj_divergence", "nga_proj_shift_p", "nga_proj_pgrad", "nga_proj_correct", "nga_proj_dmomdt",
+           "nga_proj_midpoint", "nga_proj_advance", "nga_proj_flow_stats"]
 
 _BOUND = False
 
@@ -32,6 +33,10 @@ def lib():
         L.nga_proj_shift_p.argtypes = [P, P, DP]
         L.nga_proj_pgrad.argtypes = [P, P, P, P, P]
         L.nga_proj_correct.argtypes = [P, P, D, P, P, P, P, P, P, P]
+        L.nga_proj_dmomdt.argtypes = [P, P, P, P, P, D, P, D, P, P, P]
+        L.nga_proj_midpoint.argtypes = [P, P, P, P, P, P, P]
+        L.nga_proj_advance.argtypes = [P, D, D, P, P, P, P, P, P, P, P, P, D, D, DP]
+        L.nga_proj_flow_stats.argtypes = [P, P, P, P, P, D, D, D, DP]
         for n in EXPORTS:
             getattr(L, n).restype = C.c_int
         _BOUND = True
@@ -101,6 +106,34 @@ class Projection:
     def correct(self, sol, dt, U, V, W, P=None, rho_U=None, rho_V=None, rho_W=None):
         self._check(self.lib.nga_proj_correct(self.h, _p(sol), float(dt), _p(rho_U), _p(rho_V), _p(rho_W),
                                               _p(P), _p(U), _p(V), _p(W)))
+
+    def get_dmomdt(self, U, V, W, P, rho=1.0, visc=None, visc0=0.0, out=None):
+        """Time derivatives of rho U, rho V, rho W (incomp's get_dmomdt) on a
+        triply periodic grid; visc is a cell-centred array or None for visc0."""
+        dU, dV, dW = out if out is not None else (self._new(), self._new(), self._new())
+        self._check(self.lib.nga_proj_dmomdt(self.h, _p(U), _p(V), _p(W), _p(P), float(rho), _p(visc), float(visc0),
+                                             _p(dU), _p(dV), _p(dW)))
+        return dU, dV, dW
+
+    def midpoint(self, U, V, W, Uold, Vold, Wold):
+        """U = 0.5*(U + Uold), V and W likewise, in place."""
+        self._check(self.lib.nga_proj_midpoint(self.h, _p(U), _p(V), _p(W), _p(Uold), _p(Vold), _p(Wold)))
+
+    def advance(self, dt, rho, U, V, W, Uold, Vold, Wold, dU, dV, dW, force_a=0.0, force_b=1.0, mean=None):
+        """The explicit update of a sub-iteration, in place on U, V, W:
+        U = 2U - Uold + (-2(rho U - rho Uold) + dt dU [+ (force_a (U - mean))/force_b])/rho."""
+        m = (C.c_double * 3)(*(mean if mean is not None else (0.0, 0.0, 0.0)))
+        self._check(self.lib.nga_proj_advance(self.h, float(dt), float(rho), _p(U), _p(V), _p(W), _p(Uold), _p(Vold),
+                                              _p(Wold), _p(dU), _p(dV), _p(dW), float(force_a), float(force_b), m))
+
+    def flow_stats(self, U, V, W, visc=None, visc0=0.0, rho=1.0, dt=1.0):
+        """dict of get_cfl's CFLs (cflc_x/y/z, cflv_x/y/z), the kinetic energy KE
+        of the cell-interpolated velocity and the mean velocities meanU/V/W."""
+        out = (C.c_double * 10)()
+        self._check(self.lib.nga_proj_flow_stats(self.h, _p(U), _p(V), _p(W), _p(visc), float(visc0), float(rho),
+                                                 float(dt), out))
+        keys = ("cflc_x", "cflc_y", "cflc_z", "cflv_x", "cflv_y", "cflv_z", "KE", "meanU", "meanV", "meanW")
+        return dict(zip(keys, list(out)))
 
     def close(self):
         if self.h:

@@ -18,6 +18,11 @@ A numpy restatement, term for term, of:
   fluid_vol = xL*yL*zL (sgrid_class.f90:260-263);
 * get_pgrad (incomp_class.f90:1163-1184);
 * the velocity correction of examples/falling_drop/src/simulation.f90:308-313;
+* get_dmomdt (incomp_class.f90:1021-1159) on triply periodic grids, with the
+  metrics extended over two layers;
+* the whole-array updates of a sub-iteration of examples/hit/src/simulation.f90
+  (mid-time velocity, explicit residual with the linear forcing) and the flow
+  statistics the loop needs (get_cfl, the kinetic energy, mean velocities);
 * cfg%sync on one rank: periodic images in the overlap.
 
 Arrays are padded numpy arrays [k, j, i] with ``g`` overlap layers; the
@@ -177,3 +182,287 @@ def correct(G, sol, dt, U, V, W, P=None, rho_U=None, rho_V=None, rho_W=None):
         G.interior(q)[...] = G.interior(P) + G.interior(sol)
         out.append(G.sync(q))
     return out
+
+
+# ----------------------------------------------------------------------------- momentum
+def momentum_metrics(x):
+    """Extended 1-D metrics of one periodic direction for get_dmomdt: cell
+    sizes' inverses dxi on cells -1..n (index c+1), centroid spacings' inverses
+    dxmi and the edge interpolation weights itp(-1), itp(0) on faces 0..n
+    (incomp_class.f90:250-446, sgrid_class.f90:160-254 with two layers of the
+    naive extension)."""
+    x = np.asarray(x, np.float64)
+    n = x.size - 1
+    xe = np.empty(n + 5)              # nodes -2 .. n+2 at index +2
+    xe[2:n + 3] = x
+    for m in (1, 0):                  # x(i) = x(i+1) - (x(imin+1) - x(imin))
+        xe[m] = xe[m + 1] - (xe[3] - xe[2])
+    for m in (n + 3, n + 4):          # x(i) = x(i-1) + (x(imax+1) - x(imax))
+        xe[m] = xe[m - 1] + (xe[n + 2] - xe[n + 1])
+    xm = 0.5 * (xe[:-1] + xe[1:])     # cells -2 .. n+1 at index +2
+    dx = xe[1:] - xe[:-1]
+    dxi = (1.0 / dx)[1:n + 3]         # cells -1 .. n
+    f = np.arange(0, n + 1)           # faces 0 .. n
+    dxmi = 1.0 / (xm[f + 2] - xm[f + 1])
+    itm = dxmi * (xm[f + 2] - xe[f + 2])   # weight of the value at index f-1
+    itz = dxmi * (xe[f + 2] - xm[f + 1])   # weight of the value at index f
+    return dxi, dxmi, itm, itz
+
+
+def dmomdt(G, U, V, W, P, rho, visc):
+    """get_dmomdt (incomp_class.f90:1021-1159) on a triply periodic grid: the
+    time derivatives of rho U, rho V, rho W on the interior faces, term for
+    term (constant density rho, cell-centred viscosity array visc).  Ghost
+    layers of U, V, W, P and visc must hold the periodic images."""
+    assert all(G.per), "periodic directions only"
+    mx, my, mz = (momentum_metrics(a) for a in (G.xn, G.yn, G.zn))
+    nx, ny, nz = G.nx, G.ny, G.nz
+    c23 = 2.0 / 3.0
+
+    def A(a, dx=0, dy=0, dz=0):
+        return G.interior(a, di=dx, dj=dy, dk=dz)
+
+    def cx(m, off):   # cell metric at interior index + off, broadcast along x
+        return m[0][1 + off:1 + off + nx][None, None, :]
+
+    def cy(m, off):
+        return m[0][1 + off:1 + off + ny][None, :, None]
+
+    def cz(m, off):
+        return m[0][1 + off:1 + off + nz][:, None, None]
+
+    def fx(m, q, off):  # face metric q (1 dxmi, 2 itm, 3 itz) at face i + off
+        return m[q][off:off + nx][None, None, :]
+
+    def fy(m, q, off):
+        return m[q][off:off + ny][None, :, None]
+
+    def fz(m, q, off):
+        return m[q][off:off + nz][:, None, None]
+
+    def two(a0, b0, a1, b1):  # sum(a(:)*b(:)) of two terms
+        return a0 * b0 + a1 * b1
+
+    # divergence at a cell, the divp sums of the normal fluxes
+    def divc(ox, oy, oz):
+        dxi, dyi, dzi = cx(mx, ox), cy(my, oy), cz(mz, oz)
+        sx = two(dxi * -1.0, A(U, ox, oy, oz), dxi * 1.0, A(U, ox + 1, oy, oz))
+        sy = two(dyi * -1.0, A(V, ox, oy, oz), dyi * 1.0, A(V, ox, oy + 1, oz))
+        sz = two(dzi * -1.0, A(W, ox, oy, oz), dzi * 1.0, A(W, ox, oy, oz + 1))
+        return (sx + sy) + sz
+
+    def normal(Q, d, off):  # FX of rhoU (d=0), FY of rhoV (1), FZ of rhoW (2) at cell + off along d
+        o = [0, 0, 0]
+        o[d] = off
+        m = (mx, my, mz)[d]
+        ci = (cx, cy, cz)[d](m, off)
+        sh = [0, 0, 0]
+        sh[d] = 1
+        q0, q1 = A(Q, *o), A(Q, o[0] + sh[0], o[1] + sh[1], o[2] + sh[2])
+        s1 = two(0.5, q0, 0.5, q1)
+        g = two(ci * -1.0, q0, ci * 1.0, q1)
+        return ((-(rho * s1 * s1)) + A(visc, *o) * ((g + g) - c23 * divc(*o))) - A(P, *o)
+
+    def edge(d1, d2, o1, o2, Qa, Qb):
+        """Edge flux in the (d1, d2) plane at face offsets o1 (along d1), o2 (along d2):
+        -rho (itp_{d1} Qa) (itp_{d2} Qb) + (itp_2d visc) (grd_{d1} Qa + grd_{d2} Qb), where Qa
+        varies along d1 and Qb along d2; the 2-D viscosity sum runs over (s1 along d1,
+        s2 along d2) in Fortran order (first index fastest) of the reference's itp_xy/yz/xz."""
+        o = [0, 0, 0]
+        o[d1] += o1
+        o[d2] += o2
+        m1, m2 = (mx, my, mz)[d1], (mx, my, mz)[d2]
+        f1, f2 = (fx, fy, fz)[d1], (fx, fy, fz)[d2]
+        e1 = [0, 0, 0]
+        e1[d1] = -1
+        e2 = [0, 0, 0]
+        e2[d2] = -1
+        qa_m = A(Qa, o[0] + e1[0], o[1] + e1[1], o[2] + e1[2])
+        qa_0 = A(Qa, *o)
+        qb_m = A(Qb, o[0] + e2[0], o[1] + e2[1], o[2] + e2[2])
+        qb_0 = A(Qb, *o)
+        a = two(f1(m1, 2, o1), qa_m, f1(m1, 3, o1), qa_0)
+        b = two(f2(m2, 2, o2), qb_m, f2(m2, 3, o2), qb_0)
+        return a, b, qa_m, qa_0, qb_m, qb_0, o, (m1, f1, o1), (m2, f2, o2)
+
+    def visc2(dlo, dhi, o, wlo, whi):
+        # sum over (st_lo, st_hi) in {-1,0}^2, st_lo fastest: itp_lo(st_lo) itp_hi(st_hi) visc(..)
+        (mlo, flo, olo), (mhi, fhi, ohi) = wlo, whi
+        itl = {-1: flo(mlo, 2, olo), 0: flo(mlo, 3, olo)}
+        ith = {-1: fhi(mhi, 2, ohi), 0: fhi(mhi, 3, ohi)}
+        s = None
+        for sh in (-1, 0):
+            for sl in (-1, 0):
+                p = list(o)
+                p[dlo] += sl
+                p[dhi] += sh
+                t = (itl[sl] * ith[sh]) * A(visc, *p)
+                s = t if s is None else s + t
+        return s
+
+    def grd(m, f, off, q_m, q_0):
+        dmi = f(m, 1, off)
+        return two(dmi * -1.0, q_m, dmi * 1.0, q_0)
+
+    # ---- rho U: FX at cells i-1, i; FY at xy edges (i, j), (i, j+1); FZ at xz edges (i, k), (i, k+1)
+    FX = [normal(U, 0, -1), normal(U, 0, 0)]
+    FY, FZ = [], []
+    for oy in (0, 1):
+        a, b, qa_m, qa_0, qb_m, qb_0, o, w1, w2 = edge(1, 0, oy, 0, U, V)   # a: itpu_y U, b: itpv_x V
+        vi = visc2(0, 1, o, w2, w1)                                           # itp_xy(x fastest, y)
+        g = grd(*w1[:2], w1[2], qa_m, qa_0) + grd(*w2[:2], w2[2], qb_m, qb_0)
+        FY.append((-(rho * a * b)) + vi * g)
+    for oz in (0, 1):
+        a, b, qa_m, qa_0, qb_m, qb_0, o, w1, w2 = edge(2, 0, oz, 0, U, W)   # a: itpu_z U, b: itpw_x W
+        vi = visc2(0, 2, o, w2, w1)                                           # itp_xz(x fastest, z)
+        g = grd(*w1[:2], w1[2], qa_m, qa_0) + grd(*w2[:2], w2[2], qb_m, qb_0)
+        FZ.append((-(rho * a * b)) + vi * g)
+    dmx = fx(mx, 1, 0)
+    dU = (two(dmx * -1.0, FX[0], dmx * 1.0, FX[1]) + two(cy(my, 0) * -1.0, FY[0], cy(my, 0) * 1.0, FY[1])) \
+        + two(cz(mz, 0) * -1.0, FZ[0], cz(mz, 0) * 1.0, FZ[1])
+
+    # ---- rho V: FX at xy edges (i, j), (i+1, j); FY at cells j-1, j; FZ at yz edges (j, k), (j, k+1)
+    FX, FZ = [], []
+    for ox in (0, 1):
+        a, b, qa_m, qa_0, qb_m, qb_0, o, w1, w2 = edge(0, 1, ox, 0, V, U)   # a: itpv_x V, b: itpu_y U
+        vi = visc2(0, 1, o, w1, w2)
+        g = grd(*w1[:2], w1[2], qa_m, qa_0) + grd(*w2[:2], w2[2], qb_m, qb_0)
+        FX.append((-(rho * a * b)) + vi * g)
+    FY = [normal(V, 1, -1), normal(V, 1, 0)]
+    for oz in (0, 1):
+        a, b, qa_m, qa_0, qb_m, qb_0, o, w1, w2 = edge(2, 1, oz, 0, V, W)   # a: itpv_z V, b: itpw_y W
+        vi = visc2(1, 2, o, w2, w1)                                           # itp_yz(y fastest, z)
+        g = grd(*w1[:2], w1[2], qa_m, qa_0) + grd(*w2[:2], w2[2], qb_m, qb_0)
+        FZ.append((-(rho * a * b)) + vi * g)
+    dmy = fy(my, 1, 0)
+    dV = (two(cx(mx, 0) * -1.0, FX[0], cx(mx, 0) * 1.0, FX[1]) + two(dmy * -1.0, FY[0], dmy * 1.0, FY[1])) \
+        + two(cz(mz, 0) * -1.0, FZ[0], cz(mz, 0) * 1.0, FZ[1])
+
+    # ---- rho W: FX at xz edges (i, k), (i+1, k); FY at yz edges (j, k), (j+1, k); FZ at cells k-1, k
+    FX, FY = [], []
+    for ox in (0, 1):
+        a, b, qa_m, qa_0, qb_m, qb_0, o, w1, w2 = edge(0, 2, ox, 0, W, U)   # a: itpw_x W, b: itpu_z U
+        vi = visc2(0, 2, o, w1, w2)
+        g = grd(*w1[:2], w1[2], qa_m, qa_0) + grd(*w2[:2], w2[2], qb_m, qb_0)
+        FX.append((-(rho * a * b)) + vi * g)
+    for oy in (0, 1):
+        a, b, qa_m, qa_0, qb_m, qb_0, o, w1, w2 = edge(1, 2, oy, 0, W, V)   # a: itpw_y W, b: itpv_z V
+        vi = visc2(1, 2, o, w1, w2)
+        g = grd(*w1[:2], w1[2], qa_m, qa_0) + grd(*w2[:2], w2[2], qb_m, qb_0)
+        FY.append((-(rho * a * b)) + vi * g)
+    FZ = [normal(W, 2, -1), normal(W, 2, 0)]
+    dmz = fz(mz, 1, 0)
+    dW = (two(cx(mx, 0) * -1.0, FX[0], cx(mx, 0) * 1.0, FX[1]) + two(cy(my, 0) * -1.0, FY[0], cy(my, 0) * 1.0, FY[1])) \
+        + two(dmz * -1.0, FZ[0], dmz * 1.0, FZ[1])
+    out = []
+    for d in (dU, dV, dW):
+        a = np.zeros(G.padded)
+        G.interior(a)[...] = d
+        out.append(G.sync(a))
+    return out
+
+
+def midpoint(U, Uold):
+    """fs%U=0.5_WP*(fs%U+fs%Uold) (examples/hit/src/simulation.f90:283-285),
+    whole padded arrays."""
+    return 0.5 * (U + Uold)
+
+
+def advance(dt, rho, U, Uold, dU, force_a=0.0, force_b=1.0, mean=0.0):
+    """The explicit update of a sub-iteration (examples/hit/src/simulation.f90:
+    291-325) for one component over the whole padded array: resU =
+    -2*(rho*U - rho*Uold) + dt*resU, plus the linear forcing
+    (force_a*(U - mean))/force_b when force_a != 0, then U = 2*U - Uold + resU/rho."""
+    res = -2.0 * (rho * U - rho * Uold) + dt * dU
+    if force_a != 0.0:
+        res = res + (force_a * (U - mean)) / force_b
+    return (2.0 * U - Uold) + res / rho
+
+
+def flow_stats(G, U, V, W, visc, rho, dt):
+    """get_cfl's six CFLs (incomp_class.f90:1497-1540), the kinetic energy of
+    interp_vel's cell velocities (incomp_class.f90:1188-1225, summed as in
+    examples/hit/src/simulation.f90:299-311) and the volume means of U, V, W
+    (config_class.f90:196-214 over fluid_vol), triply periodic grids."""
+    mx, my, mz = (momentum_metrics(a) for a in (G.xn, G.yn, G.zn))
+    nx, ny, nz = G.nx, G.ny, G.nz
+    u, v, w, vis = G.interior(U), G.interior(V), G.interior(W), G.interior(visc)
+    cflc = [(np.abs(u) * mx[1][:nx][None, None, :]).max() * dt,
+            (np.abs(v) * my[1][:ny][None, :, None]).max() * dt,
+            (np.abs(w) * mz[1][:nz][:, None, None]).max() * dt]
+    dxi, dyi, dzi = mx[0][1:nx + 1], my[0][1:ny + 1], mz[0][1:nz + 1]
+    cflv = [((4.0 * vis) * (dxi * dxi)[None, None, :] / rho).max() * dt,
+            ((4.0 * vis) * (dyi * dyi)[None, :, None] / rho).max() * dt,
+            ((4.0 * vis) * (dzi * dzi)[:, None, None] / rho).max() * dt]
+    ui = 0.5 * u + 0.5 * G.interior(U, di=1)
+    vi = 0.5 * v + 0.5 * G.interior(V, dj=1)
+    wi = 0.5 * w + 0.5 * G.interior(W, dk=1)
+    ke = (0.5 * ((ui * ui + vi * vi) + wi * wi)).sum()
+    vol = G.vol
+    means = [(vol * a).sum() / G.vol_total for a in (u, v, w)]
+    return np.array(cflc + cflv + [ke] + means)
+
+
+class HITOracle:
+    """examples/hit/src/simulation.f90 on the CPU (lines 100-135 for the
+    initial field, 256-352 for the time loop; no particles), built from the
+    functions above and a pressure solve ``solve(opr, rhs) -> sol`` on
+    interior arrays (the oracle bbmg in the tests).  dt follows
+    timetracker_class.f90:88-97 (adjust_dt, alpha = 0.7) and 68-84."""
+
+    def __init__(self, n, solve, Lx=1.0, visc=0.01, rho=1.0, urms0=5.0, tau_eddy=0.1, dtmax=1e-3, cflmax=0.9,
+                 itmax=2, seed=0, g=1, forcing=True):
+        x = np.arange(n + 1, dtype=np.float64) / float(n) * Lx
+        self.G = G = Grid(x, x, x, (True, True, True), g)
+        self.solve, self.rho, self.tau, self.forcing = solve, float(rho), float(tau_eddy), forcing
+        self.visc = np.full(G.padded, float(visc))
+        self.rho_face = np.full(G.padded, self.rho)
+        self.opr = laplacian(G)
+        self.dtmax, self.cflmax, self.itmax = dtmax, cflmax, itmax
+        self.dt, self.t, self.n, self.cfl = dtmax, 0.0, 0, 0.0
+        rng = np.random.default_rng(seed)
+        self.U, self.V, self.W = (self._fill(rng.normal(0.0, urms0, size=(n, n, n))) for _ in range(3))
+        self.P = np.zeros(G.padded)
+        self.sol = np.zeros(G.padded)
+        self._project(self.dt)
+        self.KE0 = flow_stats(G, self.U, self.V, self.W, self.visc, self.rho, 1.0)[6]
+
+    def _fill(self, inner):
+        a = np.zeros(self.G.padded)
+        self.G.interior(a)[...] = inner
+        return self.G.sync(a)
+
+    def _project(self, dt):
+        G = self.G
+        _, rhs = divergence(G, self.U, self.V, self.W, rho=self.rho, dt=dt)
+        x = self.solve(np.ascontiguousarray(G.interior(self.opr)), np.ascontiguousarray(G.interior(rhs)))
+        sol = self._fill(x)
+        sol, _ = shift_p(G, sol)
+        self.sol = sol
+        self.U, self.V, self.W, self.P = correct(G, sol, dt, self.U, self.V, self.W, self.P, self.rho_face,
+                                                 self.rho_face, self.rho_face)
+
+    def step(self):
+        G = self.G
+        s = flow_stats(G, self.U, self.V, self.W, self.visc, self.rho, self.dt)
+        self.cfl = s[:6].max()
+        dtold = self.dt
+        if self.cfl > 0.0:
+            self.dt = min(dtold * self.cflmax / self.cfl, self.dtmax)
+        if self.dt > dtold:
+            self.dt = 0.7 * self.dt + (1.0 - 0.7) * dtold
+        self.t += self.dt
+        self.n += 1
+        dt = self.dt
+        Uo, Vo, Wo = self.U.copy(), self.V.copy(), self.W.copy()
+        for _ in range(self.itmax):
+            self.U, self.V, self.W = midpoint(self.U, Uo), midpoint(self.V, Vo), midpoint(self.W, Wo)
+            dU, dV, dW = dmomdt(G, self.U, self.V, self.W, self.P, self.rho, self.visc)
+            fa, mean = 0.0, (0.0, 0.0, 0.0)
+            if self.forcing:
+                st = flow_stats(G, self.U, self.V, self.W, self.visc, self.rho, 1.0)
+                fa, mean = dt * self.KE0 / st[6], st[7:10]
+            self.U = advance(dt, self.rho, self.U, Uo, dU, fa, 2.0 * self.tau, mean[0])
+            self.V = advance(dt, self.rho, self.V, Vo, dV, fa, 2.0 * self.tau, mean[1])
+            self.W = advance(dt, self.rho, self.W, Wo, dW, fa, 2.0 * self.tau, mean[2])
+            self._project(dt)
