@@ -135,6 +135,39 @@ class Incomp:
         self.proj.correct(self.sol, dt, self.U, self.V, self.W, self.P, self.rho_face, self.rho_face, self.rho_face)
         return it, rerr, st
 
+    def time_step(self, time, force=None, on_solve=None):
+        """One step of the example's time loop (simulation.f90:262-352): dt
+        from get_cfl and adjust_dt, Uold = U, then time.itmax sub-iterations
+        of midpoint, get_dmomdt, explicit update and pressure projection.
+        ``force(fs) -> (force_a, force_b, mean)`` supplies the linear forcing
+        of each sub-iteration (None: unforced); ``on_solve(fs, prev_sol)`` is
+        called after each pressure projection with the solution the solve
+        replaced.  Returns each solve's PCG iteration count."""
+        _, time.cfl = self.get_cfl(time.dt)
+        time.adjust_dt()
+        time.increment()
+        for a, b in ((self.Uold, self.U), (self.Vold, self.V), (self.Wold, self.W)):
+            a.copy_(b)
+        its = []
+        while time.it <= time.itmax:
+            self.proj.midpoint(self.U, self.V, self.W, self.Uold, self.Vold, self.Wold)
+            self.get_dmomdt()
+            fa, fb, mean = force(self) if force is not None else (0.0, 1.0, None)
+            self.proj.advance(time.dt, self.rho, self.U, self.V, self.W, self.Uold, self.Vold, self.Wold, self.resU,
+                              self.resV, self.resW, force_a=fa, force_b=fb, mean=mean)
+            prev = self.sol.clone() if on_solve is not None else None
+            it, rerr, st = self.pressure_projection(time.dt)
+            its.append(it)
+            if on_solve is not None:
+                on_solve(self, prev)
+            time.it += 1
+        self.get_div()
+        return its
+
+    def interior(self, a):
+        g = self.g
+        return a[g:g + self.nz, g:g + self.ny, g:g + self.nx]
+
     def close(self):
         self.psolv.close()
         self.proj.close()
@@ -169,40 +202,21 @@ class HIT:
         self.KE0 = fs.stats()["KE"]
         self.KE = self.KE0
 
+    def _force(self, fs):
+        s = fs.stats()
+        self.KE = s["KE"]
+        return self.time.dt * self.KE0 / self.KE, 2.0 * self.tau_eddy, (s["meanU"], s["meanV"], s["meanW"])
+
     def step(self, keep=False):
         """One time step; returns the number of PCG iterations of each
         sub-iteration's pressure solve.  With keep, each solve's (rhs,
         previous solution, solution) is appended to ``records``."""
-        fs, time = self.fs, self.time
-        _, time.cfl = fs.get_cfl(time.dt)
-        time.adjust_dt()
-        time.increment()
-        for a, b in ((fs.Uold, fs.U), (fs.Vold, fs.V), (fs.Wold, fs.W)):
-            a.copy_(b)
-        its = []
-        while time.it <= time.itmax:
-            fs.proj.midpoint(fs.U, fs.V, fs.W, fs.Uold, fs.Vold, fs.Wold)
-            fs.get_dmomdt()
-            fa, mean = 0.0, None
-            if self.forcing:
-                s = fs.stats()
-                self.KE = s["KE"]
-                fa, mean = time.dt * self.KE0 / self.KE, (s["meanU"], s["meanV"], s["meanW"])
-            fs.proj.advance(time.dt, fs.rho, fs.U, fs.V, fs.W, fs.Uold, fs.Vold, fs.Wold, fs.resU, fs.resV, fs.resW,
-                            force_a=fa, force_b=2.0 * self.tau_eddy, mean=mean)
-            prev = fs.sol.clone() if keep else None
-            it, rerr, st = fs.pressure_projection(time.dt)
-            its.append(it)
-            if keep:
-                self.records.append(self._record(prev))
-            time.it += 1
-        fs.get_div()
-        return its
+        keep_fn = (lambda fs, prev: self.records.append(self._record(prev))) if keep else None
+        return self.fs.time_step(self.time, force=self._force if self.forcing else None, on_solve=keep_fn)
 
     def _record(self, prev):
-        fs, g = self.fs, self.fs.g
-        n = fs.nx
-        inner = lambda a: a[g:g + n, g:g + n, g:g + n].contiguous()
+        fs = self.fs
+        inner = lambda a: fs.interior(a).contiguous()
         return {"rhs": inner(fs.rhs), "p_prev": inner(prev), "dp": inner(fs.sol), "dt": self.time.dt,
                 "step": self.time.n, "it": fs.psolv_it}
 
