@@ -26,7 +26,7 @@ cudaError_t setup_direct(const Lay &L, const double *opr, double *OP, double *LU
 // solve.cu
 template <typename T>
 cudaError_t launch_relax(const Lay &L, const NbrOff &nb, int npt, bool fuse, const T *opr, T *v, const T *f, int dir,
-                         cudaStream_t s);
+                         cudaStream_t s, bool skip_first = false);
 // `nsweeps` alternating sweeps starting with `first_dir` (the relax loops of
 // cycle, bbmg_class.f90:754-758 and 772-775)
 template <typename T>

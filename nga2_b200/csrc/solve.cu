@@ -1550,9 +1550,9 @@ static cudaError_t launch_colour(const Lay &L, const Off27 &off, const T *opr, T
 
 template <typename T>
 cudaError_t launch_relax(const Lay &L, const NbrOff &nb, int npt, bool fuse, const T *opr, T *v, const T *f, int dir,
-                         cudaStream_t s) {
+                         cudaStream_t s, bool skip_first) {
     const bool per = L.xper || L.yper || L.zper;
-    for (int c = 0; c < 8; c++) {
+    for (int c = skip_first ? 1 : 0; c < 8; c++) {
         int col = dir > 0 ? c : 7 - c;  // colours 1..8 forward, 8..1 backward
         int px = col & 1, py = (col >> 1) & 1, pz = (col >> 2) & 1;
         long long n = (long long)((L.nx - px + 1) >> 1) * ((L.ny - py + 1) >> 1) * ((L.nz - pz + 1) >> 1);
@@ -1616,7 +1616,11 @@ cudaError_t launch_relax_sweeps(const Lay &L, const NbrOff &nb, int npt, bool fu
     if (npt == 27 || !fuse) {
         int dir = first_dir;
         for (int i = 0; i < nsweeps; i++) {
-            cudaError_t e = launch_relax<T>(L, nb, npt, fuse, opr, v, f, dir, s);
+            // the first colour of a sweep after the opposite sweep is the colour
+            // that sweep ended with: the reference's update (rhs minus the
+            // neighbours' sum, over the centre) reads only the other colours,
+            // so recomputing it gives the same bits and is skipped
+            cudaError_t e = launch_relax<T>(L, nb, npt, fuse, opr, v, f, dir, s, i > 0);
             if (e != cudaSuccess) return e;
             dir = -dir;
         }
@@ -1916,9 +1920,14 @@ __device__ __forceinline__ void pass_sync() {
     else __syncthreads();
 }
 
+// skip: leave out the first colour (the one the opposite sweep before ended
+// with; recomputing it gives the same bits).  The loop keeps its fixed start:
+// with a runtime start ptxas gave the tail kernel half the registers (64
+// against 127) and its passes ran ~40 % slower.
 template <bool CL, typename T>
-__device__ void tail_relax(const TailLvl<T> &l, int dir, int tid, int nth) {
+__device__ void tail_relax(const TailLvl<T> &l, int dir, int tid, int nth, bool skip) {
     for (int c = 0; c < 8; c++) {
+        if (c == 0 && skip) continue;
         const int col = dir > 0 ? c : 7 - c;  // colours 1..8 forward, 8..1 backward
         const int px = col & 1, py = (col >> 1) & 1, pz = (col >> 2) & 1;
         const Lay &L = l.L;
@@ -1939,7 +1948,9 @@ __device__ void tail_relax(const TailLvl<T> &l, int dir, int tid, int nth) {
 template <bool CL, typename T>
 __device__ void tail_down(const TailArgs<T> &A, const TailLvl<T> &l, const TailLvl<T> &c, int tid, int nth) {
     int dir = 1;
-    for (int i = 0; i < A.pre; i++, dir = -dir) tail_relax<CL>(l, dir, tid, nth);
+    for (int i = 0; i < A.pre; i++, dir = -dir) {
+        tail_relax<CL>(l, dir, tid, nth, i > 0);
+    }
     const Lay &L = l.L;
     for (int it = tid; it < L.nx * L.ny * L.nz; it += nth) {
         const int i = it % L.nx, row = it / L.nx;
@@ -1964,7 +1975,9 @@ __device__ void tail_up(const TailArgs<T> &A, const TailLvl<T> &l, const TailLvl
     }
     pass_sync<CL>();
     int dir = (A.pre & 1) ? -1 : 1;
-    for (int i = 0; i < A.post; i++, dir = -dir) tail_relax<CL>(l, dir, tid, nth);
+    for (int i = 0; i < A.post; i++, dir = -dir) {
+        tail_relax<CL>(l, dir, tid, nth, i > 0);
+    }
 }
 
 // coarsest level (bbmg_class.f90:741-748): block 0 solves with the stored LU
@@ -1977,7 +1990,9 @@ __device__ void tail_coarsest(const TailArgs<T> &A, double *sm, int tid, int nth
         return;
     }
     int dir = 1;
-    for (int i = 0; i < A.pre + A.post; i++, dir = -dir) tail_relax<CL>(lc, dir, tid, nth);
+    for (int i = 0; i < A.pre + A.post; i++, dir = -dir) {
+        tail_relax<CL>(lc, dir, tid, nth, i > 0);
+    }
 }
 
 // The launch is one cluster.  Levels [0, A.split) run on every block of it;
@@ -2059,7 +2074,7 @@ template cudaError_t launch_vtail<float>(const TailArgs<float> &, int, size_t, c
 
 #define BB_INST(T)                                                                                                   \
     template cudaError_t launch_relax<T>(const Lay &, const NbrOff &, int, bool, const T *, T *, const T *, int,     \
-                                         cudaStream_t);                                                              \
+                                         cudaStream_t, bool);                                                        \
     template cudaError_t launch_relax_sweeps<T>(const Lay &, const NbrOff &, int, bool, const T *, T *, const T *,   \
                                                 int, int, cudaStream_t);                                             \
     template cudaError_t launch_residual<T>(const Lay &, const NbrOff &, int, const T *, const T *, const T *, T *,  \
