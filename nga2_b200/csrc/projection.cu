@@ -366,13 +366,23 @@ __device__ __forceinline__ double pa(double a, double b) { return __dadd_rn(a, b
 __device__ __forceinline__ double pm(double a, double b) { return __dmul_rn(a, b); }
 // sum(a(:)*b(:)) over two entries, in order
 __device__ __forceinline__ double two(double a0, double b0, double a1, double b1) { return pa(pm(a0, b0), pm(a1, b1)); }
-// sum(itp2d(:,:)*visc(..)) with the lower index (l) fastest
+// sum(itp2d(:,:)*visc(..)) with the lower index (l) fastest, where itp2d =
+// itp_l(st1)*itp_h(st2) (incomp_class.f90:277-288) divided by its own sum
+// (adjust_metrics, incomp_class.f90:505-511), summed in the same order
 __device__ __forceinline__ double visc_edge(double lm, double lz, double hm, double hz, double v_mm, double v_zm,
                                             double v_mz, double v_zz) {
-    double t = pm(pm(lm, hm), v_mm);
-    t = pa(t, pm(pm(lz, hm), v_zm));
-    t = pa(t, pm(pm(lm, hz), v_mz));
-    return pa(t, pm(pm(lz, hz), v_zz));
+    double w_mm = pm(lm, hm), w_zm = pm(lz, hm), w_mz = pm(lm, hz), w_zz = pm(lz, hz);
+    const double s = pa(pa(pa(w_mm, w_zm), w_mz), w_zz);
+    if (s > 0.0) {
+        w_mm = __ddiv_rn(w_mm, s);
+        w_zm = __ddiv_rn(w_zm, s);
+        w_mz = __ddiv_rn(w_mz, s);
+        w_zz = __ddiv_rn(w_zz, s);
+    }
+    double t = pm(w_mm, v_mm);
+    t = pa(t, pm(w_zm, v_zm));
+    t = pa(t, pm(w_mz, v_mz));
+    return pa(t, pm(w_zz, v_zz));
 }
 // -rho (itp_a Qa) (itp_b Qb) + vi (grd_a Qa + grd_b Qb)
 __device__ __forceinline__ double edge_flux(double rho, double am, double az, double qam, double qa0, double bm,

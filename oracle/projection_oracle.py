@@ -286,18 +286,24 @@ def dmomdt(G, U, V, W, P, rho, visc):
         return a, b, qa_m, qa_0, qb_m, qb_0, o, (m1, f1, o1), (m2, f2, o2)
 
     def visc2(dlo, dhi, o, wlo, whi):
-        # sum over (st_lo, st_hi) in {-1,0}^2, st_lo fastest: itp_lo(st_lo) itp_hi(st_hi) visc(..)
+        # itp_2d(st_lo, st_hi) = itp_lo(st_lo) itp_hi(st_hi) (incomp_class.f90:277-288), rescaled
+        # by its sum in adjust_metrics (incomp_class.f90:505-511); then sum(itp_2d * visc(..)),
+        # both sums over (st_lo, st_hi) in {-1,0}^2 with st_lo fastest
         (mlo, flo, olo), (mhi, fhi, ohi) = wlo, whi
         itl = {-1: flo(mlo, 2, olo), 0: flo(mlo, 3, olo)}
         ith = {-1: fhi(mhi, 2, ohi), 0: fhi(mhi, 3, ohi)}
+        order = [(sl, sh) for sh in (-1, 0) for sl in (-1, 0)]
+        w = {key: itl[key[0]] * ith[key[1]] for key in order}
+        mysum = ((w[order[0]] + w[order[1]]) + w[order[2]]) + w[order[3]]
+        assert np.all(mysum > 0.0)
+        w = {key: val / mysum for key, val in w.items()}
         s = None
-        for sh in (-1, 0):
-            for sl in (-1, 0):
-                p = list(o)
-                p[dlo] += sl
-                p[dhi] += sh
-                t = (itl[sl] * ith[sh]) * A(visc, *p)
-                s = t if s is None else s + t
+        for sl, sh in order:
+            p = list(o)
+            p[dlo] += sl
+            p[dhi] += sh
+            t = w[(sl, sh)] * A(visc, *p)
+            s = t if s is None else s + t
         return s
 
     def grd(m, f, off, q_m, q_0):
