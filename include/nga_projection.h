@@ -95,10 +95,13 @@ int nga_proj_correct(nga_proj *p, const double *sol, double dt, const double *rh
 /* get_dmomdt (incomp_class.f90:1021-1159): the time derivatives of rho U,
  * rho V, rho W on the faces from the convective, viscous and pressure fluxes
  * (constant density rho; cell-centred viscosity visc, or visc0 everywhere
- * when visc is NULL), synchronised.  Triply periodic grids only: walls need
- * the metric adjustments of adjust_metrics (incomp_class.f90:449-700), which
- * are not implemented (BBMG_BAD_ARGS).  The overlap of U, V, W, P and visc
- * must hold the periodic images. */
+ * when visc is NULL), synchronised.  A non-periodic direction has walls at
+ * both ends, as when cfg%VF = 0 outside the domain (the channel example):
+ * the edge coefficients are adjust_metrics' (incomp_class.f90:449-700) and
+ * the derivative of the wall-normal component is 0 on the wall faces; the
+ * caller keeps the velocity in the wall cells and on the wall faces (the
+ * no-slip values, 0).  The overlap of periodic directions must hold the
+ * periodic images. */
 int nga_proj_dmomdt(nga_proj *p, const double *U, const double *V, const double *W, const double *P, double rho,
                     const double *visc, double visc0, double *drhoUdt, double *drhoVdt, double *drhoWdt);
 

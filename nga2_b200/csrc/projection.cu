@@ -42,8 +42,7 @@ struct nga_proj {
     // momentum metrics per direction (two layers of the naive extension):
     // dxi on cells -1..n (index c+1), dxmi and the edge weights itm (of the
     // value at f-1) and itz (of the value at f) on faces 0..n
-    double *mdi[3] = {nullptr, nullptr, nullptr}, *mdmi[3] = {nullptr, nullptr, nullptr};
-    double *mitm[3] = {nullptr, nullptr, nullptr}, *mitz[3] = {nullptr, nullptr, nullptr};
+    const double *mom[3][9] = {};  // per direction, in momentum_metrics' order
     double *mmetrics = nullptr;
 };
 
@@ -341,25 +340,60 @@ void axis_metrics(const double *x, int n, bool per, std::vector<double> &dp0, st
 
 // Momentum metrics of one direction (incomp_class.f90:250-446 with the mesh of
 // sgrid_class.f90:160-254 extended naively by two layers).
-void momentum_metrics(const double *x, int n, std::vector<double> &di, std::vector<double> &dmi,
-                      std::vector<double> &itm, std::vector<double> &itz) {
+// Momentum metrics of one direction (q order): 0 dxi on cells -1..n (index
+// c+1); on faces 0..n: 1 dxmi, 2/3 the interpolation weights itm (value at
+// f-1) and itz (value at f); with walls at both ends of a non-periodic
+// direction (cfg%VF = 0 outside the domain, as the channel example sets it)
+// the adjust_metrics versions (incomp_class.f90:449-700): 4/5 interpolation
+// weights and 6 gradient coefficient of a velocity component tangential to
+// the direction at its faces -- [1,0], [0,1] and [-1,+1]/delta on the two
+// wall faces -- and 7/8 the 1-D factors of the edge viscosity weights with the
+// wall cell's entry zeroed.  Periodic directions: 4-8 equal 2, 3, 1, 2, 3.
+constexpr int kMomQ = 9;
+void momentum_metrics(const double *x, int n, bool walls, std::vector<double> (&m)[kMomQ]) {
     std::vector<double> xe(n + 5), xm(n + 4);  // nodes -2..n+2, cells -2..n+1 at index +2
     for (int i = 0; i <= n; i++) xe[i + 2] = x[i];
-    for (int m = 1; m >= 0; m--) xe[m] = xe[m + 1] - (xe[3] - xe[2]);
-    for (int m = n + 3; m <= n + 4; m++) xe[m] = xe[m - 1] + (xe[n + 2] - xe[n + 1]);
-    for (int m = 0; m < n + 4; m++) xm[m] = 0.5 * (xe[m] + xe[m + 1]);
-    di.assign(n + 2, 0.0);
-    for (int c = -1; c <= n; c++) di[c + 1] = 1.0 / (xe[c + 3] - xe[c + 2]);
-    dmi.assign(n + 1, 0.0); itm.assign(n + 1, 0.0); itz.assign(n + 1, 0.0);
+    for (int k = 1; k >= 0; k--) xe[k] = xe[k + 1] - (xe[3] - xe[2]);
+    for (int k = n + 3; k <= n + 4; k++) xe[k] = xe[k - 1] + (xe[n + 2] - xe[n + 1]);
+    for (int k = 0; k < n + 4; k++) xm[k] = 0.5 * (xe[k] + xe[k + 1]);
+    m[0].assign(n + 2, 0.0);
+    for (int c = -1; c <= n; c++) m[0][c + 1] = 1.0 / (xe[c + 3] - xe[c + 2]);
+    for (int q = 1; q < kMomQ; q++) m[q].assign(n + 1, 0.0);
     for (int f = 0; f <= n; f++) {
-        dmi[f] = 1.0 / (xm[f + 2] - xm[f + 1]);
-        itm[f] = dmi[f] * (xm[f + 2] - xe[f + 2]);
-        itz[f] = dmi[f] * (xe[f + 2] - xm[f + 1]);
+        const double dmi = 1.0 / (xm[f + 2] - xm[f + 1]);
+        const double itm = dmi * (xm[f + 2] - xe[f + 2]), itz = dmi * (xe[f + 2] - xm[f + 1]);
+        m[1][f] = dmi;
+        m[2][f] = m[4][f] = m[7][f] = itm;
+        m[3][f] = m[5][f] = m[8][f] = itz;
+        m[6][f] = dmi;
+    }
+    if (walls) {
+        m[4][0] = 1.0; m[5][0] = 0.0;                   // [1,0]: the wall-side value
+        m[6][0] = 1.0 / (xm[2] - xe[2]);                 // delta = xm(0) - x(0)
+        m[4][n] = 0.0; m[5][n] = 1.0;                   // [0,1]
+        m[6][n] = 1.0 / (xe[n + 2] - xm[n + 1]);         // delta = x(n) - xm(n-1)
+        m[7][0] = 0.0;                                   // cell -1 is wall
+        m[8][n] = 0.0;                                   // cell n is wall
     }
 }
 
 struct MomM {
     const double *di[3], *dmi[3], *itm[3], *itz[3];
+    const double *vtm[3], *vtz[3], *gdm[3], *wtm[3], *wtz[3];
+    int nf[3];    // faces per direction minus one (n)
+    int walls[3]; // walls at both ends (non-periodic direction)
+    // a face of the component normal to direction d lies on a wall
+    __device__ __forceinline__ bool wall_face(int d, int f) const { return walls[d] && (f == 0 || f == nf[d]); }
+    // interpolation weights and gradient coefficients (-g, +g) along d at face f
+    // of a component whose own face is a wall face (cw: both values masked,
+    // interpolation unchanged, gradient zero) or not
+    __device__ __forceinline__ void tang(int d, int f, bool cw, double &tm, double &tz, double &gm, double &gz) const {
+        if (cw) {
+            tm = itm[d][f]; tz = itz[d][f]; gm = 0.0; gz = 0.0;
+        } else {
+            tm = vtm[d][f]; tz = vtz[d][f]; gz = gdm[d][f]; gm = -gz;
+        }
+    }
 };
 
 __device__ __forceinline__ double pa(double a, double b) { return __dadd_rn(a, b); }
@@ -386,16 +420,34 @@ __device__ __forceinline__ double visc_edge(double lm, double lz, double hm, dou
 }
 // -rho (itp_a Qa) (itp_b Qb) + vi (grd_a Qa + grd_b Qb)
 __device__ __forceinline__ double edge_flux(double rho, double am, double az, double qam, double qa0, double bm,
-                                            double bz, double qbm, double qb0, double dma, double dmb, double vi) {
+                                            double bz, double qbm, double qb0, double gam, double gaz, double gbm,
+                                            double gbz, double vi) {
     const double a = two(am, qam, az, qa0), b = two(bm, qbm, bz, qb0);
-    const double g = pa(two(-dma, qam, dma, qa0), two(-dmb, qbm, dmb, qb0));
+    const double g = pa(two(gam, qam, gaz, qa0), two(gbm, qbm, gbz, qb0));
     return pa(-pm(pm(rho, a), b), pm(vi, g));
 }
 
-// get_dmomdt (incomp_class.f90:1021-1159) on a triply periodic grid, one
-// thread per cell computing the three face derivatives there; every flux is
-// recomputed by the threads that need it (the same bits each time) instead of
-// being stored.  Terms and order follow the reference expression by expression.
+// The edge flux in the plane (d1, d2) at faces f1 (along d1) and f2 (along d2)
+// for Qa = the component along d2 varying along d1 and Qb = the component along
+// d1 varying along d2 (e.g. d1 = y, d2 = x: U along y, V along x), element o
+// at the edge's upper corner; sa, sb the strides along d1 and d2; the
+// viscosity weights with the lower of the two directions first.
+__device__ __forceinline__ double edge_at(const MomM &M, double rho, int d1, int f1, int d2, int f2,
+                                          const double *__restrict__ Qa, const double *__restrict__ Qb, long long o,
+                                          long long sa, long long sb, double vi) {
+    double am, az, gam, gaz, bm, bz, gbm, gbz;
+    M.tang(d1, f1, M.wall_face(d2, f2), am, az, gam, gaz);
+    M.tang(d2, f2, M.wall_face(d1, f1), bm, bz, gbm, gbz);
+    return edge_flux(rho, am, az, Qa[o - sa], Qa[o], bm, bz, Qb[o - sb], Qb[o], gam, gaz, gbm, gbz, vi);
+}
+
+// get_dmomdt (incomp_class.f90:1021-1159), one thread per cell computing the
+// three face derivatives there; every flux is recomputed by the threads that
+// need it (the same bits each time) instead of being stored.  Terms and order
+// follow the reference expression by expression.  Non-periodic directions have
+// walls at both ends: the edge coefficients come from the adjusted metrics
+// (MomM::tang, the wall-zeroed viscosity weights) and the derivative of the
+// component normal to a wall is zero on the wall face (divu = 0 where umask > 0).
 __global__ void __launch_bounds__(kThreads) k_dmomdt(Pad P, MomM M, const double *__restrict__ U,
                                                       const double *__restrict__ V, const double *__restrict__ W,
                                                       const double *__restrict__ Pr, double rho,
@@ -435,22 +487,22 @@ __global__ void __launch_bounds__(kThreads) k_dmomdt(Pad P, MomM M, const double
             for (int oy = 0; oy < 2; oy++) {  // xy edge (x-face i, y-face j+oy)
                 const int f = j + oy;
                 const long long o = e + oy * sy;
-                const double vi = visc_edge(M.itm[0][i], M.itz[0][i], M.itm[1][f], M.itz[1][f], vs(o - sx - sy),
+                const double vi = visc_edge(M.wtm[0][i], M.wtz[0][i], M.wtm[1][f], M.wtz[1][f], vs(o - sx - sy),
                                             vs(o - sy), vs(o - sx), vs(o));
-                fy[oy] = edge_flux(rho, M.itm[1][f], M.itz[1][f], U[o - sy], U[o], M.itm[0][i], M.itz[0][i], V[o - sx],
-                                   V[o], M.dmi[1][f], M.dmi[0][i], vi);
+                fy[oy] = edge_at(M, rho, 1, f, 0, i, U, V, o, sy, sx, vi);
             }
 #pragma unroll
             for (int oz = 0; oz < 2; oz++) {  // xz edge (x-face i, z-face k+oz)
                 const int f = k + oz;
                 const long long o = e + oz * sz;
-                const double vi = visc_edge(M.itm[0][i], M.itz[0][i], M.itm[2][f], M.itz[2][f], vs(o - sx - sz),
+                const double vi = visc_edge(M.wtm[0][i], M.wtz[0][i], M.wtm[2][f], M.wtz[2][f], vs(o - sx - sz),
                                             vs(o - sz), vs(o - sx), vs(o));
-                fz[oz] = edge_flux(rho, M.itm[2][f], M.itz[2][f], U[o - sz], U[o], M.itm[0][i], M.itz[0][i], W[o - sx],
-                                   W[o], M.dmi[2][f], M.dmi[0][i], vi);
+                fz[oz] = edge_at(M, rho, 2, f, 0, i, U, W, o, sz, sx, vi);
             }
             const double dmx = M.dmi[0][i], dy = M.di[1][j + 1], dz = M.di[2][k + 1];
-            dU[e] = pa(pa(two(-dmx, fxm, dmx, fx0), two(-dy, fy[0], dy, fy[1])), two(-dz, fz[0], dz, fz[1]));
+            dU[e] = M.wall_face(0, i) ? 0.0
+                                      : pa(pa(two(-dmx, fxm, dmx, fx0), two(-dy, fy[0], dy, fy[1])),
+                                           two(-dz, fz[0], dz, fz[1]));
         }
         // ---- rho V at y-face j
         {
@@ -459,10 +511,9 @@ __global__ void __launch_bounds__(kThreads) k_dmomdt(Pad P, MomM M, const double
             for (int ox = 0; ox < 2; ox++) {  // xy edge (x-face i+ox, y-face j)
                 const int f = i + ox;
                 const long long o = e + ox * sx;
-                const double vi = visc_edge(M.itm[0][f], M.itz[0][f], M.itm[1][j], M.itz[1][j], vs(o - sx - sy),
+                const double vi = visc_edge(M.wtm[0][f], M.wtz[0][f], M.wtm[1][j], M.wtz[1][j], vs(o - sx - sy),
                                             vs(o - sy), vs(o - sx), vs(o));
-                fx[ox] = edge_flux(rho, M.itm[0][f], M.itz[0][f], V[o - sx], V[o], M.itm[1][j], M.itz[1][j], U[o - sy],
-                                   U[o], M.dmi[0][f], M.dmi[1][j], vi);
+                fx[ox] = edge_at(M, rho, 0, f, 1, j, V, U, o, sx, sy, vi);
             }
             const double fym = normal(V, sy, M.di[1][j], e - sy, i, j - 1, k);
             const double fy0 = normal(V, sy, M.di[1][j + 1], e, i, j, k);
@@ -470,13 +521,14 @@ __global__ void __launch_bounds__(kThreads) k_dmomdt(Pad P, MomM M, const double
             for (int oz = 0; oz < 2; oz++) {  // yz edge (y-face j, z-face k+oz)
                 const int f = k + oz;
                 const long long o = e + oz * sz;
-                const double vi = visc_edge(M.itm[1][j], M.itz[1][j], M.itm[2][f], M.itz[2][f], vs(o - sy - sz),
+                const double vi = visc_edge(M.wtm[1][j], M.wtz[1][j], M.wtm[2][f], M.wtz[2][f], vs(o - sy - sz),
                                             vs(o - sz), vs(o - sy), vs(o));
-                fz[oz] = edge_flux(rho, M.itm[2][f], M.itz[2][f], V[o - sz], V[o], M.itm[1][j], M.itz[1][j], W[o - sy],
-                                   W[o], M.dmi[2][f], M.dmi[1][j], vi);
+                fz[oz] = edge_at(M, rho, 2, f, 1, j, V, W, o, sz, sy, vi);
             }
             const double dx = M.di[0][i + 1], dmy = M.dmi[1][j], dz = M.di[2][k + 1];
-            dV[e] = pa(pa(two(-dx, fx[0], dx, fx[1]), two(-dmy, fym, dmy, fy0)), two(-dz, fz[0], dz, fz[1]));
+            dV[e] = M.wall_face(1, j) ? 0.0
+                                      : pa(pa(two(-dx, fx[0], dx, fx[1]), two(-dmy, fym, dmy, fy0)),
+                                           two(-dz, fz[0], dz, fz[1]));
         }
         // ---- rho W at z-face k
         {
@@ -485,24 +537,24 @@ __global__ void __launch_bounds__(kThreads) k_dmomdt(Pad P, MomM M, const double
             for (int ox = 0; ox < 2; ox++) {  // xz edge (x-face i+ox, z-face k)
                 const int f = i + ox;
                 const long long o = e + ox * sx;
-                const double vi = visc_edge(M.itm[0][f], M.itz[0][f], M.itm[2][k], M.itz[2][k], vs(o - sx - sz),
+                const double vi = visc_edge(M.wtm[0][f], M.wtz[0][f], M.wtm[2][k], M.wtz[2][k], vs(o - sx - sz),
                                             vs(o - sz), vs(o - sx), vs(o));
-                fx[ox] = edge_flux(rho, M.itm[0][f], M.itz[0][f], W[o - sx], W[o], M.itm[2][k], M.itz[2][k], U[o - sz],
-                                   U[o], M.dmi[0][f], M.dmi[2][k], vi);
+                fx[ox] = edge_at(M, rho, 0, f, 2, k, W, U, o, sx, sz, vi);
             }
 #pragma unroll
             for (int oy = 0; oy < 2; oy++) {  // yz edge (y-face j+oy, z-face k)
                 const int f = j + oy;
                 const long long o = e + oy * sy;
-                const double vi = visc_edge(M.itm[1][f], M.itz[1][f], M.itm[2][k], M.itz[2][k], vs(o - sy - sz),
+                const double vi = visc_edge(M.wtm[1][f], M.wtz[1][f], M.wtm[2][k], M.wtz[2][k], vs(o - sy - sz),
                                             vs(o - sz), vs(o - sy), vs(o));
-                fy[oy] = edge_flux(rho, M.itm[1][f], M.itz[1][f], W[o - sy], W[o], M.itm[2][k], M.itz[2][k], V[o - sz],
-                                   V[o], M.dmi[1][f], M.dmi[2][k], vi);
+                fy[oy] = edge_at(M, rho, 1, f, 2, k, W, V, o, sy, sz, vi);
             }
             const double fzm = normal(W, sz, M.di[2][k], e - sz, i, j, k - 1);
             const double fz0 = normal(W, sz, M.di[2][k + 1], e, i, j, k);
             const double dx = M.di[0][i + 1], dy = M.di[1][j + 1], dmz = M.dmi[2][k];
-            dW[e] = pa(pa(two(-dx, fx[0], dx, fx[1]), two(-dy, fy[0], dy, fy[1])), two(-dmz, fzm, dmz, fz0));
+            dW[e] = M.wall_face(2, k) ? 0.0
+                                      : pa(pa(two(-dx, fx[0], dx, fx[1]), two(-dy, fy[0], dy, fy[1])),
+                                           two(-dmz, fzm, dmz, fz0));
         }
     }
 }
@@ -675,14 +727,14 @@ extern "C" int nga_proj_create(const bbmg_grid *grid, const double *x, const dou
     }
     {
         std::vector<double> mh;
-        size_t mo[3][4];
+        size_t mo[3][kMomQ];
+        const int per[3] = {g.xper, g.yper, g.zper};
         for (int a = 0; a < 3; a++) {
-            std::vector<double> di, dmi, itm, itz;
-            momentum_metrics(xs[a], ns[a], di, dmi, itm, itz);
-            const std::vector<double> *parts[4] = {&di, &dmi, &itm, &itz};
-            for (int q = 0; q < 4; q++) {
+            std::vector<double> m[kMomQ];
+            momentum_metrics(xs[a], ns[a], !per[a], m);
+            for (int q = 0; q < kMomQ; q++) {
                 mo[a][q] = mh.size();
-                mh.insert(mh.end(), parts[q]->begin(), parts[q]->end());
+                mh.insert(mh.end(), m[q].begin(), m[q].end());
             }
         }
         cudaError_t e2 = cudaMalloc((void **)&p->mmetrics, mh.size() * sizeof(double));
@@ -693,12 +745,8 @@ extern "C" int nga_proj_create(const bbmg_grid *grid, const double *x, const dou
             return pfail(e2 == cudaErrorMemoryAllocation ? BBMG_NO_MEMORY : BBMG_CUDA, "momentum metrics: %s",
                          cudaGetErrorString(e2));
         }
-        for (int a = 0; a < 3; a++) {
-            p->mdi[a] = p->mmetrics + mo[a][0];
-            p->mdmi[a] = p->mmetrics + mo[a][1];
-            p->mitm[a] = p->mmetrics + mo[a][2];
-            p->mitz[a] = p->mmetrics + mo[a][3];
-        }
+        for (int a = 0; a < 3; a++)
+            for (int q = 0; q < kMomQ; q++) p->mom[a][q] = p->mmetrics + mo[a][q];
     }
     // fluid_vol = vol_total = xL*yL*zL (sgrid_class.f90:260-263; config_class.f90:129)
     const double xL = x[g.nx] - x[0], yL = y[g.ny] - y[0], zL = z[g.nz] - z[0];
@@ -812,12 +860,30 @@ extern "C" int nga_proj_correct(nga_proj *p, const double *sol, double dt, const
     return sync_arrays(p, U, V, W, pres);
 }
 
+namespace {
+MomM momentum_of(const nga_proj *p) {
+    MomM M;
+    const int per[3] = {p->g.xper, p->g.yper, p->g.zper}, nn[3] = {p->g.nx, p->g.ny, p->g.nz};
+    for (int a = 0; a < 3; a++) {
+        M.di[a] = p->mom[a][0];
+        M.dmi[a] = p->mom[a][1];
+        M.itm[a] = p->mom[a][2];
+        M.itz[a] = p->mom[a][3];
+        M.vtm[a] = p->mom[a][4];
+        M.vtz[a] = p->mom[a][5];
+        M.gdm[a] = p->mom[a][6];
+        M.wtm[a] = p->mom[a][7];
+        M.wtz[a] = p->mom[a][8];
+        M.nf[a] = nn[a];
+        M.walls[a] = per[a] ? 0 : 1;
+    }
+    return M;
+}
+}  // namespace
+
 extern "C" int nga_proj_dmomdt(nga_proj *p, const double *U, const double *V, const double *W, const double *P_,
                                double rho, const double *visc, double visc0, double *dU, double *dV, double *dW) {
     if (!p) return pfail(BBMG_BAD_ARGS, "null projection handle");
-    if (!(p->g.xper && p->g.yper && p->g.zper))
-        return pfail(BBMG_BAD_ARGS, "nga_proj_dmomdt needs a triply periodic grid (walls need the metric "
-                                    "adjustments of adjust_metrics, which are not implemented)");
     PCHK(check_dev(U, "U"));
     PCHK(check_dev(V, "V"));
     PCHK(check_dev(W, "W"));
@@ -828,30 +894,14 @@ extern "C" int nga_proj_dmomdt(nga_proj *p, const double *U, const double *V, co
     PCHK(check_dev(dW, "drhoWdt"));
     PCU(cudaSetDevice(p->device));
     const Pad P = pad_of(p->g);
-    MomM M;
-    for (int a = 0; a < 3; a++) {
-        M.di[a] = p->mdi[a];
-        M.dmi[a] = p->mdmi[a];
-        M.itm[a] = p->mitm[a];
-        M.itz[a] = p->mitz[a];
-    }
     const long long n = (long long)P.nx * P.ny * P.nz;
-    k_dmomdt<<<grid_cells(n), kThreads, 0, p->stream>>>(P, M, U, V, W, P_, rho, visc, visc0, dU, dV, dW);
+    k_dmomdt<<<grid_cells(n), kThreads, 0, p->stream>>>(P, momentum_of(p), U, V, W, P_, rho, visc, visc0, dU, dV,
+                                                         dW);
     PCU(cudaGetLastError());
     return sync_arrays(p, dU, dV, dW, nullptr);
 }
 
 namespace {
-MomM momentum_of(const nga_proj *p) {
-    MomM M;
-    for (int a = 0; a < 3; a++) {
-        M.di[a] = p->mdi[a];
-        M.dmi[a] = p->mdmi[a];
-        M.itm[a] = p->mitm[a];
-        M.itz[a] = p->mitz[a];
-    }
-    return M;
-}
 long long padded_size(const bbmg_grid &g) {
     return (g.nx + 2LL * g.ghost) * (g.ny + 2LL * g.ghost) * (g.nz + 2LL * g.ghost);
 }

@@ -108,8 +108,9 @@ class Projection:
                                               _p(P), _p(U), _p(V), _p(W)))
 
     def get_dmomdt(self, U, V, W, P, rho=1.0, visc=None, visc0=0.0, out=None):
-        """Time derivatives of rho U, rho V, rho W (incomp's get_dmomdt) on a
-        triply periodic grid; visc is a cell-centred array or None for visc0."""
+        """Time derivatives of rho U, rho V, rho W (incomp's get_dmomdt); a
+        non-periodic direction has walls at both ends; visc is a cell-centred
+        array or None for visc0."""
         dU, dV, dW = out if out is not None else (self._new(), self._new(), self._new())
         self._check(self.lib.nga_proj_dmomdt(self.h, _p(U), _p(V), _p(W), _p(P), float(rho), _p(visc), float(visc0),
                                              _p(dU), _p(dV), _p(dW)))

@@ -185,12 +185,18 @@ def correct(G, sol, dt, U, V, W, P=None, rho_U=None, rho_V=None, rho_W=None):
 
 
 # ----------------------------------------------------------------------------- momentum
-def momentum_metrics(x):
-    """Extended 1-D metrics of one periodic direction for get_dmomdt: cell
-    sizes' inverses dxi on cells -1..n (index c+1), centroid spacings' inverses
-    dxmi and the edge interpolation weights itp(-1), itp(0) on faces 0..n
-    (incomp_class.f90:250-446, sgrid_class.f90:160-254 with two layers of the
-    naive extension)."""
+def momentum_metrics(x, walls=False):
+    """Extended 1-D metrics of one direction for get_dmomdt: cell sizes'
+    inverses dxi on cells -1..n (index c+1); on faces 0..n the centroid
+    spacings' inverses dxmi and the edge interpolation weights itm, itz (of
+    the values at f-1 and f) (incomp_class.f90:250-446, sgrid_class.f90:
+    160-254 with two layers of the naive extension); then the adjust_metrics
+    versions (incomp_class.f90:449-700) for walls at both ends of a
+    non-periodic direction (cfg%VF = 0 outside the domain): vtm, vtz, gdm,
+    the interpolation weights and gradient coefficient of a velocity
+    component tangential to the direction ([1,0], [0,1] and 1/delta on the
+    wall faces), and wtm, wtz, the 1-D factors of the edge viscosity weights
+    with the wall cell's entry zeroed."""
     x = np.asarray(x, np.float64)
     n = x.size - 1
     xe = np.empty(n + 5)              # nodes -2 .. n+2 at index +2
@@ -206,160 +212,131 @@ def momentum_metrics(x):
     dxmi = 1.0 / (xm[f + 2] - xm[f + 1])
     itm = dxmi * (xm[f + 2] - xe[f + 2])   # weight of the value at index f-1
     itz = dxmi * (xe[f + 2] - xm[f + 1])   # weight of the value at index f
-    return dxi, dxmi, itm, itz
+    vtm, vtz, gdm, wtm, wtz = itm.copy(), itz.copy(), dxmi.copy(), itm.copy(), itz.copy()
+    if walls:
+        vtm[0], vtz[0], gdm[0] = 1.0, 0.0, 1.0 / (xm[2] - xe[2])              # delta = xm(0) - x(0)
+        vtm[n], vtz[n], gdm[n] = 0.0, 1.0, 1.0 / (xe[n + 2] - xm[n + 1])      # delta = x(n) - xm(n-1)
+        wtm[0] = 0.0                                                          # cell -1 is wall
+        wtz[n] = 0.0                                                          # cell n is wall
+    return dxi, dxmi, itm, itz, vtm, vtz, gdm, wtm, wtz
 
 
 def dmomdt(G, U, V, W, P, rho, visc):
-    """get_dmomdt (incomp_class.f90:1021-1159) on a triply periodic grid: the
-    time derivatives of rho U, rho V, rho W on the interior faces, term for
-    term (constant density rho, cell-centred viscosity array visc).  Ghost
-    layers of U, V, W, P and visc must hold the periodic images."""
-    assert all(G.per), "periodic directions only"
-    mx, my, mz = (momentum_metrics(a) for a in (G.xn, G.yn, G.zn))
+    """get_dmomdt (incomp_class.f90:1021-1159): the time derivatives of rho U,
+    rho V, rho W on the interior faces, term for term (constant density rho,
+    cell-centred viscosity array visc).  A non-periodic direction has walls
+    at both ends (cfg%VF = 0 outside the domain): edge coefficients from
+    adjust_metrics and a zero derivative of the wall-normal component on the
+    wall faces (divu = 0 where umask > 0).  Ghost layers of periodic
+    directions must hold the periodic images."""
+    walls = [not p for p in G.per]
+    ms = [momentum_metrics(a, w) for a, w in zip((G.xn, G.yn, G.zn), walls)]
     nx, ny, nz = G.nx, G.ny, G.nz
+    ns = (nx, ny, nz)
     c23 = 2.0 / 3.0
 
     def A(a, dx=0, dy=0, dz=0):
         return G.interior(a, di=dx, dj=dy, dk=dz)
 
-    def cx(m, off):   # cell metric at interior index + off, broadcast along x
-        return m[0][1 + off:1 + off + nx][None, None, :]
+    def shape(d, v):  # broadcast a 1-D array along direction d
+        return v[None, None, :] if d == 0 else (v[None, :, None] if d == 1 else v[:, None, None])
 
-    def cy(m, off):
-        return m[0][1 + off:1 + off + ny][None, :, None]
+    def cell(d, off):  # dxi of direction d at interior cell index + off
+        return shape(d, ms[d][0][1 + off:1 + off + ns[d]])
 
-    def cz(m, off):
-        return m[0][1 + off:1 + off + nz][:, None, None]
+    def face(d, q, off):  # face metric q of direction d at interior index + off
+        return shape(d, ms[d][q][off:off + ns[d]])
 
-    def fx(m, q, off):  # face metric q (1 dxmi, 2 itm, 3 itz) at face i + off
-        return m[q][off:off + nx][None, None, :]
-
-    def fy(m, q, off):
-        return m[q][off:off + ny][None, :, None]
-
-    def fz(m, q, off):
-        return m[q][off:off + nz][:, None, None]
+    def wall_face(d, off):  # the face (interior index + off) along d lies on a wall
+        idx = np.arange(off, off + ns[d])
+        return shape(d, walls[d] & ((idx == 0) | (idx == ns[d])))
 
     def two(a0, b0, a1, b1):  # sum(a(:)*b(:)) of two terms
         return a0 * b0 + a1 * b1
 
+    def shifted(o, d, s):
+        p = list(o)
+        p[d] += s
+        return p
+
     # divergence at a cell, the divp sums of the normal fluxes
     def divc(ox, oy, oz):
-        dxi, dyi, dzi = cx(mx, ox), cy(my, oy), cz(mz, oz)
+        dxi, dyi, dzi = cell(0, ox), cell(1, oy), cell(2, oz)
         sx = two(dxi * -1.0, A(U, ox, oy, oz), dxi * 1.0, A(U, ox + 1, oy, oz))
         sy = two(dyi * -1.0, A(V, ox, oy, oz), dyi * 1.0, A(V, ox, oy + 1, oz))
         sz = two(dzi * -1.0, A(W, ox, oy, oz), dzi * 1.0, A(W, ox, oy, oz + 1))
         return (sx + sy) + sz
 
     def normal(Q, d, off):  # FX of rhoU (d=0), FY of rhoV (1), FZ of rhoW (2) at cell + off along d
-        o = [0, 0, 0]
-        o[d] = off
-        m = (mx, my, mz)[d]
-        ci = (cx, cy, cz)[d](m, off)
-        sh = [0, 0, 0]
-        sh[d] = 1
-        q0, q1 = A(Q, *o), A(Q, o[0] + sh[0], o[1] + sh[1], o[2] + sh[2])
+        o = shifted([0, 0, 0], d, off)
+        ci = cell(d, off)
+        q0, q1 = A(Q, *o), A(Q, *shifted(o, d, 1))
         s1 = two(0.5, q0, 0.5, q1)
         g = two(ci * -1.0, q0, ci * 1.0, q1)
         return ((-(rho * s1 * s1)) + A(visc, *o) * ((g + g) - c23 * divc(*o))) - A(P, *o)
 
-    def edge(d1, d2, o1, o2, Qa, Qb):
-        """Edge flux in the (d1, d2) plane at face offsets o1 (along d1), o2 (along d2):
-        -rho (itp_{d1} Qa) (itp_{d2} Qb) + (itp_2d visc) (grd_{d1} Qa + grd_{d2} Qb), where Qa
-        varies along d1 and Qb along d2; the 2-D viscosity sum runs over (s1 along d1,
-        s2 along d2) in Fortran order (first index fastest) of the reference's itp_xy/yz/xz."""
-        o = [0, 0, 0]
-        o[d1] += o1
-        o[d2] += o2
-        m1, m2 = (mx, my, mz)[d1], (mx, my, mz)[d2]
-        f1, f2 = (fx, fy, fz)[d1], (fx, fy, fz)[d2]
-        e1 = [0, 0, 0]
-        e1[d1] = -1
-        e2 = [0, 0, 0]
-        e2[d2] = -1
-        qa_m = A(Qa, o[0] + e1[0], o[1] + e1[1], o[2] + e1[2])
-        qa_0 = A(Qa, *o)
-        qb_m = A(Qb, o[0] + e2[0], o[1] + e2[1], o[2] + e2[2])
-        qb_0 = A(Qb, *o)
-        a = two(f1(m1, 2, o1), qa_m, f1(m1, 3, o1), qa_0)
-        b = two(f2(m2, 2, o2), qb_m, f2(m2, 3, o2), qb_0)
-        return a, b, qa_m, qa_0, qb_m, qb_0, o, (m1, f1, o1), (m2, f2, o2)
+    def tang(d, off, cw):
+        """Interpolation weights and gradient pair along d at face + off of a
+        component whose own face is a wall face (cw) or not."""
+        tm = np.where(cw, face(d, 2, off), face(d, 4, off))
+        tz = np.where(cw, face(d, 3, off), face(d, 5, off))
+        g = face(d, 6, off)
+        return tm, tz, np.where(cw, 0.0, -g), np.where(cw, 0.0, g)
 
-    def visc2(dlo, dhi, o, wlo, whi):
-        # itp_2d(st_lo, st_hi) = itp_lo(st_lo) itp_hi(st_hi) (incomp_class.f90:277-288), rescaled
-        # by its sum in adjust_metrics (incomp_class.f90:505-511); then sum(itp_2d * visc(..)),
-        # both sums over (st_lo, st_hi) in {-1,0}^2 with st_lo fastest
-        (mlo, flo, olo), (mhi, fhi, ohi) = wlo, whi
-        itl = {-1: flo(mlo, 2, olo), 0: flo(mlo, 3, olo)}
-        ith = {-1: fhi(mhi, 2, ohi), 0: fhi(mhi, 3, ohi)}
+    def edge(d1, o1, d2, o2, Qa, Qb):
+        """Edge flux in the (d1, d2) plane at face offsets o1 (along d1), o2 (along d2),
+        Qa the component along d2 varying along d1, Qb the component along d1 varying
+        along d2: -rho (itp_d1 Qa) (itp_d2 Qb) + (itp_2d visc) (grd_d1 Qa + grd_d2 Qb)."""
+        o = shifted(shifted([0, 0, 0], d1, o1), d2, o2)
+        qa_m, qa_0 = A(Qa, *shifted(o, d1, -1)), A(Qa, *o)
+        qb_m, qb_0 = A(Qb, *shifted(o, d2, -1)), A(Qb, *o)
+        am, az, gam, gaz = tang(d1, o1, wall_face(d2, o2))
+        bm, bz, gbm, gbz = tang(d2, o2, wall_face(d1, o1))
+        a = two(am, qa_m, az, qa_0)
+        b = two(bm, qb_m, bz, qb_0)
+        g = two(gam, qa_m, gaz, qa_0) + two(gbm, qb_m, gbz, qb_0)
+        # itp_2d(st_lo, st_hi) = itp_lo(st_lo) itp_hi(st_hi) (incomp_class.f90:277-288), wall
+        # cells' entries zeroed and the rest rescaled by the sum (adjust_metrics,
+        # incomp_class.f90:497-511); sums over (st_lo, st_hi) with st_lo fastest
+        (dlo, olo), (dhi, ohi) = sorted(((d1, o1), (d2, o2)))
+        itl = {-1: face(dlo, 7, olo), 0: face(dlo, 8, olo)}
+        ith = {-1: face(dhi, 7, ohi), 0: face(dhi, 8, ohi)}
         order = [(sl, sh) for sh in (-1, 0) for sl in (-1, 0)]
         w = {key: itl[key[0]] * ith[key[1]] for key in order}
         mysum = ((w[order[0]] + w[order[1]]) + w[order[2]]) + w[order[3]]
         assert np.all(mysum > 0.0)
-        w = {key: val / mysum for key, val in w.items()}
-        s = None
+        vi = None
         for sl, sh in order:
-            p = list(o)
-            p[dlo] += sl
-            p[dhi] += sh
-            t = w[(sl, sh)] * A(visc, *p)
-            s = t if s is None else s + t
-        return s
-
-    def grd(m, f, off, q_m, q_0):
-        dmi = f(m, 1, off)
-        return two(dmi * -1.0, q_m, dmi * 1.0, q_0)
+            t = (w[(sl, sh)] / mysum) * A(visc, *shifted(shifted(o, dlo, sl), dhi, sh))
+            vi = t if vi is None else vi + t
+        return (-(rho * a * b)) + vi * g
 
     # ---- rho U: FX at cells i-1, i; FY at xy edges (i, j), (i, j+1); FZ at xz edges (i, k), (i, k+1)
     FX = [normal(U, 0, -1), normal(U, 0, 0)]
-    FY, FZ = [], []
-    for oy in (0, 1):
-        a, b, qa_m, qa_0, qb_m, qb_0, o, w1, w2 = edge(1, 0, oy, 0, U, V)   # a: itpu_y U, b: itpv_x V
-        vi = visc2(0, 1, o, w2, w1)                                           # itp_xy(x fastest, y)
-        g = grd(*w1[:2], w1[2], qa_m, qa_0) + grd(*w2[:2], w2[2], qb_m, qb_0)
-        FY.append((-(rho * a * b)) + vi * g)
-    for oz in (0, 1):
-        a, b, qa_m, qa_0, qb_m, qb_0, o, w1, w2 = edge(2, 0, oz, 0, U, W)   # a: itpu_z U, b: itpw_x W
-        vi = visc2(0, 2, o, w2, w1)                                           # itp_xz(x fastest, z)
-        g = grd(*w1[:2], w1[2], qa_m, qa_0) + grd(*w2[:2], w2[2], qb_m, qb_0)
-        FZ.append((-(rho * a * b)) + vi * g)
-    dmx = fx(mx, 1, 0)
-    dU = (two(dmx * -1.0, FX[0], dmx * 1.0, FX[1]) + two(cy(my, 0) * -1.0, FY[0], cy(my, 0) * 1.0, FY[1])) \
-        + two(cz(mz, 0) * -1.0, FZ[0], cz(mz, 0) * 1.0, FZ[1])
+    FY = [edge(1, oy, 0, 0, U, V) for oy in (0, 1)]
+    FZ = [edge(2, oz, 0, 0, U, W) for oz in (0, 1)]
+    dmx, dy, dz = face(0, 1, 0), cell(1, 0), cell(2, 0)
+    dU = (two(dmx * -1.0, FX[0], dmx * 1.0, FX[1]) + two(dy * -1.0, FY[0], dy * 1.0, FY[1])) \
+        + two(dz * -1.0, FZ[0], dz * 1.0, FZ[1])
+    dU = np.where(wall_face(0, 0), 0.0, dU)
 
     # ---- rho V: FX at xy edges (i, j), (i+1, j); FY at cells j-1, j; FZ at yz edges (j, k), (j, k+1)
-    FX, FZ = [], []
-    for ox in (0, 1):
-        a, b, qa_m, qa_0, qb_m, qb_0, o, w1, w2 = edge(0, 1, ox, 0, V, U)   # a: itpv_x V, b: itpu_y U
-        vi = visc2(0, 1, o, w1, w2)
-        g = grd(*w1[:2], w1[2], qa_m, qa_0) + grd(*w2[:2], w2[2], qb_m, qb_0)
-        FX.append((-(rho * a * b)) + vi * g)
+    FX = [edge(0, ox, 1, 0, V, U) for ox in (0, 1)]
     FY = [normal(V, 1, -1), normal(V, 1, 0)]
-    for oz in (0, 1):
-        a, b, qa_m, qa_0, qb_m, qb_0, o, w1, w2 = edge(2, 1, oz, 0, V, W)   # a: itpv_z V, b: itpw_y W
-        vi = visc2(1, 2, o, w2, w1)                                           # itp_yz(y fastest, z)
-        g = grd(*w1[:2], w1[2], qa_m, qa_0) + grd(*w2[:2], w2[2], qb_m, qb_0)
-        FZ.append((-(rho * a * b)) + vi * g)
-    dmy = fy(my, 1, 0)
-    dV = (two(cx(mx, 0) * -1.0, FX[0], cx(mx, 0) * 1.0, FX[1]) + two(dmy * -1.0, FY[0], dmy * 1.0, FY[1])) \
-        + two(cz(mz, 0) * -1.0, FZ[0], cz(mz, 0) * 1.0, FZ[1])
+    FZ = [edge(2, oz, 1, 0, V, W) for oz in (0, 1)]
+    dx, dmy = cell(0, 0), face(1, 1, 0)
+    dV = (two(dx * -1.0, FX[0], dx * 1.0, FX[1]) + two(dmy * -1.0, FY[0], dmy * 1.0, FY[1])) \
+        + two(dz * -1.0, FZ[0], dz * 1.0, FZ[1])
+    dV = np.where(wall_face(1, 0), 0.0, dV)
 
     # ---- rho W: FX at xz edges (i, k), (i+1, k); FY at yz edges (j, k), (j+1, k); FZ at cells k-1, k
-    FX, FY = [], []
-    for ox in (0, 1):
-        a, b, qa_m, qa_0, qb_m, qb_0, o, w1, w2 = edge(0, 2, ox, 0, W, U)   # a: itpw_x W, b: itpu_z U
-        vi = visc2(0, 2, o, w1, w2)
-        g = grd(*w1[:2], w1[2], qa_m, qa_0) + grd(*w2[:2], w2[2], qb_m, qb_0)
-        FX.append((-(rho * a * b)) + vi * g)
-    for oy in (0, 1):
-        a, b, qa_m, qa_0, qb_m, qb_0, o, w1, w2 = edge(1, 2, oy, 0, W, V)   # a: itpw_y W, b: itpv_z V
-        vi = visc2(1, 2, o, w1, w2)
-        g = grd(*w1[:2], w1[2], qa_m, qa_0) + grd(*w2[:2], w2[2], qb_m, qb_0)
-        FY.append((-(rho * a * b)) + vi * g)
+    FX = [edge(0, ox, 2, 0, W, U) for ox in (0, 1)]
+    FY = [edge(1, oy, 2, 0, W, V) for oy in (0, 1)]
     FZ = [normal(W, 2, -1), normal(W, 2, 0)]
-    dmz = fz(mz, 1, 0)
-    dW = (two(cx(mx, 0) * -1.0, FX[0], cx(mx, 0) * 1.0, FX[1]) + two(cy(my, 0) * -1.0, FY[0], cy(my, 0) * 1.0, FY[1])) \
+    dmz = face(2, 1, 0)
+    dW = (two(dx * -1.0, FX[0], dx * 1.0, FX[1]) + two(dy * -1.0, FY[0], dy * 1.0, FY[1])) \
         + two(dmz * -1.0, FZ[0], dmz * 1.0, FZ[1])
+    dW = np.where(wall_face(2, 0), 0.0, dW)
     out = []
     for d in (dU, dV, dW):
         a = np.zeros(G.padded)

@@ -292,16 +292,19 @@ def test_oracle_dmomdt_converges_on_taylor_green():
     assert errs[0] < 0.05 and errs[1] < errs[0] / 3.5, errs
 
 
-PCASES = [((12, 10, 9), 1), ((8, 8, 8), 2), ((16, 12, 10), 2), ((5, 17, 6), 1)]
-PIDS = ["x".join(map(str, d)) + f"-g{g}" for d, g in PCASES]
+PCASES = [((12, 10, 9), (True, True, True), 1), ((8, 8, 8), (True, True, True), 2),
+          ((16, 12, 10), (True, True, True), 2), ((5, 17, 6), (True, True, True), 1),
+          ((12, 10, 9), (True, False, True), 1), ((8, 8, 8), (False, False, False), 2),
+          ((16, 12, 10), (False, True, True), 1), ((6, 9, 7), (True, True, False), 2)]
+PIDS = ["x".join(map(str, d)) + "-" + "".join("p" if p else "w" for p in per) + f"-g{g}" for d, per, g in PCASES]
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("dims,g", PCASES, ids=PIDS)
-def test_dmomdt_bitexact(dims, g):
-    """k_dmomdt equals the oracle's get_dmomdt bit for bit on stretched
-    periodic grids, with a viscosity array and with a constant viscosity."""
-    per = (True, True, True)
+@pytest.mark.parametrize("dims,per,g", PCASES, ids=PIDS)
+def test_dmomdt_bitexact(dims, per, g):
+    """k_dmomdt equals the oracle's get_dmomdt bit for bit on stretched grids,
+    periodic or with walls, with a viscosity array and with a constant
+    viscosity (random values in every overlap and wall cell)."""
     G, pr, (U, V, W, Pr, _), T = gpu_setup(dims, per, g, 11)
     U, V, W, Pr = (G.sync(a) for a in (U, V, W, Pr))
     rng = np.random.default_rng(12)
@@ -315,9 +318,23 @@ def test_dmomdt_bitexact(dims, g):
     pr.close()
 
 
-@pytest.mark.gpu
-def test_dmomdt_rejects_walls():
-    G, pr, (U, V, W, Pr, _), T = gpu_setup((8, 8, 8), (True, False, True), 1, 13)
-    with pytest.raises(RuntimeError, match="periodic"):
-        pr.get_dmomdt(T(U), T(V), T(W), T(Pr))
-    pr.close()
+def test_oracle_dmomdt_walls_poiseuille():
+    """A parabolic channel profile between walls in y (zero velocity in the
+    wall cells): the viscous term is mu U'' = -8 mu Um exactly in the interior
+    rows and -6 mu Um in the rows next to the walls, where the wall gradient
+    is NGA2's one-sided (U(0) - U_wall) / (ym(0) - y(0)); the other components'
+    derivatives vanish."""
+    nx, ny, nz, mu, um, rho = 8, 16, 4, 0.02, 1.5, 1.3
+    xn, yn, zn = P.uniform_nodes(nx, 2.0), P.uniform_nodes(ny), P.uniform_nodes(nz, 0.5)
+    G = PO.Grid(xn, yn, zn, (True, False, True), 1)
+    ym = 0.5 * (yn[:-1] + yn[1:])
+    U = np.zeros(G.padded)
+    G.interior(U)[...] = (4.0 * um * ym * (1.0 - ym))[None, :, None]
+    U = G.sync(U)
+    Z = np.zeros(G.padded)
+    dU, dV, dW = PO.dmomdt(G, U, Z, Z, Z, rho, np.full(G.padded, mu))
+    d = G.interior(dU)
+    ref = np.full(d.shape, -8.0 * mu * um)
+    ref[:, 0, :] = ref[:, -1, :] = -6.0 * mu * um
+    assert np.abs(d - ref).max() < 1e-11
+    assert np.abs(G.interior(dV)).max() < 1e-12 and np.abs(G.interior(dW)).max() < 1e-12
