@@ -1,15 +1,19 @@
-// projection.cu -- the projection steps either side of the pressure solve on
-// the GPU: operator assembly, divergence and right-hand side, mean removal,
-// pressure gradient and velocity correction (nga_projection.h).
+// projection.cu -- the steps of the flow solvers' time loop around the
+// pressure solve on the GPU (nga_projection.h): operator assembly, divergence
+// and right-hand side, mean removal, pressure gradient and velocity
+// correction; get_dmomdt, the sub-iteration updates and the flow statistics
+// of the incompressible time loop.
 //
-// Every kernel is a single pass over the interior in the caller's padded
-// Fortran layout (i fastest): one thread per cell, consecutive threads on
-// consecutive i, so every array access of a warp is one contiguous run.  The
-// metrics are 1-D (a rectilinear pgrid) and stay in L1.  HBM traffic per
-// cell, FP64: assembly 3 face densities in + 7 coefficients out (80 B);
-// divergence 3 velocities in + div and rhs out (40 B); correction sol,
-// 3 densities, 3 velocities and P in, 3 velocities and P out (96 B);
-// mean removal 2 passes of 8 + 16 B.
+// Every kernel is a single pass over the interior (or, for the whole-array
+// updates, the padded array) in the caller's Fortran layout (i fastest): one
+// thread per cell, consecutive threads on consecutive i, so every array
+// access of a warp is one contiguous run.  The metrics are 1-D (a rectilinear
+// pgrid) and stay in L1.  HBM traffic per cell, FP64: assembly 3 face
+// densities in + 7 coefficients out (80 B); divergence 3 velocities in + div
+// and rhs out (40 B); correction sol, 3 densities, 3 velocities and P in,
+// 3 velocities and P out (96 B); mean removal 2 passes of 8 + 16 B;
+// get_dmomdt U, V, W, P, visc in + 3 derivatives out (64 B, the neighbour
+// planes from L1/L2); midpoint 72 B; explicit update 96 B; statistics 24 B.
 //
 // Arithmetic follows the reference's expressions term for term with
 // __dadd_rn / __dmul_rn / __ddiv_rn (no contraction), so outputs equal the
