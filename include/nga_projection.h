@@ -130,9 +130,22 @@ int nga_proj_advance(nga_proj *p, double dt, double rho, double *U, double *V, d
  * volume means of U, V, W (config_class.f90:196-214 / fluid_vol).  visc may
  * be NULL for visc0 everywhere.  The sums are fixed-order parallel
  * reductions (round-off from the reference's sequential loops; the maxima
- * are exact).  Triply periodic grids only. */
+ * are exact).  With walls the velocity on the wall faces enters as the
+ * reference's arrays hold it (the no-slip value). */
 int nga_proj_flow_stats(nga_proj *p, const double *U, const double *V, const double *W, const double *visc,
                         double visc0, double rho, double dt, double *out);
+
+/* The 7-point operator that solve_implicit (incomp_class.f90:1744-1910)
+ * assembles for velocity component comp (0 U, 1 V, 2 W) before its implicit
+ * solve: rho + dt/2 times the convective terms linearised about U, V, W minus
+ * dt/2 times the viscous terms (viscosity visc, or visc0 when NULL), in
+ * NGA2's stencil order [0,+x,-x,+y,-y,+z,-z], written on the interior cells
+ * of opr ([k][j][i][7], padded like the fields).  Walls as in
+ * nga_proj_dmomdt; the rows of the component's wall faces are rho alone.
+ * The operator goes to bbmg_setup and the momentum residual to bbmg_solve
+ * (bbmg's BBMG_BBOX method: the operator is not symmetric). */
+int nga_proj_implicit_operator(nga_proj *p, int comp, double dt, double rho, const double *U, const double *V,
+                               const double *W, const double *visc, double visc0, double *opr);
 
 #ifdef __cplusplus
 }

@@ -600,6 +600,101 @@ __global__ void __launch_bounds__(kThreads) k_advance(long long n, double dt, do
     }
 }
 
+// The operator solve_implicit assembles for velocity component C
+// (incomp_class.f90:1744-1910), one thread per cell (the component's face at
+// the cell's lower side): rho + dt/2 (linearised convection) - dt/2
+// (viscous terms), stencil order [0, +x, -x, +y, -y, +z, -z], written into the
+// padded [k][j][i][7] array.  Per direction the two terms are summed upper
+// then lower, x, y, z, as the reference does; the rows of the component's
+// wall faces are rho alone (divu = 0 there).
+template <int C>
+__global__ void __launch_bounds__(kThreads) k_implicit_opr(Pad P, MomM M, const double *__restrict__ U,
+                                                            const double *__restrict__ V,
+                                                            const double *__restrict__ W,
+                                                            const double *__restrict__ visc, double visc0, double rho,
+                                                            double dt, double *__restrict__ opr) {
+    const long long n = (long long)P.nx * P.ny * P.nz;
+    const long long st[3] = {1, P.sy, P.sz};
+    const double *Q[3] = {U, V, W};
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        cell_of(P, t, i, j, k);
+        const long long e = P.at(i, j, k);
+        const int fi[3] = {i, j, k};
+        double *out = opr + 7 * e;
+        if (M.wall_face(C, fi[C])) {
+            out[0] = rho;
+#pragma unroll
+            for (int q = 1; q < 7; q++) out[q] = 0.0;
+            continue;
+        }
+        auto vs = [&](long long o) { return visc ? visc[o] : visc0; };
+        double cd[6], vd[6], co[6], vo[6];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const long long sc = st[C], sd = st[d];
+            if (d == C) {
+                const double wn0 = 0.5, wnm = (M.walls[C] && fi[C] == 0) ? 0.0 : 0.5;  // cell f-1 a wall cell
+                const double *q = Q[C];
+                const double rp = pm(pm(rho, pa(pm(wn0, q[e]), pm(wn0, q[e + sc]))), 2.0);
+                const double rm = pm(pm(rho, pa(pm(wnm, q[e - sc]), pm(wnm, q[e]))), 2.0);
+                const double dup = M.dmi[C][fi[C]], dlo = pm(dup, -1.0);
+                cd[2 * d] = pm(pm(dup, wn0), rp);
+                cd[2 * d + 1] = pm(pm(dlo, wnm), rm);
+                co[2 * d] = cd[2 * d];
+                co[2 * d + 1] = cd[2 * d + 1];
+                const double ci0 = M.di[C][fi[C] + 1], cim = M.di[C][fi[C]];
+                const double fu = pm(__ddiv_rn(pm(dup, 4.0), 3.0), vs(e)), fl = pm(__ddiv_rn(pm(dlo, 4.0), 3.0), vs(e - sc));
+                vd[2 * d] = pm(fu, pm(ci0, -1.0));
+                vd[2 * d + 1] = pm(fl, pm(cim, 1.0));
+                vo[2 * d] = pm(fu, pm(ci0, 1.0));
+                vo[2 * d + 1] = pm(fl, pm(cim, -1.0));
+            } else {
+                const bool cw = M.wall_face(C, fi[C]);
+                double am_u, az_u, gm_u, gz_u, am_l, az_l, gm_l, gz_l, bm_u, bz_u, bm_l, bz_l, g0, g1;
+                M.tang(d, fi[d] + 1, cw, am_u, az_u, gm_u, gz_u);
+                M.tang(d, fi[d], cw, am_l, az_l, gm_l, gz_l);
+                M.tang(C, fi[C], M.wall_face(d, fi[d] + 1), bm_u, bz_u, g0, g1);
+                M.tang(C, fi[C], M.wall_face(d, fi[d]), bm_l, bz_l, g0, g1);
+                const double *q = Q[d];
+                const double rp = pm(rho, pa(pm(bm_u, q[e - sc + sd]), pm(bz_u, q[e + sd])));
+                const double rm = pm(rho, pa(pm(bm_l, q[e - sc]), pm(bz_l, q[e])));
+                const double dup = M.di[d][fi[d] + 1], dlo = pm(dup, -1.0);
+                cd[2 * d] = pm(pm(dup, am_u), rp);
+                cd[2 * d + 1] = pm(pm(dlo, az_l), rm);
+                co[2 * d] = pm(pm(dup, az_u), rp);
+                co[2 * d + 1] = pm(pm(dlo, am_l), rm);
+                // edge viscosities at (c-face, d-face + 1) and (c-face, d-face), lower direction first
+                const int lo = C < d ? C : d, hi = C < d ? d : C;
+                const long long sl = st[lo], sh = st[hi];
+                double ve[2];
+#pragma unroll
+                for (int u = 0; u < 2; u++) {
+                    const int fd = fi[d] + (1 - u);
+                    const int flo = lo == C ? fi[C] : fd, fhi = hi == C ? fi[C] : fd;
+                    const long long o = e + (1 - u) * sd;
+                    ve[u] = visc_edge(M.wtm[lo][flo], M.wtz[lo][flo], M.wtm[hi][fhi], M.wtz[hi][fhi], vs(o - sl - sh),
+                                      vs(o - sh), vs(o - sl), vs(o));
+                }
+                vd[2 * d] = pm(pm(dup, ve[0]), gm_u);
+                vd[2 * d + 1] = pm(pm(dlo, ve[1]), gz_l);
+                vo[2 * d] = pm(pm(dup, ve[0]), gz_u);
+                vo[2 * d + 1] = pm(pm(dlo, ve[1]), gm_l);
+            }
+        }
+        double sc = cd[0], sv = vd[0];
+#pragma unroll
+        for (int q = 1; q < 6; q++) {
+            sc = pa(sc, cd[q]);
+            sv = pa(sv, vd[q]);
+        }
+        const double hd = pm(0.5, dt);
+        out[0] = __dsub_rn(pa(rho, pm(hd, sc)), pm(hd, sv));
+#pragma unroll
+        for (int q = 0; q < 6; q++) out[q + 1] = __dsub_rn(pa(0.0, pm(hd, co[q])), pm(hd, vo[q]));
+    }
+}
+
 // Flow statistics, block partials over the interior cells (fixed grid, fixed
 // per-thread order): q 0-2 max|U|*dxmi (get_cfl, incomp_class.f90:1497-1540),
 // 3-5 max 4*visc*dxi**2/rho, 6 sum 0.5*(Ui**2+Vi**2+Wi**2) with the
@@ -958,8 +1053,6 @@ extern "C" int nga_proj_advance(nga_proj *p, double dt, double rho, double *U, d
 extern "C" int nga_proj_flow_stats(nga_proj *p, const double *U, const double *V, const double *W,
                                    const double *visc, double visc0, double rho, double dt, double *out) {
     if (!p) return pfail(BBMG_BAD_ARGS, "null projection handle");
-    if (!(p->g.xper && p->g.yper && p->g.zper))
-        return pfail(BBMG_BAD_ARGS, "nga_proj_flow_stats needs a triply periodic grid");
     if (!out) return pfail(BBMG_BAD_ARGS, "out is NULL");
     PCHK(check_dev(U, "U"));
     PCHK(check_dev(V, "V"));
@@ -977,3 +1070,28 @@ extern "C" int nga_proj_flow_stats(nga_proj *p, const double *U, const double *V
     PCU(cudaStreamSynchronize(p->stream));
     return BBMG_OK;
 }
+
+extern "C" int nga_proj_implicit_operator(nga_proj *p, int comp, double dt, double rho, const double *U,
+                                          const double *V, const double *W, const double *visc, double visc0,
+                                          double *opr) {
+    if (!p) return pfail(BBMG_BAD_ARGS, "null projection handle");
+    if (comp < 0 || comp > 2) return pfail(BBMG_BAD_ARGS, "comp must be 0 (U), 1 (V) or 2 (W), got %d", comp);
+    PCHK(check_dev(U, "U"));
+    PCHK(check_dev(V, "V"));
+    PCHK(check_dev(W, "W"));
+    PCHK(check_opt(visc, "visc"));
+    PCHK(check_dev(opr, "opr"));
+    PCU(cudaSetDevice(p->device));
+    const Pad P = pad_of(p->g);
+    const long long n = (long long)P.nx * P.ny * P.nz;
+    const MomM M = momentum_of(p);
+    if (comp == 0)
+        k_implicit_opr<0><<<grid_cells(n), kThreads, 0, p->stream>>>(P, M, U, V, W, visc, visc0, rho, dt, opr);
+    else if (comp == 1)
+        k_implicit_opr<1><<<grid_cells(n), kThreads, 0, p->stream>>>(P, M, U, V, W, visc, visc0, rho, dt, opr);
+    else
+        k_implicit_opr<2><<<grid_cells(n), kThreads, 0, p->stream>>>(P, M, U, V, W, visc, visc0, rho, dt, opr);
+    PCU(cudaGetLastError());
+    return BBMG_OK;
+}
+

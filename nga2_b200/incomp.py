@@ -70,10 +70,11 @@ class Incomp:
     with rho = 1, incomp_class.f90:766-785)."""
 
     def __init__(self, xn, yn, zn, rho=1.0, visc=0.0, ghost=1, precision=B.FP64, rcvg=1e-10, maxit=100,
-                 device=0):
+                 device=0, per=(True, True, True), implicit_rcvg=1e-6, implicit_maxit=100):
         import torch
         self.torch = torch
-        self.proj = Projection(xn, yn, zn, True, True, True, ghost=ghost, device=device)
+        self.per = tuple(bool(p) for p in per)
+        self.proj = Projection(xn, yn, zn, *self.per, ghost=ghost, device=device)
         g = self.proj.grid
         self.nx, self.ny, self.nz, self.g = g.nx, g.ny, g.nz, ghost
         self.shape = self.proj.shape
@@ -86,21 +87,30 @@ class Incomp:
         self.visc = torch.full(self.shape, float(visc), dtype=torch.float64, device="cuda")
         self.rho_face = torch.full(self.shape, self.rho, dtype=torch.float64, device="cuda")
         self.opr = self.proj.update_laplacian()
-        self.psolv = B.BBMG(self.nx, self.ny, self.nz, True, True, True, ghost=ghost, method=B.PCG_BBOX,
+        self.psolv = B.BBMG(self.nx, self.ny, self.nz, *self.per, ghost=ghost, method=B.PCG_BBOX,
                             precision=precision, rcvg=rcvg, maxit=maxit, device=device)
         self.psolv.setup(STC7, self.opr)
         self.psolv_it, self.psolv_rerr = 0, 0.0
+        # the implicit velocity solver (created on first use): bbmg's multigrid
+        # iteration, since the implicit operator is not symmetric
+        self.implicit_rcvg, self.implicit_maxit, self.device = implicit_rcvg, implicit_maxit, device
+        self.isolv = None
+        self.implicit_its = []
         self.solve_ms = 0.0  # device time of the pressure solves, accumulated
 
     # ------------------------------------------------------------ operations
     def sync(self, a):
-        """cfg%sync: the overlap of a padded field takes the periodic images."""
-        torch = self.torch
+        """cfg%sync: the overlap of a padded field takes the periodic images
+        (periodic directions only; the overlap of a wall direction is left)."""
         g = self.g
         if g == 0:
             return a
-        i = a[g:-g, g:-g, g:-g]
-        a.copy_(torch.nn.functional.pad(i[None], (g, g, g, g, g, g), mode="circular")[0])
+        for ax, per in ((2, self.per[0]), (1, self.per[1]), (0, self.per[2])):
+            if not per:
+                continue
+            n = a.shape[ax] - 2 * g
+            a.narrow(ax, 0, g).copy_(a.narrow(ax, n, g))
+            a.narrow(ax, n + g, g).copy_(a.narrow(ax, g, g))
         return a
 
     def get_dmomdt(self):
@@ -122,6 +132,30 @@ class Incomp:
         s = self.stats(dt)
         cflc = max(s["cflc_x"], s["cflc_y"], s["cflc_z"])
         return cflc, max(cflc, s["cflv_x"], s["cflv_y"], s["cflv_z"])
+
+    def solve_implicit(self, dt, res=None):
+        """solve_implicit (incomp_class.f90:1744-1910): for U, V and W in
+        turn, assemble the operator linearised about the current velocity,
+        solve it from a zero guess with the component's residual as
+        right-hand side, and replace the residual with the solution."""
+        import torch
+        res = res if res is not None else (self.resU, self.resV, self.resW)
+        if self.isolv is None:
+            self.isolv = B.BBMG(self.nx, self.ny, self.nz, *self.per, ghost=self.g, method=B.BBOX, precision=B.FP64,
+                                rcvg=self.implicit_rcvg, maxit=self.implicit_maxit, device=self.device)
+            self.iopr = torch.zeros(self.shape + (7,), dtype=torch.float64, device="cuda")
+            self.isol = torch.zeros(self.shape, dtype=torch.float64, device="cuda")
+        its = []
+        for c, r in enumerate(res):
+            self.proj.implicit_operator(c, dt, self.rho, self.U, self.V, self.W, visc=self.visc, opr=self.iopr)
+            self.isolv.setup(STC7, self.iopr)
+            self.isol.zero_()
+            _, it, rerr, st = self.isolv.solve(r, self.isol)
+            its.append(it)
+            r.copy_(self.isol)
+            self.sync(r)
+        self.implicit_its.append(its)
+        return its
 
     def pressure_projection(self, dt):
         """get_div, rhs = -vol*div*rho/dt, sol = 0, psolv%solve, shift_p,
@@ -169,6 +203,8 @@ class Incomp:
         return a[g:g + self.nz, g:g + self.ny, g:g + self.nx]
 
     def close(self):
+        if self.isolv is not None:
+            self.isolv.close()
         self.psolv.close()
         self.proj.close()
 

@@ -14,7 +14,7 @@ from . import bbmg as B
 
 EXPORTS = ["nga_proj_create", "nga_proj_destroy", "nga_proj_set_stream", "nga_proj_laplacian",
            "nga_proj_divergence", "nga_proj_shift_p", "nga_proj_pgrad", "nga_proj_correct", "nga_proj_dmomdt",
-           "nga_proj_midpoint", "nga_proj_advance", "nga_proj_flow_stats"]
+           "nga_proj_midpoint", "nga_proj_advance", "nga_proj_flow_stats", "nga_proj_implicit_operator"]
 
 _BOUND = False
 
@@ -37,6 +37,7 @@ def lib():
         L.nga_proj_midpoint.argtypes = [P, P, P, P, P, P, P]
         L.nga_proj_advance.argtypes = [P, D, D, P, P, P, P, P, P, P, P, P, D, D, DP]
         L.nga_proj_flow_stats.argtypes = [P, P, P, P, P, D, D, D, DP]
+        L.nga_proj_implicit_operator.argtypes = [P, I, D, D, P, P, P, P, D, P]
         for n in EXPORTS:
             getattr(L, n).restype = C.c_int
         _BOUND = True
@@ -135,6 +136,13 @@ class Projection:
                                                  float(dt), out))
         keys = ("cflc_x", "cflc_y", "cflc_z", "cflv_x", "cflv_y", "cflv_z", "KE", "meanU", "meanV", "meanW")
         return dict(zip(keys, list(out)))
+
+    def implicit_operator(self, comp, dt, rho, U, V, W, visc=None, visc0=0.0, opr=None):
+        """solve_implicit's 7-point operator for component comp (0 U, 1 V, 2 W)."""
+        opr = self._new(7) if opr is None else opr
+        self._check(self.lib.nga_proj_implicit_operator(self.h, int(comp), float(dt), float(rho), _p(U), _p(V),
+                                                        _p(W), _p(visc), float(visc0), _p(opr)))
+        return opr
 
     def close(self):
         if self.h:

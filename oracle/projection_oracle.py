@@ -449,3 +449,118 @@ class HITOracle:
             self.V = advance(dt, self.rho, self.V, Vo, dV, fa, 2.0 * self.tau, mean[1])
             self.W = advance(dt, self.rho, self.W, Wo, dW, fa, 2.0 * self.tau, mean[2])
             self._project(dt)
+
+
+def implicit_operator(G, comp, dt, rho, U, V, W, visc):
+    """The 7-point operator solve_implicit assembles for velocity component
+    comp (0 U, 1 V, 2 W) (incomp_class.f90:1744-1910): rho on the diagonal
+    plus 0.5*dt times the linearised convective terms, minus 0.5*dt times the
+    viscous terms, in NGA2's stencil order [0, +x, -x, +y, -y, +z, -z]; the
+    interior of a (nz, ny, nx, 7) array.  Walls as in dmomdt: the metrics of
+    non-periodic directions carry adjust_metrics' wall coefficients and the
+    rows of the component's wall faces are rho alone."""
+    walls = [not p for p in G.per]
+    ms = [momentum_metrics(a, w) for a, w in zip((G.xn, G.yn, G.zn), walls)]
+    ns = (G.nx, G.ny, G.nz)
+    Q = (U, V, W)
+    c = comp
+
+    def A(a, o):
+        return G.interior(a, di=o[0], dj=o[1], dk=o[2])
+
+    def shape(d, v):
+        return v[None, None, :] if d == 0 else (v[None, :, None] if d == 1 else v[:, None, None])
+
+    def cell(d, off):
+        return shape(d, ms[d][0][1 + off:1 + off + ns[d]])
+
+    def face(d, q, off):
+        return shape(d, ms[d][q][off:off + ns[d]])
+
+    def wall_face(d, off):
+        idx = np.arange(off, off + ns[d])
+        return shape(d, walls[d] & ((idx == 0) | (idx == ns[d])))
+
+    def sh(d, s):
+        o = [0, 0, 0]
+        o[d] = s
+        return o
+
+    def add(o1, o2):
+        return [a + b for a, b in zip(o1, o2)]
+
+    def tang(d, off, cw):
+        tm = np.where(cw, face(d, 2, off), face(d, 4, off))
+        tz = np.where(cw, face(d, 3, off), face(d, 5, off))
+        g = face(d, 6, off)
+        return tm, tz, np.where(cw, 0.0, -g), np.where(cw, 0.0, g)
+
+    def visc_edge(d, off):
+        """Viscosity at the edge in the (c, d) plane at c-face 0 and d-face off."""
+        (dlo, olo), (dhi, ohi) = sorted(((c, 0), (d, off)))
+        itl = {-1: face(dlo, 7, olo), 0: face(dlo, 8, olo)}
+        ith = {-1: face(dhi, 7, ohi), 0: face(dhi, 8, ohi)}
+        order = [(sl, s2) for s2 in (-1, 0) for sl in (-1, 0)]
+        w = {key: itl[key[0]] * ith[key[1]] for key in order}
+        mysum = ((w[order[0]] + w[order[1]]) + w[order[2]]) + w[order[3]]
+        base = sh(d, off)
+        v = None
+        for sl, s2 in order:
+            t = (w[(sl, s2)] / mysum) * A(visc, add(add(base, sh(dlo, sl)), sh(dhi, s2)))
+            v = t if v is None else v + t
+        return v
+
+    conv_d, conv_off = [], {}
+    visc_d, visc_off = [], {}
+    for d in range(3):
+        if d == c:
+            # normal: cells f (above) and f-1 (below) of the face; itpn = [0.5, 0.5] (0 in wall cells)
+            def itpn(off):
+                idx = np.arange(off, off + ns[c])
+                wallcell = walls[c] & ((idx < 0) | (idx >= ns[c]))
+                return shape(c, np.where(wallcell, 0.0, 0.5))
+            rp = (rho * (itpn(0) * A(Q[c], [0, 0, 0]) + itpn(0) * A(Q[c], sh(c, 1)))) * 2.0
+            rm = (rho * (itpn(-1) * A(Q[c], sh(c, -1)) + itpn(-1) * A(Q[c], [0, 0, 0]))) * 2.0
+            dup, dlo = face(c, 1, 0), face(c, 1, 0) * -1.0
+            tp, tm_ = (dup * itpn(0)) * rp, (dlo * itpn(-1)) * rm
+            op, om = (dup * itpn(0)) * rp, (dlo * itpn(-1)) * rm
+            ci0, cim = cell(c, 0), cell(c, -1)
+            vp = (((dup * 4.0) / 3.0) * A(visc, [0, 0, 0])) * (ci0 * -1.0)
+            vm = (((dlo * 4.0) / 3.0) * A(visc, sh(c, -1))) * (cim * 1.0)
+            wp = (((dup * 4.0) / 3.0) * A(visc, [0, 0, 0])) * (ci0 * 1.0)
+            wm = (((dlo * 4.0) / 3.0) * A(visc, sh(c, -1))) * (cim * -1.0)
+        else:
+            # tangential: edges at d-faces g+1 (upper) and g (lower) of the cell row
+            cw_c = wall_face(c, 0)                       # the component's own face on a wall
+            am_u, az_u, gm_u, gz_u = tang(d, 1, cw_c)    # Q_c along d at edge g+1
+            am_l, az_l, gm_l, gz_l = tang(d, 0, cw_c)    # Q_c along d at edge g
+            bm_u, bz_u, _, _ = tang(c, 0, wall_face(d, 1))  # Q_d along c at the c-face, edge g+1
+            bm_l, bz_l, _, _ = tang(c, 0, wall_face(d, 0))
+            qd = Q[d]
+            rp = rho * (bm_u * A(qd, add(sh(c, -1), sh(d, 1))) + bz_u * A(qd, sh(d, 1)))
+            rm = rho * (bm_l * A(qd, sh(c, -1)) + bz_l * A(qd, [0, 0, 0]))
+            dup, dlo = cell(d, 0), cell(d, 0) * -1.0
+            tp, tm_ = (dup * am_u) * rp, (dlo * az_l) * rm
+            op, om = (dup * az_u) * rp, (dlo * am_l) * rm
+            veu, vel = visc_edge(d, 1), visc_edge(d, 0)
+            vp, vm = (dup * veu) * gm_u, (dlo * vel) * gz_l
+            wp, wm = (dup * veu) * gz_u, (dlo * vel) * gm_l
+        conv_d += [tp, tm_]
+        visc_d += [vp, vm]
+        conv_off[(d, 1)], conv_off[(d, -1)] = op, om
+        visc_off[(d, 1)], visc_off[(d, -1)] = wp, wm
+    hd = 0.5 * dt
+    s = conv_d[0]
+    for t in conv_d[1:]:
+        s = s + t
+    v = visc_d[0]
+    for t in visc_d[1:]:
+        v = v + t
+    out = np.zeros((G.nz, G.ny, G.nx, 7))
+    out[..., 0] = (rho + hd * s) - hd * v
+    for q, key in enumerate([(0, 1), (0, -1), (1, 1), (1, -1), (2, 1), (2, -1)], start=1):
+        out[..., q] = (0.0 + hd * conv_off[key]) - hd * visc_off[key]
+    wf = wall_face(c, 0)
+    out[..., 0] = np.where(wf, rho, out[..., 0])
+    out[..., 1:] = np.where(wf[..., None], 0.0, out[..., 1:])
+    return out
