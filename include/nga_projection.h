@@ -147,6 +147,29 @@ int nga_proj_flow_stats(nga_proj *p, const double *U, const double *V, const dou
 int nga_proj_implicit_operator(nga_proj *p, int comp, double dt, double rho, const double *U, const double *V,
                                const double *W, const double *visc, double visc0, double *opr);
 
+/* The explicit residual of a sub-iteration that is followed by
+ * solve_implicit (examples/channel simulation.f90:290-301), whole padded
+ * arrays: resU = -2*(rho*U - rho*Uold) + dt*resU (resU holding drhoUdt on
+ * entry), V and W likewise; then for each component whose bit is set in
+ * force_mask (1 U, 2 V, 4 W) resU = (resU + force[0]) - force[1] where umask
+ * is 0 (force[2..3] for V, force[4..5] for W; host array; the channel's
+ * Ubulk and meanU). */
+int nga_proj_mom_residual(nga_proj *p, double dt, double rho, const double *U, const double *V, const double *W,
+                          const double *Uold, const double *Vold, const double *Wold, double *resU, double *resV,
+                          double *resW, int force_mask, const double *force);
+
+/* U = 2*U - Uold + resU after solve_implicit (examples/channel
+ * simulation.f90:319-321), V and W likewise, whole padded arrays. */
+int nga_proj_apply_residual(nga_proj *p, double *U, double *V, double *W, const double *Uold, const double *Vold,
+                            const double *Wold, const double *resU, const double *resV, const double *resW);
+
+/* The bulk-velocity sums of the channel forcing (examples/channel
+ * simulation.f90:280-298) over the interior faces with umask = 0, into the
+ * host array out[6]: sum(dxm*dy*dz*(2*U - Uold)), sum(dxm*dy*dz) for U, then
+ * the same for V (dx*dym*dz) and W (dx*dy*dzm).  Fixed-order parallel sums. */
+int nga_proj_bulk(nga_proj *p, const double *U, const double *V, const double *W, const double *Uold,
+                  const double *Vold, const double *Wold, double *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -46,7 +46,7 @@ struct nga_proj {
     // momentum metrics per direction (two layers of the naive extension):
     // dxi on cells -1..n (index c+1), dxmi and the edge weights itm (of the
     // value at f-1) and itz (of the value at f) on faces 0..n
-    const double *mom[3][9] = {};  // per direction, in momentum_metrics' order
+    const double *mom[3][10] = {};  // per direction, in momentum_metrics' order
     double *mmetrics = nullptr;
 };
 
@@ -353,7 +353,7 @@ void axis_metrics(const double *x, int n, bool per, std::vector<double> &dp0, st
 // the direction at its faces -- [1,0], [0,1] and [-1,+1]/delta on the two
 // wall faces -- and 7/8 the 1-D factors of the edge viscosity weights with the
 // wall cell's entry zeroed.  Periodic directions: 4-8 equal 2, 3, 1, 2, 3.
-constexpr int kMomQ = 9;
+constexpr int kMomQ = 10;  // 9: the centroid spacing xm(f) - xm(f-1) itself (cfg%dxm)
 void momentum_metrics(const double *x, int n, bool walls, std::vector<double> (&m)[kMomQ]) {
     std::vector<double> xe(n + 5), xm(n + 4);  // nodes -2..n+2, cells -2..n+1 at index +2
     for (int i = 0; i <= n; i++) xe[i + 2] = x[i];
@@ -367,6 +367,7 @@ void momentum_metrics(const double *x, int n, bool walls, std::vector<double> (&
         const double dmi = 1.0 / (xm[f + 2] - xm[f + 1]);
         const double itm = dmi * (xm[f + 2] - xe[f + 2]), itz = dmi * (xe[f + 2] - xm[f + 1]);
         m[1][f] = dmi;
+        m[9][f] = xm[f + 2] - xm[f + 1];
         m[2][f] = m[4][f] = m[7][f] = itm;
         m[3][f] = m[5][f] = m[8][f] = itz;
         m[6][f] = dmi;
@@ -383,11 +384,23 @@ void momentum_metrics(const double *x, int n, bool walls, std::vector<double> (&
 
 struct MomM {
     const double *di[3], *dmi[3], *itm[3], *itz[3];
-    const double *vtm[3], *vtz[3], *gdm[3], *wtm[3], *wtz[3];
+    const double *vtm[3], *vtz[3], *gdm[3], *wtm[3], *wtz[3], *dm[3];
     int nf[3];    // faces per direction minus one (n)
     int walls[3]; // walls at both ends (non-periodic direction)
     // a face of the component normal to direction d lies on a wall
     __device__ __forceinline__ bool wall_face(int d, int f) const { return walls[d] && (f == 0 || f == nf[d]); }
+    // umask/vmask/wmask > 0 at padded indices (i, j, k) of component c: a
+    // wall or overlap face of its own direction, or a wall-cell row of another
+    __device__ __forceinline__ bool masked(int c, int i, int j, int k) const {
+        const int f[3] = {i, j, k};
+        bool m = false;
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            if (!walls[d]) continue;
+            m = m || (d == c ? (f[d] <= 0 || f[d] >= nf[d]) : (f[d] < 0 || f[d] >= nf[d]));
+        }
+        return m;
+    }
     // interpolation weights and gradient coefficients (-g, +g) along d at face f
     // of a component whose own face is a wall face (cw: both values masked,
     // interpolation unchanged, gradient zero) or not
@@ -695,6 +708,86 @@ __global__ void __launch_bounds__(kThreads) k_implicit_opr(Pad P, MomM M, const 
     }
 }
 
+// The explicit residual of a sub-iteration before an implicit solve (the
+// channel example, simulation.f90:290-301): res = -2*(rho*U - rho*Uold) +
+// dt*res, then, for the components in fmask, res = (res + fa) - fb where the
+// face is not masked; whole padded arrays.
+__global__ void __launch_bounds__(kThreads) k_mom_residual(Pad P, MomM M, double dt, double rho, CVel3 U, CVel3 Uo,
+                                                           Vel3 R, int fmask, double a0, double b0, double a1,
+                                                           double b1, double a2, double b2) {
+    const long long ex = P.nx + 2LL * P.g, ey = P.ny + 2LL * P.g, ez = P.nz + 2LL * P.g, n = ex * ey * ez;
+    const double fa[3] = {a0, a1, a2}, fb[3] = {b0, b1, b2};
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % ex) - P.g;
+        const long long r = t / ex;
+        const int j = (int)(r % ey) - P.g, k = (int)(r / ey) - P.g;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            double v = pa(pm(-2.0, __dsub_rn(pm(rho, U.a[c][t]), pm(rho, Uo.a[c][t]))), pm(dt, R.a[c][t]));
+            if (((fmask >> c) & 1) && !M.masked(c, i, j, k)) v = __dsub_rn(pa(v, fa[c]), fb[c]);
+            R.a[c][t] = v;
+        }
+    }
+}
+
+// U = 2*U - Uold + res after the implicit solve (simulation.f90:319-321)
+__global__ void __launch_bounds__(kThreads) k_apply_residual(long long n, Vel3 U, CVel3 Uo, CVel3 R) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) U.a[c][t] = pa(__dsub_rn(pm(2.0, U.a[c][t]), Uo.a[c][t]), R.a[c][t]);
+    }
+}
+
+// Bulk velocities of the channel forcing (simulation.f90:280-298): per
+// component c, sums over the unmasked interior faces of w*(2*U - Uold) and
+// of w, with w = dxm(i)*dy(j)*dz(k) for U (dx*dym*dz for V, dx*dy*dzm for W);
+// block partials in part[q*kRedBlocks + b], q = 2c (sum) and 2c+1 (volume).
+constexpr int kBulk = 6;
+__global__ void __launch_bounds__(kThreads) k_bulk(Pad P, Metrics Mp, MomM M, CVel3 U, CVel3 Uo,
+                                                   double *__restrict__ part) {
+    __shared__ double sh[kBulk][kThreads];
+    double acc[kBulk];
+#pragma unroll
+    for (int q = 0; q < kBulk; q++) acc[q] = 0.0;
+    const long long n = (long long)P.nx * P.ny * P.nz;
+    const double *cellw[3] = {Mp.dx, Mp.dy, Mp.dz};
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        cell_of(P, t, i, j, k);
+        const long long e = P.at(i, j, k);
+        const int f[3] = {i, j, k};
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            if (M.masked(c, i, j, k)) continue;
+            const double w0 = c == 0 ? M.dm[0][f[0]] : cellw[0][f[0]];
+            const double w1 = c == 1 ? M.dm[1][f[1]] : cellw[1][f[1]];
+            const double w2 = c == 2 ? M.dm[2][f[2]] : cellw[2][f[2]];
+            const double w = pm(pm(w0, w1), w2);
+            acc[2 * c] = pa(acc[2 * c], pm(w, __dsub_rn(pm(2.0, U.a[c][e]), Uo.a[c][e])));
+            acc[2 * c + 1] = pa(acc[2 * c + 1], w);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < kBulk; q++) sh[q][threadIdx.x] = acc[q];
+    __syncthreads();
+    for (int h = kThreads / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) {
+#pragma unroll
+            for (int q = 0; q < kBulk; q++) sh[q][threadIdx.x] = pa(sh[q][threadIdx.x], sh[q][threadIdx.x + h]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < kBulk) part[threadIdx.x * kRedBlocks + blockIdx.x] = sh[threadIdx.x][0];
+}
+
+__global__ void __launch_bounds__(kBulk * 32) k_bulk_final(double *__restrict__ part) {
+    const int q = threadIdx.x / 32, l = threadIdx.x % 32;
+    double s = 0.0;
+    for (int b = l; b < kRedBlocks; b += 32) s = pa(s, part[q * kRedBlocks + b]);
+    for (int o = 16; o > 0; o >>= 1) s = pa(s, __shfl_down_sync(0xffffffffu, s, o));
+    if (l == 0) part[kBulk * kRedBlocks + q] = s;
+}
+
 // Flow statistics, block partials over the interior cells (fixed grid, fixed
 // per-thread order): q 0-2 max|U|*dxmi (get_cfl, incomp_class.f90:1497-1540),
 // 3-5 max 4*visc*dxi**2/rho, 6 sum 0.5*(Ui**2+Vi**2+Wi**2) with the
@@ -973,6 +1066,7 @@ MomM momentum_of(const nga_proj *p) {
         M.gdm[a] = p->mom[a][6];
         M.wtm[a] = p->mom[a][7];
         M.wtz[a] = p->mom[a][8];
+        M.dm[a] = p->mom[a][9];
         M.nf[a] = nn[a];
         M.walls[a] = per[a] ? 0 : 1;
     }
@@ -1092,6 +1186,76 @@ extern "C" int nga_proj_implicit_operator(nga_proj *p, int comp, double dt, doub
     else
         k_implicit_opr<2><<<grid_cells(n), kThreads, 0, p->stream>>>(P, M, U, V, W, visc, visc0, rho, dt, opr);
     PCU(cudaGetLastError());
+    return BBMG_OK;
+}
+
+extern "C" int nga_proj_mom_residual(nga_proj *p, double dt, double rho, const double *U, const double *V,
+                                     const double *W, const double *Uold, const double *Vold, const double *Wold,
+                                     double *resU, double *resV, double *resW, int force_mask, const double *force) {
+    if (!p) return pfail(BBMG_BAD_ARGS, "null projection handle");
+    PCHK(check_dev(U, "U"));
+    PCHK(check_dev(V, "V"));
+    PCHK(check_dev(W, "W"));
+    PCHK(check_dev(Uold, "Uold"));
+    PCHK(check_dev(Vold, "Vold"));
+    PCHK(check_dev(Wold, "Wold"));
+    PCHK(check_dev(resU, "resU"));
+    PCHK(check_dev(resV, "resV"));
+    PCHK(check_dev(resW, "resW"));
+    if (force_mask & ~7) return pfail(BBMG_BAD_ARGS, "force_mask holds bits 1 (U), 2 (V), 4 (W) only");
+    if (force_mask && !force) return pfail(BBMG_BAD_ARGS, "force is NULL");
+    PCU(cudaSetDevice(p->device));
+    double f[6] = {0, 0, 0, 0, 0, 0};
+    if (force_mask)
+        for (int q = 0; q < 6; q++) f[q] = force[q];
+    const long long n = padded_size(p->g);
+    k_mom_residual<<<grid_cells(n), kThreads, 0, p->stream>>>(pad_of(p->g), momentum_of(p), dt, rho,
+                                                              CVel3{{U, V, W}}, CVel3{{Uold, Vold, Wold}},
+                                                              Vel3{{resU, resV, resW}}, force_mask, f[0], f[1], f[2],
+                                                              f[3], f[4], f[5]);
+    PCU(cudaGetLastError());
+    return BBMG_OK;
+}
+
+extern "C" int nga_proj_apply_residual(nga_proj *p, double *U, double *V, double *W, const double *Uold,
+                                       const double *Vold, const double *Wold, const double *resU,
+                                       const double *resV, const double *resW) {
+    if (!p) return pfail(BBMG_BAD_ARGS, "null projection handle");
+    PCHK(check_dev(U, "U"));
+    PCHK(check_dev(V, "V"));
+    PCHK(check_dev(W, "W"));
+    PCHK(check_dev(Uold, "Uold"));
+    PCHK(check_dev(Vold, "Vold"));
+    PCHK(check_dev(Wold, "Wold"));
+    PCHK(check_dev(resU, "resU"));
+    PCHK(check_dev(resV, "resV"));
+    PCHK(check_dev(resW, "resW"));
+    PCU(cudaSetDevice(p->device));
+    const long long n = padded_size(p->g);
+    k_apply_residual<<<grid_cells(n), kThreads, 0, p->stream>>>(n, Vel3{{U, V, W}}, CVel3{{Uold, Vold, Wold}},
+                                                                CVel3{{resU, resV, resW}});
+    PCU(cudaGetLastError());
+    return BBMG_OK;
+}
+
+extern "C" int nga_proj_bulk(nga_proj *p, const double *U, const double *V, const double *W, const double *Uold,
+                             const double *Vold, const double *Wold, double *out) {
+    if (!p) return pfail(BBMG_BAD_ARGS, "null projection handle");
+    if (!out) return pfail(BBMG_BAD_ARGS, "out is NULL");
+    PCHK(check_dev(U, "U"));
+    PCHK(check_dev(V, "V"));
+    PCHK(check_dev(W, "W"));
+    PCHK(check_dev(Uold, "Uold"));
+    PCHK(check_dev(Vold, "Vold"));
+    PCHK(check_dev(Wold, "Wold"));
+    PCU(cudaSetDevice(p->device));
+    k_bulk<<<kRedBlocks, kThreads, 0, p->stream>>>(pad_of(p->g), metrics_of(p), momentum_of(p), CVel3{{U, V, W}},
+                                                   CVel3{{Uold, Vold, Wold}}, p->part);
+    PCU(cudaGetLastError());
+    k_bulk_final<<<1, kBulk * 32, 0, p->stream>>>(p->part);
+    PCU(cudaGetLastError());
+    PCU(cudaMemcpyAsync(out, p->part + kBulk * kRedBlocks, kBulk * sizeof(double), cudaMemcpyDefault, p->stream));
+    PCU(cudaStreamSynchronize(p->stream));
     return BBMG_OK;
 }
 

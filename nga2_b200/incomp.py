@@ -258,3 +258,96 @@ class HIT:
 
     def close(self):
         self.fs.close()
+
+
+def _face_mask(shape, g, ns, per, c):
+    """umask (c = 0), vmask (1), wmask (2) > 0 on a padded array [k, j, i] for
+    walls at both ends of every non-periodic direction (incomp_class.f90:
+    196-242 with cfg%VF = 0 outside the domain)."""
+    m = np.zeros(shape, bool)
+    for d in range(3):
+        if per[d]:
+            continue
+        idx = np.arange(-g, ns[d] + g)
+        md = ((idx <= 0) | (idx >= ns[d])) if d == c else ((idx < 0) | (idx >= ns[d]))
+        m |= md[None, None, :] if d == 0 else (md[None, :, None] if d == 1 else md[:, None, None])
+    return m
+
+
+def _centres(x, g):
+    """Cell centres of the padded cells -g .. n+g-1 (the naive node extension)."""
+    n = x.size - 1
+    xe = np.empty(n + 1 + 2 * g)
+    xe[g:g + n + 1] = x
+    for m in range(g - 1, -1, -1):
+        xe[m] = xe[m + 1] - (xe[g + 1] - xe[g])
+    for m in range(g + n + 1, n + 1 + 2 * g):
+        xe[m] = xe[m - 1] + (xe[g + n] - xe[g + n - 1])
+    return 0.5 * (xe[:-1] + xe[1:])
+
+
+class Channel:
+    """The channel example (examples/channel/src/simulation.f90) on the GPU:
+    x and z periodic, walls in y on the tanh-stretched grid of its
+    geometry.f90 (lines 30-61), velocity initialised to the bulk values with
+    the optional cosine perturbation (lines 147-167), then the time loop
+    (lines 256-340): dt from the CFL, ``itmax`` sub-iterations of mid-point
+    velocity, get_dmomdt, explicit residual with the bulk-velocity forcing of
+    U and W, solve_implicit (three non-symmetric 7-point solves by bbmg
+    multigrid), U = 2U - Uold + res and a pressure projection.  Defaults are
+    the example's input file, with nz > 1 (the file's nz = 1 needs
+    adjust_metrics' lower-dimension zeroing, which is not restated)."""
+
+    def __init__(self, nx=128, ny=40, nz=8, Lx=5.0, Ly=1.0, Lz=0.04, stretch=2.1, visc=0.01, rho=1.0, Ubulk=1.0,
+                 Wbulk=0.0, amp=0.0, dtmax=2e-2, cflmax=0.9, itmax=2, ghost=1, precision=B.FP64, rcvg=1e-10,
+                 maxit=100, implicit_rcvg=1e-6, implicit_maxit=100, device=0):
+        import torch
+        x = np.arange(nx + 1, dtype=np.float64) / float(nx) * Lx
+        j = np.arange(ny + 1, dtype=np.float64)
+        y = 0.5 * Ly * np.tanh(stretch * (2.0 * j / float(ny) - 1.0)) / np.tanh(stretch)
+        z = np.arange(nz + 1, dtype=np.float64) / float(nz) * Lz - 0.5 * Lz
+        per = (True, False, True)
+        self.fs = fs = Incomp(x, y, z, rho=rho, visc=visc, ghost=ghost, precision=precision, rcvg=rcvg, maxit=maxit,
+                              device=device, per=per, implicit_rcvg=implicit_rcvg, implicit_maxit=implicit_maxit)
+        self.time = TimeTracker(dtmax, cflmax, itmax)
+        self.Ubulk, self.Wbulk = float(Ubulk), float(Wbulk)
+        g, ns = ghost, (nx, ny, nz)
+        vel = np.sqrt(Ubulk ** 2 + Wbulk ** 2)
+        zm = _centres(z, g)[:, None, None]
+        xm = _centres(x, g)[None, None, :]
+        one = np.ones(fs.shape)
+        um, wm = _face_mask(fs.shape, g, ns, per, 0), _face_mask(fs.shape, g, ns, per, 2)
+        U = np.where(um, 0.0, Ubulk * one)
+        U = np.where(um, U, U + amp * vel * np.cos(8.0 * 2.0 * np.pi * zm / Lz))
+        W = np.where(wm, 0.0, Wbulk * one)
+        W = np.where(wm, W, W + amp * vel * np.cos(8.0 * 2.0 * np.pi * xm / Lx))
+        fs.U.copy_(torch.from_numpy(U))
+        fs.W.copy_(torch.from_numpy(W))
+        self.meanU, self.meanW = self.Ubulk, self.Wbulk
+
+    def step(self):
+        """One time step; returns the pressure solves' PCG iterations."""
+        fs, time = self.fs, self.time
+        _, time.cfl = fs.get_cfl(time.dt)
+        time.adjust_dt()
+        time.increment()
+        for a, b in ((fs.Uold, fs.U), (fs.Vold, fs.V), (fs.Wold, fs.W)):
+            a.copy_(b)
+        its = []
+        while time.it <= time.itmax:
+            fs.proj.midpoint(fs.U, fs.V, fs.W, fs.Uold, fs.Vold, fs.Wold)
+            fs.get_dmomdt()
+            (su, vu), _, (sw, vw) = fs.proj.bulk(fs.U, fs.V, fs.W, fs.Uold, fs.Vold, fs.Wold)
+            self.meanU, self.meanW = su / vu, sw / vw
+            fs.proj.mom_residual(time.dt, fs.rho, fs.U, fs.V, fs.W, fs.Uold, fs.Vold, fs.Wold, fs.resU, fs.resV,
+                                 fs.resW, force={0: (self.Ubulk, self.meanU), 2: (self.Wbulk, self.meanW)})
+            fs.solve_implicit(time.dt)
+            fs.proj.apply_residual(fs.U, fs.V, fs.W, fs.Uold, fs.Vold, fs.Wold, fs.resU, fs.resV, fs.resW)
+            it, rerr, st = fs.pressure_projection(time.dt)
+            its.append(it)
+            time.it += 1
+        fs.get_div()
+        return its
+
+    def close(self):
+        self.fs.close()

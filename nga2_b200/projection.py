@@ -14,7 +14,8 @@ from . import bbmg as B
 
 EXPORTS = ["nga_proj_create", "nga_proj_destroy", "nga_proj_set_stream", "nga_proj_laplacian",
            "nga_proj_divergence", "nga_proj_shift_p", "nga_proj_pgrad", "nga_proj_correct", "nga_proj_dmomdt",
-           "nga_proj_midpoint", "nga_proj_advance", "nga_proj_flow_stats", "nga_proj_implicit_operator"]
+           "nga_proj_midpoint", "nga_proj_advance", "nga_proj_flow_stats", "nga_proj_implicit_operator",
+           "nga_proj_mom_residual", "nga_proj_apply_residual", "nga_proj_bulk"]
 
 _BOUND = False
 
@@ -38,6 +39,9 @@ def lib():
         L.nga_proj_advance.argtypes = [P, D, D, P, P, P, P, P, P, P, P, P, D, D, DP]
         L.nga_proj_flow_stats.argtypes = [P, P, P, P, P, D, D, D, DP]
         L.nga_proj_implicit_operator.argtypes = [P, I, D, D, P, P, P, P, D, P]
+        L.nga_proj_mom_residual.argtypes = [P, D, D, P, P, P, P, P, P, P, P, P, I, DP]
+        L.nga_proj_apply_residual.argtypes = [P, P, P, P, P, P, P, P, P, P]
+        L.nga_proj_bulk.argtypes = [P, P, P, P, P, P, P, DP]
         for n in EXPORTS:
             getattr(L, n).restype = C.c_int
         _BOUND = True
@@ -143,6 +147,28 @@ class Projection:
         self._check(self.lib.nga_proj_implicit_operator(self.h, int(comp), float(dt), float(rho), _p(U), _p(V),
                                                         _p(W), _p(visc), float(visc0), _p(opr)))
         return opr
+
+    def mom_residual(self, dt, rho, U, V, W, Uold, Vold, Wold, resU, resV, resW, force=None):
+        """res = -2(rho U - rho Uold) + dt res in place; force maps a component
+        (0, 1, 2) to (a, b): res = (res + a) - b on its unmasked faces."""
+        f = (C.c_double * 6)()
+        mask = 0
+        for c, (a, b) in (force or {}).items():
+            f[2 * c], f[2 * c + 1] = float(a), float(b)
+            mask |= 1 << c
+        self._check(self.lib.nga_proj_mom_residual(self.h, float(dt), float(rho), _p(U), _p(V), _p(W), _p(Uold),
+                                                   _p(Vold), _p(Wold), _p(resU), _p(resV), _p(resW), mask, f))
+
+    def apply_residual(self, U, V, W, Uold, Vold, Wold, resU, resV, resW):
+        """U = 2U - Uold + resU, V and W likewise, in place."""
+        self._check(self.lib.nga_proj_apply_residual(self.h, _p(U), _p(V), _p(W), _p(Uold), _p(Vold), _p(Wold),
+                                                     _p(resU), _p(resV), _p(resW)))
+
+    def bulk(self, U, V, W, Uold, Vold, Wold):
+        """[(sum w (2U - Uold), sum w) for U, V, W] over the unmasked faces."""
+        out = (C.c_double * 6)()
+        self._check(self.lib.nga_proj_bulk(self.h, _p(U), _p(V), _p(W), _p(Uold), _p(Vold), _p(Wold), out))
+        return [(out[2 * c], out[2 * c + 1]) for c in range(3)]
 
     def close(self):
         if self.h:

@@ -218,7 +218,8 @@ def momentum_metrics(x, walls=False):
         vtm[n], vtz[n], gdm[n] = 0.0, 1.0, 1.0 / (xe[n + 2] - xm[n + 1])      # delta = x(n) - xm(n-1)
         wtm[0] = 0.0                                                          # cell -1 is wall
         wtz[n] = 0.0                                                          # cell n is wall
-    return dxi, dxmi, itm, itz, vtm, vtz, gdm, wtm, wtz
+    dm = xm[f + 2] - xm[f + 1]        # cfg%dxm on faces 0 .. n
+    return dxi, dxmi, itm, itz, vtm, vtz, gdm, wtm, wtz, dm
 
 
 def dmomdt(G, U, V, W, P, rho, visc):
@@ -564,3 +565,132 @@ def implicit_operator(G, comp, dt, rho, U, V, W, visc):
     out[..., 0] = np.where(wf, rho, out[..., 0])
     out[..., 1:] = np.where(wf[..., None], 0.0, out[..., 1:])
     return out
+
+
+def extended_centres(x, g):
+    """Cell centres xm of padded cells -g .. n+g-1 (the naive node extension)."""
+    x = np.asarray(x, np.float64)
+    n = x.size - 1
+    xe = np.empty(n + 1 + 2 * g)
+    xe[g:g + n + 1] = x
+    for m in range(g - 1, -1, -1):
+        xe[m] = xe[m + 1] - (xe[g + 1] - xe[g])
+    for m in range(g + n + 1, n + 1 + 2 * g):
+        xe[m] = xe[m - 1] + (xe[g + n] - xe[g + n - 1])
+    return 0.5 * (xe[:-1] + xe[1:])
+
+
+def face_mask(G, c):
+    """umask (c = 0), vmask (1), wmask (2) > 0 on the padded array for walls
+    at both ends of every non-periodic direction (incomp_class.f90:196-242
+    with cfg%VF = 0 outside the domain)."""
+    g, ns = G.g, (G.nx, G.ny, G.nz)
+    m = np.zeros(G.padded, bool)
+    for d in range(3):
+        if G.per[d]:
+            continue
+        idx = np.arange(-g, ns[d] + g)
+        md = ((idx <= 0) | (idx >= ns[d])) if d == c else ((idx < 0) | (idx >= ns[d]))
+        m |= md[None, None, :] if d == 0 else (md[None, :, None] if d == 1 else md[:, None, None])
+    return m
+
+
+def mom_residual(G, c, dt, rho, U, Uold, res, force=None):
+    """resU = -2*(rho*U - rho*Uold) + dt*resU, then (resU + a) - b where umask
+    is 0 for force = (a, b) (examples/channel/src/simulation.f90:290-301)."""
+    r = -2.0 * (rho * U - rho * Uold) + dt * res
+    if force is not None:
+        r = np.where(face_mask(G, c), r, (r + force[0]) - force[1])
+    return r
+
+
+def apply_residual(U, Uold, res):
+    """U = 2*U - Uold + resU (examples/channel/src/simulation.f90:319-321)."""
+    return (2.0 * U - Uold) + res
+
+
+def bulk(G, c, U, Uold):
+    """The channel forcing's sums (examples/channel/src/simulation.f90:
+    280-298) for component c: sum over the interior faces with mask 0 of
+    w*(2*U - Uold) and of w, w = dxm*dy*dz for U (dx*dym*dz, dx*dy*dzm)."""
+    ns = (G.nx, G.ny, G.nz)
+    w = None
+    for d, xn in enumerate((G.xn, G.yn, G.zn)):
+        v = momentum_metrics(xn, not G.per[d])[9][:ns[d]] if d == c else np.diff(np.asarray(xn, np.float64))
+        v = v[None, None, :] if d == 0 else (v[None, :, None] if d == 1 else v[:, None, None])
+        w = v if w is None else w * v
+    w = np.broadcast_to(w, (G.nz, G.ny, G.nx))
+    keep = ~G.interior(face_mask(G, c))
+    return (w * (2.0 * G.interior(U) - G.interior(Uold)))[keep].sum(), w[keep].sum()
+
+
+class ChannelOracle:
+    """examples/channel/src/simulation.f90 on the CPU (initial field lines
+    147-167, time loop 256-340) on its geometry (geometry.f90:30-61: x and z
+    periodic, tanh-stretched y between walls), with solves
+    ``solve_p(opr, rhs)`` (pressure) and ``solve_v(opr, rhs)`` (implicit
+    velocity) on interior arrays."""
+
+    def __init__(self, nx, ny, nz, solve_p, solve_v, Lx=5.0, Ly=1.0, Lz=0.04, stretch=2.1, visc=0.01, rho=1.0,
+                 Ubulk=1.0, Wbulk=0.0, amp=0.0, dtmax=2e-2, cflmax=0.9, itmax=2, g=1):
+        x = np.arange(nx + 1, dtype=np.float64) / float(nx) * Lx
+        j = np.arange(ny + 1, dtype=np.float64)
+        y = 0.5 * Ly * np.tanh(stretch * (2.0 * j / float(ny) - 1.0)) / np.tanh(stretch)
+        z = np.arange(nz + 1, dtype=np.float64) / float(nz) * Lz - 0.5 * Lz
+        self.G = G = Grid(x, y, z, (True, False, True), g)
+        self.solve_p, self.solve_v = solve_p, solve_v
+        self.rho, self.Ubulk, self.Wbulk = float(rho), float(Ubulk), float(Wbulk)
+        self.visc = np.full(G.padded, float(visc))
+        self.rho_face = np.full(G.padded, self.rho)
+        self.opr = laplacian(G)
+        self.dtmax, self.cflmax, self.itmax = dtmax, cflmax, itmax
+        self.dt, self.t, self.n = dtmax, 0.0, 0
+        vel = np.sqrt(Ubulk ** 2 + Wbulk ** 2)
+        zm = extended_centres(z, g)[:, None, None]
+        xm = extended_centres(x, g)[None, None, :]
+        one = np.ones(G.padded)
+        self.U = np.where(face_mask(G, 0), 0.0, Ubulk * one)
+        self.U = np.where(face_mask(G, 0), self.U, self.U + amp * vel * np.cos(8.0 * 2.0 * np.pi * zm / Lz))
+        self.V = np.zeros(G.padded)
+        self.W = np.where(face_mask(G, 2), 0.0, Wbulk * one)
+        self.W = np.where(face_mask(G, 2), self.W, self.W + amp * vel * np.cos(8.0 * 2.0 * np.pi * xm / Lx))
+        self.P = np.zeros(G.padded)
+
+    def _fill(self, inner):
+        a = np.zeros(self.G.padded)
+        self.G.interior(a)[...] = inner
+        return self.G.sync(a)
+
+    def step(self):
+        G = self.G
+        s = flow_stats(G, self.U, self.V, self.W, self.visc, self.rho, self.dt)
+        cfl = s[:6].max()
+        dtold = self.dt
+        if cfl > 0.0:
+            self.dt = min(dtold * self.cflmax / cfl, self.dtmax)
+        if self.dt > dtold:
+            self.dt = 0.7 * self.dt + (1.0 - 0.7) * dtold
+        self.t += self.dt
+        self.n += 1
+        dt, rho = self.dt, self.rho
+        Uo, Vo, Wo = self.U.copy(), self.V.copy(), self.W.copy()
+        for _ in range(self.itmax):
+            self.U, self.V, self.W = midpoint(self.U, Uo), midpoint(self.V, Vo), midpoint(self.W, Wo)
+            dU, dV, dW = dmomdt(G, self.U, self.V, self.W, self.P, rho, self.visc)
+            su, vu = bulk(G, 0, self.U, Uo)
+            sw, vw = bulk(G, 2, self.W, Wo)
+            res = [mom_residual(G, 0, dt, rho, self.U, Uo, dU, (self.Ubulk, su / vu)),
+                   mom_residual(G, 1, dt, rho, self.V, Vo, dV),
+                   mom_residual(G, 2, dt, rho, self.W, Wo, dW, (self.Wbulk, sw / vw))]
+            for c in range(3):   # solve_implicit
+                A = implicit_operator(G, c, dt, rho, self.U, self.V, self.W, self.visc)
+                res[c] = self._fill(self.solve_v(A, np.ascontiguousarray(G.interior(res[c]))))
+            self.U = apply_residual(self.U, Uo, res[0])
+            self.V = apply_residual(self.V, Vo, res[1])
+            self.W = apply_residual(self.W, Wo, res[2])
+            _, rhs = divergence(G, self.U, self.V, self.W, rho=rho, dt=dt)
+            sol = self._fill(self.solve_p(np.ascontiguousarray(G.interior(self.opr)),
+                                          np.ascontiguousarray(G.interior(rhs))))
+            sol, _ = shift_p(G, sol)
+            self.U, self.V, self.W, self.P = correct(G, sol, dt, self.U, self.V, self.W, self.P, self.rho_face,
+                                                     self.rho_face, self.rho_face)

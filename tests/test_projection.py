@@ -34,7 +34,7 @@ def test_library_exports_every_projection_symbol():
     from nga2_b200 import projection as PR
     lib = B.load()
     names = header_functions()
-    assert len(names) == 13
+    assert len(names) == 16
     for n in names:
         assert hasattr(lib, n), n
     assert sorted(PR.EXPORTS) == names
