@@ -1,14 +1,17 @@
-"""The projection steps around the pressure solve (include/nga_projection.h):
-operator assembly, divergence and right-hand side, shift_p, get_pgrad and
-the velocity correction.
+"""The steps of the time loop around the pressure solve (include/nga_projection.h):
+operator assembly, divergence and right-hand side, shift_p, get_pgrad, the
+velocity correction, get_dmomdt and solve_implicit's operator.
 
 CPU: the library exports every declared symbol; the numpy oracle
 (oracle/projection_oracle.py) agrees with the problem generators' operator and
-divergence, and a whole projection through the oracle leaves a
-divergence-free velocity.  GPU: every kernel equals the oracle bit for bit
-(shift_p's mean to round-off), and a projection chained entirely on the
-device (assembly -> setup -> divergence -> solve -> shift -> correction) leaves
-a divergence-free velocity.
+divergence, a whole projection through the oracle leaves a divergence-free
+velocity, its get_dmomdt converges at second order on a Taylor-Green field and
+gives the one-sided wall values on a Poiseuille profile, and its implicit
+operator equals rho - dt/2 (viscous get_dmomdt) and the linearised convective
+get_dmomdt to round-off.  GPU: every kernel equals the oracle bit for bit
+(shift_p's mean to round-off), periodic and with walls, and a projection
+chained entirely on the device (assembly -> setup -> divergence -> solve ->
+shift -> correction) leaves a divergence-free velocity.
 """
 import math
 import os
