@@ -1,24 +1,32 @@
-"""Constant-density incompressible flow on the GPU, triply periodic pgrids.
+"""Constant-density incompressible flow on the GPU.
 
 The device counterpart of NGA2's ``incomp`` solver
-(src/constant_density/incomp_class.f90) for the calls that the homogeneous
-isotropic turbulence example makes in its time loop
-(examples/hit/src/simulation.f90:256-352), with the pressure Poisson equation
-solved by this package's bbmg (pcg_bbox) in place of the example's FFT
-solver.  Every field operation runs as a kernel of the projection library
+(src/constant_density/incomp_class.f90) for the calls that its examples make
+in their time loops -- the forced homogeneous turbulence example
+(examples/hit/src/simulation.f90:256-352, triply periodic, explicit
+sub-iterations) and the channel example (examples/channel/src/simulation.f90:
+256-340, walls in y, implicit viscous solves) -- with the pressure Poisson
+equation and the implicit velocity systems solved by this package's bbmg.
+Every field operation runs as a kernel of the projection library
 (include/nga_projection.h):
 
 * ``get_dmomdt``                           -> nga_proj_dmomdt
 * ``U = 0.5*(U + Uold)``                   -> nga_proj_midpoint
 * residual, linear forcing, ``U = 2U - Uold + res/rho`` -> nga_proj_advance
+* residual with bulk forcing, ``U = 2U - Uold + res``
+                                           -> nga_proj_mom_residual, nga_proj_apply_residual
+* ``solve_implicit``                       -> nga_proj_implicit_operator + bbmg (BBMG_BBOX)
 * ``get_cfl``, interp_vel's kinetic energy, ``cfg%integrate`` means
                                            -> nga_proj_flow_stats
+* the channel's bulk velocities            -> nga_proj_bulk
 * ``get_div`` and ``rhs = -vol*div*rho/dt`` -> nga_proj_divergence
 * ``shift_p``                              -> nga_proj_shift_p
 * ``get_pgrad``, ``P += sol``, ``U -= dt*grad/rho`` -> nga_proj_correct
 
 Fields are CUDA float64 tensors in NGA2's padded layout [k, j, i] with
-``ghost`` overlap layers holding the periodic images.  There is no CPU path.
+``ghost`` overlap layers; periodic overlaps hold the periodic images, walls
+(non-periodic directions) keep the no-slip value 0 in their cells and faces.
+There is no CPU path.
 """
 from __future__ import annotations
 
