@@ -632,7 +632,8 @@ class ChannelOracle:
     velocity) on interior arrays."""
 
     def __init__(self, nx, ny, nz, solve_p, solve_v, Lx=5.0, Ly=1.0, Lz=0.04, stretch=2.1, visc=0.01, rho=1.0,
-                 Ubulk=1.0, Wbulk=0.0, amp=0.0, dtmax=2e-2, cflmax=0.9, itmax=2, g=1):
+                 Ubulk=1.0, Wbulk=0.0, amp=0.0, dtmax=2e-2, cflmax=0.9, itmax=2, g=1, forcing=True):
+        self.forcing = forcing
         x = np.arange(nx + 1, dtype=np.float64) / float(nx) * Lx
         j = np.arange(ny + 1, dtype=np.float64)
         y = 0.5 * Ly * np.tanh(stretch * (2.0 * j / float(ny) - 1.0)) / np.tanh(stretch)
@@ -679,9 +680,11 @@ class ChannelOracle:
             dU, dV, dW = dmomdt(G, self.U, self.V, self.W, self.P, rho, self.visc)
             su, vu = bulk(G, 0, self.U, Uo)
             sw, vw = bulk(G, 2, self.W, Wo)
-            res = [mom_residual(G, 0, dt, rho, self.U, Uo, dU, (self.Ubulk, su / vu)),
+            fu = (self.Ubulk, su / vu) if self.forcing else None
+            fw = (self.Wbulk, sw / vw) if self.forcing else None
+            res = [mom_residual(G, 0, dt, rho, self.U, Uo, dU, fu),
                    mom_residual(G, 1, dt, rho, self.V, Vo, dV),
-                   mom_residual(G, 2, dt, rho, self.W, Wo, dW, (self.Wbulk, sw / vw))]
+                   mom_residual(G, 2, dt, rho, self.W, Wo, dW, fw)]
             for c in range(3):   # solve_implicit
                 A = implicit_operator(G, c, dt, rho, self.U, self.V, self.W, self.visc)
                 res[c] = self._fill(self.solve_v(A, np.ascontiguousarray(G.interior(res[c]))))

@@ -276,3 +276,26 @@ def test_residual_update_and_bulk_kernels():
         assert abs(got[c][0] - s_ref) <= 1e-12 * np.abs(2.0 * U[c] - Uo[c]).max() * v_ref
     pr.close()
 
+
+
+def test_oracle_channel_forcing_holds_the_bulk_velocity():
+    """The bulk forcing of the channel loop: from a uniform start the wall
+    friction slows the flow; the forced run keeps its bulk velocity nearer
+    Ubulk than the same loop without the forcing."""
+    from oracle.oracle import OracleBBMG, BBOX
+    nx, ny, nz = 8, 10, 4
+    ov = OracleBBMG(nx, ny, nz, True, False, True, method=BBOX, rcvg=1e-12, maxit=200)
+
+    def solve_v(opr, rhs):
+        ov.setup(P.STC7, np.ascontiguousarray(opr))
+        return ov.solve(rhs)[0]
+    runs = [PO.ChannelOracle(nx, ny, nz, oracle_solver_walls(nx, ny, nz), solve_v, Lz=0.5, visc=0.05, forcing=f)
+            for f in (True, False)]
+    for _ in range(4):
+        for ch in runs:
+            ch.step()
+    G = runs[0].G
+    bulk = [PO.bulk(G, 0, ch.U, ch.U) for ch in runs]
+    mean = [s / v for s, v in bulk]
+    assert mean[1] < mean[0] <= 1.0 + 1e-12
+    assert 1.0 - mean[0] < 0.5 * (1.0 - mean[1])
