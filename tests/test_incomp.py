@@ -1,14 +1,17 @@
-"""The incompressible time loop on the GPU (nga2_b200/incomp.py): the kernels
-of a sub-iteration (nga_proj_midpoint, nga_proj_advance, nga_proj_flow_stats)
-against the numpy oracle, and whole time steps of the turbulence example
-(examples/hit/src/simulation.f90) against the oracle's restatement of the
-same loop.
+"""The incompressible time loops on the GPU (nga2_b200/incomp.py): the kernels
+of a sub-iteration (nga_proj_midpoint, nga_proj_advance, nga_proj_flow_stats,
+nga_proj_mom_residual, nga_proj_apply_residual, nga_proj_bulk) against the
+numpy oracle, and whole time steps of the turbulence example
+(examples/hit/src/simulation.f90) and of the channel example
+(examples/channel/src/simulation.f90, walls and implicit solves) against the
+oracle's restatements of the same loops.
 
-CPU: the oracle loop keeps the velocity divergence-free and its linear
-forcing holds the kinetic energy nearer its initial value than free decay;
-the timetracker's dt rule.  GPU: midpoint and advance bit for bit; the
+CPU: the oracle loops keep the velocity divergence-free, the linear forcing
+holds the turbulence's kinetic energy and the bulk forcing the channel's bulk
+velocity nearer their targets than the unforced loops; the timetracker's dt
+rule.  GPU: midpoint, advance, residual and update bit for bit; the
 statistics' maxima bit for bit and sums to round-off; three time steps of
-the loop to the pressure solver's tolerance.
+each loop to the solvers' tolerance.
 """
 import numpy as np
 import pytest
