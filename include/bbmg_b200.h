@@ -81,7 +81,10 @@ typedef struct {
     int it;                /* iterations of the last solve                   */
     double rerr;           /* reported relative residual (inf-norm ratio)    */
     double res0;           /* initial residual inf-norm                      */
-    double true_rerr;      /* FP64 b - A x inf-norm ratio at exit            */
+    double true_rerr;      /* max|b - A x| / (rerr's denominator), with x the
+                              returned solution and the product recomputed in
+                              FP64 after the last iteration (the reported rerr
+                              of pcg_bbox is the CG recurrence's residual)   */
     double setup_ms;       /* device time of the last setup                  */
     double solve_ms;       /* device time of the last solve                  */
     long long device_bytes;/* device memory held by the handle               */
@@ -91,6 +94,9 @@ typedef struct {
     int fallback_it;       /* mixed precision: iteration after which the solve
                               continued in FP64 because the FP32 V-cycle stopped
                               reducing the residual (0 = never)               */
+    double true_res;       /* max|b - A x| at exit (absolute, FP64)           */
+    double l2_rerr;        /* ||b - A x||_2 / ||r0||_2 at exit, r0 the initial
+                              residual (||rhs||_2 under BBMG_NORM_RHS)        */
 } bbmg_info;
 
 /* Fill `p` with the ILS values: pcg_bbox, FP64, V(2,2), ncell_coarsest 300,
@@ -193,14 +199,18 @@ int bbmg_debug_direct(bbmg_handle *h, double *op, double *lu, int *piv, int *np)
  * out[1] = max|rhs| and out[2] = out[0] / out[1] over the interior of the
  * caller's system, with A the caller's stencil (stc host array int[nst][3],
  * opr in bbmg_setup's layout), overlap cells of non-periodic directions taken
- * as zero and periodic directions wrapped -- the residual bbmg_solve reports.
- * opr, rhs, sol and out (3 doubles) must be device memory.  Nothing is
- * allocated: the only scratch is a static device array of 8192 plane slots
- * that every GPU loading the library holds until exit, so grids with
- * nz > 8192 are rejected with BBMG_BAD_ARGS.  The first call on a device
- * looks up that array's device address (make it before any stream capture).
- * Calls share the array: calls that overlap on the GPU race and must be
- * serialised by the caller.  Errors: bbmg_last_error(NULL).
+ * as zero and periodic directions wrapped.  out[2] is the rerr bbmg_solve
+ * reports for a solve that started from a zero guess (its max|r0| is then
+ * max|rhs|); for a zero rhs out[2] is 0 if the residual is 0, else +inf.
+ * opr, rhs, sol and out (3 doubles) must be memory of the current device.
+ * Nothing is allocated: the only scratch is a static device array of 8192
+ * plane slots that every GPU loading the library holds until exit, so grids
+ * with nz > 8192 are rejected with BBMG_BAD_ARGS.  Each call looks up that
+ * array's address on the current device; under CUDA's lazy module loading the
+ * first call on a device also loads the library's device code there, which can
+ * synchronise the device, so make one warm-up call before a time loop or any
+ * stream capture.  Calls share the array: calls that overlap on the GPU race
+ * and must be serialised by the caller.  Errors: bbmg_last_error(NULL).
  * ---------------------------------------------------------------------- */
 int bbmg_residual_norm_noalloc(const bbmg_grid *grid, int nst, const int *stc, const double *opr,
                                const double *rhs, const double *sol, double *out, void *stream);

@@ -59,7 +59,8 @@ class Info(C.Structure):
                 ("coarse_pinned", C.c_int), ("it", C.c_int), ("rerr", C.c_double), ("res0", C.c_double),
                 ("true_rerr", C.c_double), ("setup_ms", C.c_double), ("solve_ms", C.c_double),
                 ("device_bytes", C.c_longlong), ("status", C.c_int), ("launches", C.c_longlong),
-                ("level1_stencil", C.c_int), ("fallback_it", C.c_int)]
+                ("level1_stencil", C.c_int), ("fallback_it", C.c_int), ("true_res", C.c_double),
+                ("l2_rerr", C.c_double)]
 
 
 _LIB = None

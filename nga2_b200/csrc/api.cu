@@ -23,6 +23,17 @@ using namespace bbmg;
 
 namespace {
 
+// slots of the handle's device scalars (dscal) and their pinned host mirror
+constexpr int kScalRes0 = 0;    // max|r0|
+constexpr int kScalRes = 1;     // max|r| of the last iteration
+constexpr int kScalInfo = 2;    // setup: LU info (an int)
+constexpr int kScalRhs = 3;     // max|rhs|
+constexpr int kScalRes0L2 = 4;  // sum r0^2
+constexpr int kScalRhsL2 = 5;   // sum rhs^2
+constexpr int kScalTrue = 6;    // max|b - A x| at exit
+constexpr int kScalTrueL2 = 7;  // sum (b - A x)^2 at exit
+constexpr int kScalN = 16;
+
 struct Level {
     Lay L;
     NbrOff nb;
@@ -81,8 +92,9 @@ struct bbmg_handle {
     // Krylov / outer iteration vectors (level-1 layout)
     double *sol = nullptr, *pp = nullptr, *pp2 = nullptr, *Ap = nullptr;  // pp/pp2 alternate per iteration
     double *x2 = nullptr;  // second solution buffer of the mixed defect correction (alternates with lv[1].v)
+    double *b1 = nullptr;  // pcg_bbox: the right-hand side (lv[1].f holds the CG residual during the solve)
     CgScal *sc = nullptr;
-    double *part = nullptr, *dscal = nullptr;  // reduction partials; [0]=res0 [1]=res
+    double *part = nullptr, *dscal = nullptr;  // reduction partials; scalars (kScal* slots)
     double *h_scal = nullptr;                  // pinned host mirror of dscal
     // staging for caller arrays
     double *d_opr_in = nullptr;
@@ -266,30 +278,30 @@ int record_iteration(bbmg_handle *h, int mode, int par) {
     case 0:  // FP64 mgsolve: cycle; residual; max|r| (bbmg_class.f90:716-722)
         if ((st = vcycle<double>(h, 1))) return st;
         CU(h, launch_residual<double>(L, l1.nb, l1.npt, l1.oprS, l1.v, l1.f, l1.r, s));
-        CU(h, launch_maxabs<double>(L, l1.r, h->part, h->dscal + 1, s));
+        CU(h, launch_maxabs<double>(L, l1.r, h->part, h->dscal + kScalRes, s));
         break;
     case 1:  // FP64 cgsolve body, v zeroed by the previous step; res lives in l1.f
         if ((st = vcycle<double>(h, 1))) return st;
         CU(h, launch_cg_rho<double>(L, l1.v, l1.f, h->part, h->sc, s));
         CU(h, launch_cg_pap_fused<double>(L, l1.nb, l1.npt, l1.oprS, l1.v, pp_old, pp_new, h->Ap, h->part, h->sc, s));
-        CU(h, launch_cg_xr_fused<double>(L, h->sol, pp_new, l1.f, h->Ap, h->sc, nullptr, l1.v, h->part, h->dscal + 1, s));
+        CU(h, launch_cg_xr_fused<double>(L, h->sol, pp_new, l1.f, h->Ap, h->sc, nullptr, l1.v, h->part, h->dscal + kScalRes, s));
         break;
     case 2: {  // mixed defect correction: e = V32(r); x += e; r = b - A x (FP64); f32/v32 prepared
         double *x_old = par ? h->x2 : l1.v, *x_new = par ? l1.v : h->x2;
         CU(h, cudaMemsetAsync(l1.v32, 0, sizeof(float) * L.plane, s));
         if ((st = vcycle<float>(h, 1))) return st;
         CU(h, launch_defect_fused(L, l1.nb, l1.npt, l1.oprS, x_old, l1.v32, l1.f, x_new, l1.f32, h->part,
-                                  h->dscal + 1, s));
+                                  h->dscal + kScalRes, s));
         break;
     }
     case 3:  // mixed PCG: FP64 Krylov vectors, FP32 V-cycle; f32/v32 prepared by the previous step
         if ((st = vcycle<float>(h, 1))) return st;
         CU(h, launch_cg_rho<float>(L, l1.v32, l1.f, h->part, h->sc, s));
         CU(h, launch_cg_pap_fused<float>(L, l1.nb, l1.npt, l1.oprS, l1.v32, pp_old, pp_new, h->Ap, h->part, h->sc, s));
-        CU(h, launch_cg_xr_fused<float>(L, h->sol, pp_new, l1.f, h->Ap, h->sc, l1.f32, l1.v32, h->part, h->dscal + 1, s));
+        CU(h, launch_cg_xr_fused<float>(L, h->sol, pp_new, l1.f, h->Ap, h->sc, l1.f32, l1.v32, h->part, h->dscal + kScalRes, s));
         break;
     }
-    CU(h, cudaMemcpyAsync(h->h_scal + 1, h->dscal + 1, sizeof(double), cudaMemcpyDeviceToHost, s));
+    CU(h, cudaMemcpyAsync(h->h_scal + kScalRes, h->dscal + kScalRes, sizeof(double), cudaMemcpyDeviceToHost, s));
     return BBMG_OK;
 }
 
@@ -376,7 +388,8 @@ int bbmg_destroy(bbmg_handle *h) {
         dfree(l.oprS32); dfree(l.c2f32); dfree(l.v32); dfree(l.f32); dfree(l.r32);
     }
     dfree(h->OP); dfree(h->LU); dfree(h->piv); dfree(h->pinned); dfree(h->d_info); dfree(h->d_flag);
-    dfree(h->sol); dfree(h->pp); dfree(h->pp2); dfree(h->Ap); dfree(h->x2); dfree(h->sc); dfree(h->part); dfree(h->dscal);
+    dfree(h->sol); dfree(h->pp); dfree(h->pp2); dfree(h->Ap); dfree(h->x2); dfree(h->b1); dfree(h->sc); dfree(h->part);
+    dfree(h->dscal);
     dfree(h->d_opr_in); dfree(h->d_stc); dfree(h->d_io);
     if (h->h_scal) cudaFreeHost(h->h_scal);
     h->copier.release();
@@ -488,12 +501,13 @@ int bbmg_create(const bbmg_grid *grid, const bbmg_params *params, bbmg_handle **
         (st = dalloc(h, &h->piv, (size_t)h->np)) || (st = dalloc(h, &h->pinned, (size_t)h->np)) ||
         (st = dalloc(h, &h->d_info, 1)) || (st = dalloc(h, &h->d_flag, 1)) ||
         (st = dalloc(h, &h->part, (size_t)kRedBlocks)) ||
-        (st = dalloc(h, &h->dscal, 8)) || (st = dalloc(h, &h->sc, 1)))
+        (st = dalloc(h, &h->dscal, kScalN)) || (st = dalloc(h, &h->sc, 1)))
         return bail(st);
     if (mixed && prm.method == BBMG_METHOD_BBOX && (st = dalloc(h, &h->x2, (size_t)L1.plane))) return bail(st);
     if (prm.method == BBMG_METHOD_PCG_BBOX) {
         if ((st = dalloc(h, &h->sol, (size_t)L1.plane)) || (st = dalloc(h, &h->pp, (size_t)L1.plane)) ||
-            (st = dalloc(h, &h->pp2, (size_t)L1.plane)) || (st = dalloc(h, &h->Ap, (size_t)L1.plane)))
+            (st = dalloc(h, &h->pp2, (size_t)L1.plane)) || (st = dalloc(h, &h->Ap, (size_t)L1.plane)) ||
+            (st = dalloc(h, &h->b1, (size_t)L1.plane)))
             return bail(st);
     }
     {
@@ -510,7 +524,7 @@ int bbmg_create(const bbmg_grid *grid, const bbmg_params *params, bbmg_handle **
         }
         if (h->tail_n0) h->tail_smem_b = tail_smem(h->np, &h->tail_mat_in_smem);
     }
-    if (cudaMallocHost((void **)&h->h_scal, 8 * sizeof(double)) != cudaSuccess) return bail(fail(h, BBMG_NO_MEMORY, "pinned host"));
+    if (cudaMallocHost((void **)&h->h_scal, kScalN * sizeof(double)) != cudaSuccess) return bail(fail(h, BBMG_NO_MEMORY, "pinned host"));
     if (cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess)
         return bail(fail(h, BBMG_CUDA, "events"));
     if (cudaStreamSynchronize(h->stream) != cudaSuccess) return bail(fail(h, BBMG_CUDA, "initialisation"));
@@ -672,11 +686,11 @@ int bbmg_setup(bbmg_handle *h, int nst, const int *stc, const double *opr) {
             if (n < h->nlvl) CU(h, launch_to_f32(l.c2f, l.c2f32, 8LL * P, s));
         }
     }
-    CU(h, cudaMemcpyAsync(h->h_scal + 2, h->d_info, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CU(h, cudaMemcpyAsync(h->h_scal + kScalInfo, h->d_info, sizeof(int), cudaMemcpyDeviceToHost, s));
     CU(h, cudaEventRecord(h->ev1, s));
     CU(h, cudaStreamSynchronize(s));
     int info;
-    memcpy(&info, h->h_scal + 2, sizeof(int));
+    memcpy(&info, h->h_scal + kScalInfo, sizeof(int));
     h->lu_info = info;
     std::vector<int> pin(h->np);
     CU(h, cudaMemcpy(pin.data(), h->pinned, sizeof(int) * h->np, cudaMemcpyDeviceToHost));
@@ -733,21 +747,29 @@ int bbmg_solve(bbmg_handle *h, const double *rhs, double *sol, int *it_out, doub
     CU(h, launch_from_caller<double>(L, xsrc, g, l1.v, s));
     // initial residual (bbmg_class.f90:626-628)
     CU(h, launch_residual<double>(L, l1.nb, l1.npt, l1.oprS, l1.v, l1.f, l1.r, s));
-    CU(h, launch_maxabs<double>(L, l1.r, h->part, h->dscal, s));
+    CU(h, launch_maxabs<double>(L, l1.r, h->part, h->dscal + kScalRes0, s));
     const bool by_rhs = h->res_norm == BBMG_NORM_RHS;
-    if (by_rhs) CU(h, launch_maxabs<double>(L, l1.f, h->part, h->dscal + 3, s));
-    CU(h, cudaMemcpyAsync(h->h_scal, h->dscal, sizeof(double) * 4, cudaMemcpyDeviceToHost, s));
+    if (by_rhs) {
+        CU(h, launch_maxabs<double>(L, l1.f, h->part, h->dscal + kScalRhs, s));
+        CU(h, launch_dot<double>(L, l1.f, l1.f, h->part, h->dscal + kScalRhsL2, s));
+    }
+    CU(h, launch_dot<double>(L, l1.r, l1.r, h->part, h->dscal + kScalRes0L2, s));
+    CU(h, cudaMemcpyAsync(h->h_scal, h->dscal, sizeof(double) * kScalTrue, cudaMemcpyDeviceToHost, s));
     double res0 = 0.0;
-    int st = sync_read(h, &res0, 0);
+    int st = sync_read(h, &res0, kScalRes0);
     if (st) return st;
     // denominator of rerr: the guess's own initial residual (the reference's
     // definition), or max|rhs|, the residual a zero guess would start from
-    double rnorm = res0;
-    if (by_rhs && h->h_scal[3] > 0.0) rnorm = h->h_scal[3];
+    double rnorm = res0, rnorm2 = h->h_scal[kScalRes0L2];
+    if (by_rhs && h->h_scal[kScalRhs] > 0.0) {
+        rnorm = h->h_scal[kScalRhs];
+        rnorm2 = h->h_scal[kScalRhsL2];
+    }
     int status = BBMG_OK;
     int fallback_it = 0;
     double *xout = l1.v;
-    long long launches = by_rhs ? 6 : 4;  // two copies-in, residual, max (two) [, max of rhs (two)]
+    // two copies-in, residual, max and sum of squares (two each) [, max and sum of squares of rhs]
+    long long launches = by_rhs ? 10 : 6;
     if (res0 == 0.0) {
         it = 0;
         rerr = 0.0;
@@ -758,7 +780,8 @@ int bbmg_solve(bbmg_handle *h, const double *rhs, double *sol, int *it_out, doub
     } else {
         int mode = (mixed ? 2 : 0) + (krylov ? 1 : 0);
         if (krylov) {
-            // res = r, sol = v (bbmg_class.f90:652-653); res lives in l1.f
+            // res = r, sol = v (bbmg_class.f90:652-653); res lives in l1.f, b is kept in b1
+            CU(h, cudaMemcpyAsync(h->b1, l1.f, sizeof(double) * L.plane, cudaMemcpyDeviceToDevice, s));
             CU(h, cudaMemcpyAsync(l1.f, l1.r, sizeof(double) * L.plane, cudaMemcpyDeviceToDevice, s));
             CU(h, cudaMemcpyAsync(h->sol, l1.v, sizeof(double) * L.plane, cudaMemcpyDeviceToDevice, s));
             CU(h, cudaMemsetAsync(h->sc, 0, sizeof(CgScal), s));
@@ -790,7 +813,7 @@ int bbmg_solve(bbmg_handle *h, const double *rhs, double *sol, int *it_out, doub
             CU(h, cudaGraphLaunch(ge[par], s));
             launches += h->gkernels[mode][par];
             double mr = 0.0;
-            if ((st = sync_read(h, &mr, 1))) return st;
+            if ((st = sync_read(h, &mr, kScalRes))) return st;
             rerr = mr / rnorm;  // bbmg_class.f90:696,723 (rnorm = res0 there)
             it = n;
             hist.push_back(rerr);
@@ -825,6 +848,22 @@ int bbmg_solve(bbmg_handle *h, const double *rhs, double *sol, int *it_out, doub
         }
         if (status == BBMG_OK && rerr > h->prm.rcvg) status = BBMG_MAXIT;
     }
+    // the true FP64 residual of the returned solution: recomputed from b and
+    // x, independent of the iteration's own residual (the CG recurrence)
+    double true_res = 0.0, true_l2 = 0.0;
+    const bool verify = res0 != 0.0 && status != BBMG_NONFINITE;
+    if (verify) {
+        double *bvec = krylov ? h->b1 : l1.f;
+        double *rscr = krylov ? h->Ap : l1.r;
+        // the CG solution is updated on the interior only: refresh its periodic images
+        if (krylov && (L.xper || L.yper || L.zper)) CU(h, wrap_planes(L, xout, 1, s));
+        CU(h, launch_residual<double>(L, l1.nb, l1.npt, l1.oprS, xout, bvec, rscr, s));
+        CU(h, launch_maxabs<double>(L, rscr, h->part, h->dscal + kScalTrue, s));
+        CU(h, launch_dot<double>(L, rscr, rscr, h->part, h->dscal + kScalTrueL2, s));
+        CU(h, cudaMemcpyAsync(h->h_scal + kScalTrue, h->dscal + kScalTrue, 2 * sizeof(double),
+                              cudaMemcpyDeviceToHost, s));
+        launches += 5 + ((krylov && (L.xper || L.yper || L.zper)) ? 1 : 0);
+    }
     // solution out (ils_class.f90:782-788)
     if (sol_dev) {
         CU(h, launch_to_caller(L, xout, g, sol, s));
@@ -840,11 +879,17 @@ int bbmg_solve(bbmg_handle *h, const double *rhs, double *sol, int *it_out, doub
     CU(h, cudaStreamSynchronize(s));
     float ms = 0.f;
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    if (verify) {
+        true_res = h->h_scal[kScalTrue];
+        true_l2 = std::sqrt(h->h_scal[kScalTrueL2]);
+    }
     h->info.solve_ms = ms;
     h->info.it = it;
     h->info.rerr = rerr;
     h->info.res0 = res0;
-    h->info.true_rerr = -1.0;
+    h->info.true_res = verify ? true_res : (res0 == 0.0 ? 0.0 : res0);
+    h->info.true_rerr = verify ? true_res / rnorm : (res0 == 0.0 ? 0.0 : rerr);
+    h->info.l2_rerr = verify ? (rnorm2 > 0.0 ? true_l2 / std::sqrt(rnorm2) : 0.0) : (res0 == 0.0 ? 0.0 : rerr);
     h->info.status = status;
     h->info.launches = launches + 1;
     h->info.fallback_it = fallback_it;

@@ -6,8 +6,11 @@
 // loop that must not allocate because cudaMalloc/cudaFree can synchronise the
 // device.  bbmg_residual_norm_noalloc gives those callers the solver's residual
 // check on their own arrays without allocating: its only scratch is the
-// file-scope array below, reserved when the library is loaded and held by
-// every GPU that loads it until the process exits.
+// file-scope array below.  CUDA places it in a GPU's memory when it loads this
+// library's device code on that GPU -- with CUDA's default lazy module loading
+// that happens at the first call on the GPU, which can synchronise the device,
+// so a caller makes one warm-up call before its time loop or any stream
+// capture -- and the GPU holds it until the process exits.
 //
 // The scratch holds one partial pair (max|r|, max|b|) per k-plane of the
 // grid, so a call accepts at most kNoAllocMaxPlanes planes and rejects larger
@@ -17,7 +20,6 @@
 // race on it and must be serialised by the caller.
 #include <cmath>
 #include <cstdio>
-#include <mutex>
 
 #include "../../include/bbmg_b200.h"
 #include "common.cuh"
@@ -31,12 +33,10 @@ namespace {
 constexpr int kNoAllocMaxPlanes = 8192;  // 2 doubles per plane: 128 KiB
 static __device__ __align__(256) double g_noalloc_scratch[2 * kNoAllocMaxPlanes];
 
-// Address of g_noalloc_scratch on each device.  In host code the array's name
-// is only a host-side stand-in, so the device address is looked up once per
-// device (with that device current) on the first call there.
-constexpr int kMaxDevices = 64;
-std::mutex g_mtx;
-double *g_scratch_ptr[kMaxDevices] = {nullptr};
+// In host code the array's name is only a host-side stand-in, not a device
+// address: every call looks up the address on the current device with
+// cudaGetSymbolAddress (a table lookup once the module is loaded), so no
+// address outlives a device reset or a new primary context.
 
 int noalloc_fail(int code, const char *msg) {
     bbmg::set_create_error(msg);  // reported by bbmg_last_error(NULL)
@@ -123,17 +123,19 @@ __global__ void __launch_bounds__(256) k_noalloc_final(int nz, const double *__r
     if (threadIdx.x == 0) {
         out[0] = shr[0];
         out[1] = shb[0];
-        out[2] = __ddiv_rn(shr[0], shb[0]);
+        // a zero rhs: 0 for a zero residual (what a zero-guess solve reports), +inf otherwise
+        out[2] = shb[0] > 0.0 ? __ddiv_rn(shr[0], shb[0]) : (shr[0] == 0.0 ? 0.0 : HUGE_VAL);
     }
 }
 
-bool on_device(const void *p) {
+// device memory of device `dev` (managed memory is reachable from any device)
+bool on_device(const void *p, int dev) {
     cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    return a.type == cudaMemoryTypeManaged || (a.type == cudaMemoryTypeDevice && a.device == dev);
 }
 
 }  // namespace
@@ -175,27 +177,23 @@ extern "C" int bbmg_residual_norm_noalloc(const bbmg_grid *grid, int nst, const 
         }
     }
     tt.first[tt.nterm] = cnt;
-    if (!on_device(opr) || !on_device(rhs) || !on_device(sol) || !on_device(out))
-        return noalloc_fail(BBMG_BAD_ARGS, "opr, rhs, sol and out must be device memory");
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    if (cudaGetDevice(&dev) != cudaSuccess) {
         cudaGetLastError();
         return noalloc_fail(BBMG_CUDA, "no current CUDA device");
     }
+    if (!on_device(opr, dev) || !on_device(rhs, dev) || !on_device(sol, dev) || !on_device(out, dev))
+        return noalloc_fail(BBMG_BAD_ARGS, "opr, rhs, sol and out must be memory of the current device");
+    // the scratch array's address on this device (the current one)
     double *scratch = nullptr;
     {
-        std::lock_guard<std::mutex> lk(g_mtx);
-        if (!g_scratch_ptr[dev]) {
-            cudaError_t e = cudaGetSymbolAddress((void **)&g_scratch_ptr[dev], g_noalloc_scratch);
-            if (e != cudaSuccess) {
-                g_scratch_ptr[dev] = nullptr;
-                cudaGetLastError();
-                char m[160];
-                snprintf(m, sizeof m, "cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
-                return noalloc_fail(BBMG_CUDA, m);
-            }
+        cudaError_t e = cudaGetSymbolAddress((void **)&scratch, g_noalloc_scratch);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            char m[160];
+            snprintf(m, sizeof m, "cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+            return noalloc_fail(BBMG_CUDA, m);
         }
-        scratch = g_scratch_ptr[dev];
     }
     cudaStream_t s = (cudaStream_t)stream;
     k_noalloc_partials<<<g.nz, 256, 0, s>>>(g, tt, opr, rhs, sol, scratch);

@@ -48,3 +48,24 @@ def test_single_rank_is_identity():
     import bench
     assert bench.max_over_ranks([3.0, 4.0], 1, "cpu") == [3.0, 4.0]
     assert bench.aggregate(1, 10, 500.0) == pytest.approx(20.0)
+
+
+def test_reference_arm_small_grid():
+    """`bench.py --impl reference` on a 24^3 grid: independent single-core oracle
+    processes solve the whole problem (no size extrapolation); the line's steps
+    times ms_per_step is the timed region, and the solves reach rerr 1e-10."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--n", "24",
+                        "--steps", "4", "--warmup", "1"], capture_output=True, text=True, timeout=600, cwd=root)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["steps"] == 4 and line["config"]["n"] == 24
+    cb = line["cpu_baseline"]
+    nsolves = sum(len(s) for s in cb["solve_s"])
+    assert nsolves == 4 and 4 % cb["cores"] == 0
+    assert line["value"] == pytest.approx(1e3 / line["ms_per_step"])
+    assert max(max(s) for s in cb["solve_s"]) <= line["ms_per_step"] * 4 / 1e3 * (1 + 1e-9)
+    assert all(it > 0 for its in cb["iterations"] for it in its)

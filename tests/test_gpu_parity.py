@@ -345,3 +345,32 @@ def test_pageable_host_arrays_match_device():
     assert sth == std == 0 and ith == itd and rh == rd
     assert np.array_equal(xh, xd.cpu().numpy())
     g.close()
+
+
+@pytest.mark.parametrize("method", [BBOX, PCG_BBOX])
+def test_true_residual_report(method):
+    """bbmg_info.true_rerr / l2_rerr: the solution's residual recomputed in FP64
+    after the last iteration.  For FP64 bbox it is the residual the iteration
+    itself ended with (same bits); for pcg_bbox it agrees with an independent
+    numpy product; a zero rhs reports zeros (it = 0)."""
+    pb = P.drops_poisson(24, seed=4, ndrops=4, rmin=2.0, rmax=4.0)
+    per = (pb.xper, pb.yper, pb.zper)
+    g = BBMG(24, 24, 24, *per, method=method, rcvg=1e-10)
+    g.setup(pb.stc, pb.opr)
+    x, it, rerr, st = g.solve(pb.rhs)
+    inf = g.info
+    o = pb.opr
+    Ax = (o[..., 0] * x + o[..., 1] * np.roll(x, -1, 2) + o[..., 2] * np.roll(x, 1, 2)
+          + o[..., 3] * np.roll(x, -1, 1) + o[..., 4] * np.roll(x, 1, 1)
+          + o[..., 5] * np.roll(x, -1, 0) + o[..., 6] * np.roll(x, 1, 0))
+    r = pb.rhs - Ax
+    ref = np.abs(r).max() / np.abs(pb.rhs).max()
+    if method == BBOX:
+        assert inf["true_rerr"] == rerr
+    assert abs(inf["true_rerr"] - ref) <= 1e-3 * ref, (inf["true_rerr"], ref)  # sums in another order
+    l2 = np.linalg.norm(r) / np.linalg.norm(pb.rhs)
+    assert abs(inf["l2_rerr"] - l2) <= 1e-3 * l2, (inf["l2_rerr"], l2)
+    assert abs(inf["true_res"] - np.abs(r).max()) <= 1e-3 * np.abs(r).max()
+    _, it0, rerr0, st0 = g.solve(np.zeros_like(pb.rhs))
+    inf0 = g.info
+    assert (it0, rerr0, st0) == (0, 0.0, 0) and inf0["true_rerr"] == 0.0 and inf0["l2_rerr"] == 0.0

@@ -86,3 +86,23 @@ def test_noalloc_rejects_too_many_planes():
                                         buf.data_ptr(), buf.data_ptr(), buf.data_ptr(), None)
     assert rc == 4
     assert b"8192" in lib.bbmg_last_error(None)
+
+
+def test_noalloc_zero_rhs():
+    """A zero rhs and a zero solution give out = (0, 0, 0), the rerr a zero-guess
+    solve reports for it; a zero rhs with a nonzero residual gives +inf."""
+    import torch
+    lib = _lib()
+    pb, g = _case("drops")
+    grid = B.Grid(pb.nx, pb.ny, pb.nz, int(pb.xper), int(pb.yper), int(pb.zper), g)
+    stc = np.ascontiguousarray(pb.stc, np.int32)
+    dopr = torch.from_numpy(_padded(pb.opr, g)).cuda()
+    zero = torch.zeros(tuple(d + 2 * g for d in (pb.nz, pb.ny, pb.nx)), dtype=torch.float64, device="cuda")
+    sol = torch.rand(zero.shape, dtype=torch.float64, device="cuda")  # not in the null space
+    out = torch.full((3,), -1.0, dtype=torch.float64, device="cuda")
+    for x, want in ((zero, 0.0), (sol, float("inf"))):
+        rc = lib.bbmg_residual_norm_noalloc(C.byref(grid), stc.shape[0], stc.ctypes.data_as(C.POINTER(C.c_int)),
+                                            dopr.data_ptr(), zero.data_ptr(), x.data_ptr(), out.data_ptr(), None)
+        assert rc == 0, lib.bbmg_last_error(None)
+        torch.cuda.synchronize()
+        assert out[1].item() == 0.0 and out[2].item() == want, out.tolist()
