@@ -46,7 +46,11 @@ extern "C" {
 #define BBMG_PREC_FP64   0  /* every step in FP64, the reference's arithmetic   */
 #define BBMG_PREC_MIXED  1  /* FP32 V-cycle inside an FP64 outer iteration; when
                                the residual falls by < 10 % over 3 iterations the
-                               solve continues with the FP64 method           */
+                               solve continues with the FP64 method.  pcg_bbox
+                               then updates its directions by the flexible rule
+                               beta = -z.Ap_old / p_old.Ap_old (FCG(1)), since the
+                               FP32 V-cycle is not an exactly symmetric fixed
+                               preconditioner                                 */
 
 typedef struct bbmg_handle bbmg_handle;
 
@@ -97,6 +101,8 @@ typedef struct {
     double true_res;       /* max|b - A x| at exit (absolute, FP64)           */
     double l2_rerr;        /* ||b - A x||_2 / ||r0||_2 at exit, r0 the initial
                               residual (||rhs||_2 under BBMG_NORM_RHS)        */
+    int stage_it;          /* iterations that applied the preconditioner stage
+                              (bbmg_set_precond_stage) in the last solve      */
 } bbmg_info;
 
 /* Fill `p` with the ILS values: pcg_bbox, FP64, V(2,2), ncell_coarsest 300,
@@ -136,6 +142,29 @@ int bbmg_set_convergence(bbmg_handle *h, int maxit, double rcvg);
 #define BBMG_NORM_GUESS 0
 #define BBMG_NORM_RHS   1
 int bbmg_set_residual_norm(bbmg_handle *h, int norm);
+
+/* First stage of a two-stage preconditioner for pcg_bbox in mixed precision.
+ * The reference preconditions its CG with one V-cycle from a zero guess
+ * (bbmg_class.f90:657-662); with a stage set, the preconditioner of an
+ * iteration is z = S(r) + V(r - A S(r)): the caller's function S gives a first
+ * approximation of A^-1 r (a learned network, for one), the FP32 V-cycle
+ * corrects what it leaves, and the residual r - A S(r) is formed in FP64.  The
+ * directions are A-orthogonalised against the previous one explicitly
+ * (flexible CG, FCG(1)), so S may be nonlinear and change between calls.
+ * r and z are the caller's device arrays of nx*ny*nz doubles (Fortran order,
+ * no overlap layers) on the handle's device: before each call of fn the solver
+ * writes the residual into r; fn(ctx, r, z, stream) writes z = S(r), enqueues
+ * its work on `stream` (a cudaStream_t) and returns 0 (any other value ends
+ * the solve with BBMG_BAD_ARGS); the solver reads z back.  `iters` = number of
+ * leading iterations that apply the stage (0 = all); later iterations use the
+ * V-cycle alone.  If the residual falls by less than 10 % over three
+ * iterations, the solve continues as the plain FP64 pcg_bbox from the current
+ * iterate (bbmg_info.fallback_it), so plain multigrid stays the fallback and
+ * the judge of convergence.  fn = NULL removes the stage.  The handle must be
+ * BBMG_METHOD_PCG_BBOX with BBMG_PREC_MIXED.  No counterpart in the
+ * reference. */
+typedef int (*bbmg_stage_fn)(void *ctx, const double *r, double *z, void *stream);
+int bbmg_set_precond_stage(bbmg_handle *h, bbmg_stage_fn fn, void *ctx, int iters, double *r, double *z);
 
 /* Run on the given cudaStream_t.  The default is a stream the handle
  * creates that synchronises with the legacy default stream, so device arrays

@@ -34,7 +34,7 @@ EXPORTS = ["bbmg_default_params", "bbmg_create", "bbmg_setup", "bbmg_solve", "bb
            "bbmg_set_residual_norm",
            "bbmg_set_stream", "bbmg_get_info", "bbmg_destroy", "bbmg_last_error", "bbmg_debug_get",
            "bbmg_debug_put", "bbmg_debug_step", "bbmg_debug_direct", "bbmg_profile_step",
-           "bbmg_residual_norm_noalloc"]
+           "bbmg_residual_norm_noalloc", "bbmg_set_precond_stage"]
 
 
 class BBMGError(RuntimeError):
@@ -60,7 +60,11 @@ class Info(C.Structure):
                 ("true_rerr", C.c_double), ("setup_ms", C.c_double), ("solve_ms", C.c_double),
                 ("device_bytes", C.c_longlong), ("status", C.c_int), ("launches", C.c_longlong),
                 ("level1_stencil", C.c_int), ("fallback_it", C.c_int), ("true_res", C.c_double),
-                ("l2_rerr", C.c_double)]
+                ("l2_rerr", C.c_double), ("stage_it", C.c_int)]
+
+
+# first preconditioner stage: int fn(void *ctx, const double *r, double *z, void *stream)
+STAGE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p)
 
 
 _LIB = None
@@ -94,6 +98,7 @@ def load(path: str = LIB_PATH):
     lib.bbmg_debug_step.argtypes = [P, I, I, I, I]
     lib.bbmg_debug_direct.argtypes = [P, P, P, P, C.POINTER(C.c_int)]
     lib.bbmg_profile_step.argtypes = [P, I, I, I, I, I, C.POINTER(C.c_double)]
+    lib.bbmg_set_precond_stage.argtypes = [P, STAGE_FN, P, I, P, P]
     _LIB = lib
     return lib
 
@@ -191,6 +196,36 @@ class BBMG:
     def set_residual_norm(self, norm):
         """NORM_GUESS (the reference's rerr) or NORM_RHS (rerr = max|r| / max|rhs|)."""
         self._check(self.lib.bbmg_set_residual_norm(self.h, norm))
+
+    def set_precond_stage(self, fn, r=None, z=None, iters=0):
+        """First preconditioner stage for mixed pcg_bbox (``fn`` None removes it).
+        ``r`` and ``z`` are contiguous float64 CUDA tensors of shape (nz, ny, nx)
+        (no overlap): before each call ``fn(r, z, stream_ptr)`` the solver
+        writes the residual into ``r``; ``fn`` writes its approximation of
+        A^-1 r into ``z``, enqueuing its work on the CUDA stream ``stream_ptr``.
+        An exception in ``fn`` ends the solve with BAD_ARGS (kept in
+        ``stage_error``).  ``iters``: leading iterations that apply it (0 = all)."""
+        if fn is None:
+            self._stage = None
+            self._check(self.lib.bbmg_set_precond_stage(self.h, STAGE_FN(), None, 0, None, None))
+            return
+        want = self.shape if self.grid.ghost == 0 else (self.grid.nz, self.grid.ny, self.grid.nx)
+        for t in (r, z):
+            if tuple(t.shape) != tuple(want):
+                raise ValueError(f"stage arrays must have shape {want}")
+        pr, _ = _ptr(r)
+        pz, _ = _ptr(z)
+
+        def call(ctx, rp, zp, stream):
+            try:
+                fn(r, z, stream)
+                return 0
+            except Exception as e:  # noqa: BLE001 -- reported through the status
+                self.stage_error = e
+                return 1
+        self.stage_error = None
+        self._stage = (STAGE_FN(call), r, z)  # kept alive with the handle
+        self._check(self.lib.bbmg_set_precond_stage(self.h, self._stage[0], None, iters, pr, pz))
 
     def set_stream(self, stream_ptr):
         self._check(self.lib.bbmg_set_stream(self.h, C.c_void_p(stream_ptr)))

@@ -33,6 +33,7 @@ constexpr int kScalRhsL2 = 5;   // sum rhs^2
 constexpr int kScalTrue = 6;    // max|b - A x| at exit
 constexpr int kScalTrueL2 = 7;  // sum (b - A x)^2 at exit
 constexpr int kScalN = 16;
+constexpr int kModes = 5;  // iteration graphs, see record_iteration
 
 struct Level {
     Lay L;
@@ -93,6 +94,17 @@ struct bbmg_handle {
     double *sol = nullptr, *pp = nullptr, *pp2 = nullptr, *Ap = nullptr;  // pp/pp2 alternate per iteration
     double *x2 = nullptr;  // second solution buffer of the mixed defect correction (alternates with lv[1].v)
     double *b1 = nullptr;  // pcg_bbox: the right-hand side (lv[1].f holds the CG residual during the solve)
+    // first preconditioner stage (mixed PCG): the caller's function, its
+    // context, the iterations that apply it (0 = all), the caller's dense
+    // (no overlap) device arrays the residual is handed over in and the
+    // stage's output comes back in, that output in the level layout and the
+    // combined z
+    bbmg_stage_fn stage_fn = nullptr;
+    void *stage_ctx = nullptr;
+    int stage_iters = 0;
+    double *stage_r = nullptr, *stage_z = nullptr;
+    double *z1 = nullptr, *zz = nullptr;
+
     CgScal *sc = nullptr;
     double *part = nullptr, *dscal = nullptr;  // reduction partials; scalars (kScal* slots)
     double *h_scal = nullptr;                  // pinned host mirror of dscal
@@ -104,10 +116,11 @@ struct bbmg_handle {
     size_t io_n = 0;
     bool setup_done = false;
     int npt1 = 27;
-    // graphs of one iteration: [mode] 0 = FP64 MG, 1 = FP64 PCG, 2 = mixed MG, 3 = mixed PCG
+    // graphs of one iteration: [mode] 0 = FP64 MG, 1 = FP64 PCG, 2 = mixed MG, 3 = mixed PCG,
+    // 4 = mixed PCG after a first preconditioner stage;
     // graphs [mode][parity of the iteration] (the CG direction vectors alternate buffers)
-    cudaGraphExec_t gexec[4][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
-    int gkernels[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};  // kernel nodes per graph
+    cudaGraphExec_t gexec[kModes][2] = {};
+    int gkernels[kModes][2] = {};  // kernel nodes per graph
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     long long bytes = 0;
     std::string err;
@@ -294,10 +307,24 @@ int record_iteration(bbmg_handle *h, int mode, int par) {
                                   h->dscal + kScalRes, s));
         break;
     }
-    case 3:  // mixed PCG: FP64 Krylov vectors, FP32 V-cycle; f32/v32 prepared by the previous step
+    case 3:  // mixed PCG: FP64 Krylov vectors, FP32 V-cycle; f32/v32 prepared by the previous step.
+             // The FP32 V-cycle is not an exactly symmetric, fixed operator (its rounding
+             // depends on the residual it is given), so the direction update is the
+             // flexible one, beta = -z.Ap_old / pap_old (FCG(1)), where the reference's
+             // rho/rho_old (bbmg_class.f90:666-672) assumes a fixed SPD preconditioner
         if ((st = vcycle<float>(h, 1))) return st;
-        CU(h, launch_cg_rho<float>(L, l1.v32, l1.f, h->part, h->sc, s));
+        CU(h, launch_fcg_rho<float>(L, l1.v32, l1.f, h->Ap, h->part, h->sc, s));
         CU(h, launch_cg_pap_fused<float>(L, l1.nb, l1.npt, l1.oprS, l1.v32, pp_old, pp_new, h->Ap, h->part, h->sc, s));
+        CU(h, launch_cg_xr_fused<float>(L, h->sol, pp_new, l1.f, h->Ap, h->sc, l1.f32, l1.v32, h->part, h->dscal + kScalRes, s));
+        break;
+    case 4:  // mixed PCG with a first preconditioner stage: z1 = stage(res) is in place
+             // (run before the graph); the V-cycle acts on the remaining residual
+             // res - A z1 and z = z1 + V(res - A z1); flexible direction update
+        CU(h, launch_residual<double>(L, l1.nb, l1.npt, l1.oprS, h->z1, l1.f, l1.r, s));
+        CU(h, launch_round_f32(L, l1.r, l1.f32, s));
+        if ((st = vcycle<float>(h, 1))) return st;
+        CU(h, launch_fcg_z(L, h->z1, l1.v32, l1.f, h->Ap, h->zz, h->part, h->sc, s));
+        CU(h, launch_cg_pap_fused<double>(L, l1.nb, l1.npt, l1.oprS, h->zz, pp_old, pp_new, h->Ap, h->part, h->sc, s));
         CU(h, launch_cg_xr_fused<float>(L, h->sol, pp_new, l1.f, h->Ap, h->sc, l1.f32, l1.v32, h->part, h->dscal + kScalRes, s));
         break;
     }
@@ -389,6 +416,7 @@ int bbmg_destroy(bbmg_handle *h) {
     }
     dfree(h->OP); dfree(h->LU); dfree(h->piv); dfree(h->pinned); dfree(h->d_info); dfree(h->d_flag);
     dfree(h->sol); dfree(h->pp); dfree(h->pp2); dfree(h->Ap); dfree(h->x2); dfree(h->b1); dfree(h->sc); dfree(h->part);
+    dfree(h->z1); dfree(h->zz);
     dfree(h->dscal);
     dfree(h->d_opr_in); dfree(h->d_stc); dfree(h->d_io);
     if (h->h_scal) cudaFreeHost(h->h_scal);
@@ -500,7 +528,7 @@ int bbmg_create(const bbmg_grid *grid, const bbmg_params *params, bbmg_handle **
     if ((st = dalloc(h, &h->OP, (size_t)h->np * h->np)) || (st = dalloc(h, &h->LU, (size_t)h->np * h->np)) ||
         (st = dalloc(h, &h->piv, (size_t)h->np)) || (st = dalloc(h, &h->pinned, (size_t)h->np)) ||
         (st = dalloc(h, &h->d_info, 1)) || (st = dalloc(h, &h->d_flag, 1)) ||
-        (st = dalloc(h, &h->part, (size_t)kRedBlocks)) ||
+        (st = dalloc(h, &h->part, 2 * (size_t)kRedBlocks)) ||
         (st = dalloc(h, &h->dscal, kScalN)) || (st = dalloc(h, &h->sc, 1)))
         return bail(st);
     if (mixed && prm.method == BBMG_METHOD_BBOX && (st = dalloc(h, &h->x2, (size_t)L1.plane))) return bail(st);
@@ -563,6 +591,41 @@ int bbmg_set_residual_norm(bbmg_handle *h, int norm) {
     if (!h) return BBMG_BAD_ARGS;
     if (norm != BBMG_NORM_GUESS && norm != BBMG_NORM_RHS) return fail(h, BBMG_BAD_ARGS, "unknown norm %d", norm);
     h->res_norm = norm;
+    return BBMG_OK;
+}
+
+int bbmg_set_precond_stage(bbmg_handle *h, bbmg_stage_fn fn, void *ctx, int iters, double *r, double *z) {
+    if (!h) return BBMG_BAD_ARGS;
+    if (!fn) {
+        h->stage_fn = nullptr;
+        h->stage_ctx = nullptr;
+        h->stage_r = h->stage_z = nullptr;
+        return BBMG_OK;
+    }
+    if (iters < 0) return fail(h, BBMG_BAD_ARGS, "stage iterations must be >= 0");
+    if (h->prm.method != BBMG_METHOD_PCG_BBOX || h->prm.precision != BBMG_PREC_MIXED)
+        return fail(h, BBMG_BAD_ARGS, "a preconditioner stage needs a pcg_bbox handle in mixed precision");
+    CU(h, cudaSetDevice(h->device));
+    for (const void *p : {(const void *)r, (const void *)z}) {
+        cudaPointerAttributes a;
+        if (!p || cudaPointerGetAttributes(&a, p) != cudaSuccess ||
+            !(a.type == cudaMemoryTypeManaged || (a.type == cudaMemoryTypeDevice && a.device == h->device))) {
+            cudaGetLastError();
+            return fail(h, BBMG_BAD_ARGS, "the stage's r and z must be device arrays of the handle's device");
+        }
+    }
+    if (r == z) return fail(h, BBMG_BAD_ARGS, "the stage's r and z must be distinct arrays");
+    if (!h->z1) {
+        const Lay &L = h->lv[1].L;
+        int st;
+        if ((st = dalloc(h, &h->z1, (size_t)L.plane)) || (st = dalloc(h, &h->zz, (size_t)L.plane))) return st;
+        h->info.device_bytes = h->bytes;
+    }
+    h->stage_fn = fn;
+    h->stage_ctx = ctx;
+    h->stage_iters = iters;
+    h->stage_r = r;
+    h->stage_z = z;
     return BBMG_OK;
 }
 
@@ -766,7 +829,7 @@ int bbmg_solve(bbmg_handle *h, const double *rhs, double *sol, int *it_out, doub
         rnorm2 = h->h_scal[kScalRhsL2];
     }
     int status = BBMG_OK;
-    int fallback_it = 0;
+    int fallback_it = 0, stage_it = 0;
     double *xout = l1.v;
     // two copies-in, residual, max and sum of squares (two each) [, max and sum of squares of rhs]
     long long launches = by_rhs ? 10 : 6;
@@ -779,6 +842,8 @@ int bbmg_solve(bbmg_handle *h, const double *rhs, double *sol, int *it_out, doub
         rerr = res0;
     } else {
         int mode = (mixed ? 2 : 0) + (krylov ? 1 : 0);
+        // a first preconditioner stage (mixed PCG only)
+        bool staged = krylov && mixed && h->stage_fn != nullptr;
         if (krylov) {
             // res = r, sol = v (bbmg_class.f90:652-653); res lives in l1.f, b is kept in b1
             CU(h, cudaMemcpyAsync(h->b1, l1.f, sizeof(double) * L.plane, cudaMemcpyDeviceToDevice, s));
@@ -796,21 +861,35 @@ int bbmg_solve(bbmg_handle *h, const double *rhs, double *sol, int *it_out, doub
             }
             launches += mixed ? 1 : 0;
             xout = h->sol;
+            // the flexible update reads the previous A p (times beta = 0 at the first iteration)
+            if (mixed) CU(h, cudaMemsetAsync(h->Ap, 0, sizeof(double) * L.plane, s));
         } else if (mixed) {
             CU(h, launch_round_f32(L, l1.r, l1.f32, s));
             CU(h, cudaMemsetAsync(l1.v32, 0, sizeof(float) * L.plane, s));
             launches += 1;
         }
-        cudaGraphExec_t ge[2] = {nullptr, nullptr};
         bool pingpong = krylov || mixed;
-        if ((st = get_graph(h, mode, 0, &ge[0]))) return st;
-        if (pingpong && (st = get_graph(h, mode, 1, &ge[1]))) return st;
         std::vector<double> hist;
         hist.reserve(h->prm.maxit + 1);
         for (int n = 1; n <= h->prm.maxit; n++) {
             const int par = pingpong ? ((n - 1) & 1) : 0;
             if (mode == 2) xout = par ? l1.v : h->x2;  // the buffer this iteration writes
-            CU(h, cudaGraphLaunch(ge[par], s));
+            if (staged) {
+                mode = (h->stage_iters == 0 || n <= h->stage_iters) ? 4 : 3;
+                if (mode == 4) {
+                    // the first stage on the current residual, in the caller's dense layout
+                    CU(h, launch_to_caller(L, l1.f, 0, h->stage_r, s));
+                    const int rc = h->stage_fn(h->stage_ctx, h->stage_r, h->stage_z, (void *)s);
+                    if (rc) return fail(h, BBMG_BAD_ARGS, "preconditioner stage returned %d at iteration %d", rc, n);
+                    CU(h, cudaGetLastError());
+                    CU(h, launch_from_caller<double>(L, h->stage_z, 0, h->z1, s));
+                    launches += 2;
+                    stage_it++;
+                }
+            }
+            cudaGraphExec_t ge = nullptr;
+            if ((st = get_graph(h, mode, par, &ge))) return st;
+            CU(h, cudaGraphLaunch(ge, s));
             launches += h->gkernels[mode][par];
             double mr = 0.0;
             if ((st = sync_read(h, &mr, kScalRes))) return st;
@@ -827,11 +906,12 @@ int bbmg_solve(bbmg_handle *h, const double *rhs, double *sol, int *it_out, doub
             // residual drops by less than 10 % over three iterations, the rest
             // of the solve runs the plain FP64 method from the current iterate.
             if (mode >= 2 && n >= 4 && rerr > 0.9 * hist[n - 4]) {
-                if (mode == 3) {
+                if (mode == 3 || mode == 4) {
                     // restart CG (beta = 0) with the FP64 V-cycle as preconditioner
                     CU(h, cudaMemsetAsync(l1.v, 0, sizeof(double) * L.plane, s));
                     CU(h, cudaMemsetAsync(h->sc, 0, sizeof(CgScal), s));
                     mode = 1;
+                    staged = false;
                 } else {
                     // mgsolve's cycles act on lvl(1)%v in place: move x there
                     if (xout != l1.v)
@@ -840,9 +920,6 @@ int bbmg_solve(bbmg_handle *h, const double *rhs, double *sol, int *it_out, doub
                     mode = 0;
                     pingpong = false;
                 }
-                ge[0] = ge[1] = nullptr;
-                if ((st = get_graph(h, mode, 0, &ge[0]))) return st;
-                if (pingpong && (st = get_graph(h, mode, 1, &ge[1]))) return st;
                 fallback_it = n;
             }
         }
@@ -893,6 +970,7 @@ int bbmg_solve(bbmg_handle *h, const double *rhs, double *sol, int *it_out, doub
     h->info.status = status;
     h->info.launches = launches + 1;
     h->info.fallback_it = fallback_it;
+    h->info.stage_it = stage_it;
     if (it_out) *it_out = it;
     if (rerr_out) *rerr_out = rerr;
     return status;

@@ -96,6 +96,9 @@ struct CgScal {
 template <typename TZ>
 cudaError_t launch_cg_rho(const Lay &L, const TZ *zz, const double *res, double *part, CgScal *sc, cudaStream_t s);
 template <typename TZ>
+cudaError_t launch_fcg_rho(const Lay &L, const TZ *zz, const double *res, const double *Ap, double *part, CgScal *sc,
+                           cudaStream_t s);
+template <typename TZ>
 cudaError_t launch_cg_pap_fused(const Lay &L, const NbrOff &nb, int npt, const double *opr, const TZ *zz,
                                 const double *pp_old, double *pp_new, double *Ap, double *part, CgScal *sc,
                                 cudaStream_t s);
@@ -106,6 +109,9 @@ cudaError_t launch_defect_fused(const Lay &L, const NbrOff &nb, int npt, const d
                                 const float *e, const double *b, double *x_new, float *f32, double *part,
                                 double *out, cudaStream_t s);
 cudaError_t launch_round_f32(const Lay &L, const double *r, float *f, cudaStream_t s);
+// flexible CG: zz = z1 + e (z1 may be null), rho = zz.res, beta = -zz.Ap_old / pap_old
+cudaError_t launch_fcg_z(const Lay &L, const double *z1, const float *e, const double *res, const double *Ap,
+                         double *zz, double *part, CgScal *sc, cudaStream_t s);
 
 // caller I/O: Fortran arrays with g overlap layers <-> level interior
 template <typename T>

@@ -1057,6 +1057,63 @@ __global__ void k_cg_pap(const double *__restrict__ part, int n, CgScal *sc) {
     }
 }
 
+// Flexible CG, FCG(1) (Notay, SIAM J. Sci. Comput. 22 (2000) 1444-1460): the
+// preconditioner may change from one iteration to the next (a learned first
+// stage followed by the V-cycle, or the V-cycle alone), so the new direction
+// is A-orthogonalised against the previous one explicitly:
+// p = z - (z.Ap_old / p_old.Ap_old) p_old, i.e. beta = -z.Ap_old / pap_old,
+// instead of the recurrence beta = rho/rho_old of bbmg_class.f90:666-672.
+// With a fixed SPD preconditioner both give the same directions in exact
+// arithmetic.  alpha = z.r / p.Ap is unchanged (r is orthogonal to p_old).
+//
+// k_fcg_z: z = z1 + e (z1 the first stage's output, absent when the stage is
+// off; e the V-cycle correction of z1's residual) on the own cell with its
+// periodic images, and the block partials of z.res (part[0..nb)) and
+// z.Ap_old (part[nb..2nb)).
+__global__ void __launch_bounds__(256) k_fcg_z(Lay L, const double *__restrict__ z1, const float *__restrict__ e,
+                                                const double *__restrict__ res, const double *__restrict__ Ap,
+                                                double *__restrict__ zz, double *__restrict__ part) {
+    pdl_entry();
+    __shared__ double sh[256];
+    double a = 0.0, b = 0.0;
+    FOR_ROWS(L.ny * L.nz) {
+        const int j = row % L.ny, k = row / L.ny;
+        FOR_CHUNKS(L.nx) {
+            const int i = x_of(L, ch);
+            const long long id = L.idx(i, j, k);
+            const double z = z1 ? __dadd_rn(z1[id], (double)e[id]) : (double)e[id];
+            zz[id] = z;
+            if (on_periodic_face(L, i, j, k)) write_images(L, zz, i, j, k, z);
+            a = __dadd_rn(a, __dmul_rn(z, res[id]));
+            b = __dadd_rn(b, __dmul_rn(z, Ap[id]));
+        }
+    }
+    a = block_reduce<1>(a, sh);
+    b = block_reduce<1>(b, sh);
+    if (block_leader()) {
+        part[block_id()] = a;
+        part[gridDim.x * gridDim.y + block_id()] = b;
+    }
+}
+// rho = z.res, beta = -z.Ap_old / pap_old (0 at the first iteration)
+__global__ void k_fcg_scal(const double *__restrict__ part, int n, CgScal *sc) {
+    pdl_entry();
+    __shared__ double sh[256];
+    double a = 0.0, b = 0.0;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        a = a + part[t];
+        b = b + part[n + t];
+    }
+    a = block_reduce<1>(a, sh);
+    b = block_reduce<1>(b, sh);
+    if (threadIdx.x == 0) {
+        sc->rho2 = sc->rho1;
+        sc->rho1 = a;
+        sc->iter += 1;
+        sc->beta = sc->iter == 1 ? 0.0 : -__ddiv_rn(b, sc->pap);
+    }
+}
+
 // pp_new = zz + beta*pp_old on the own cell (with images) and Ap = A pp_new,
 // the neighbours' pp_new formed on the fly from zz and pp_old (bit-identical
 // to the stored value), plus the block partial of pp_new.Ap
@@ -1337,6 +1394,72 @@ __global__ void __launch_bounds__(256) k_dot2_part(Lay L, const TA *__restrict__
     }
     s = block_reduce<1>(s, sh);
     if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// The flexible CG's two dots in one pass, two positions at a time: block
+// partials of a.b (rho = z.res) into part[0..nb) and of a.c (z.Ap_old) into
+// part[nb..2nb), the sums in k_dot2_part's order.
+template <typename TA>
+__global__ void __launch_bounds__(256) k_dot2_flex_part(Lay L, const TA *__restrict__ a, const double *__restrict__ b,
+                                                         const double *__restrict__ c, double *__restrict__ part) {
+    pdl_entry();
+    __shared__ double sh[256];
+    const int CH = L.nx >> 2;
+    const long long total = (long long)L.ny * L.nz * 2 * CH;
+    double s = 0.0, t2 = 0.0;
+    const long long st = gstride();
+    for (long long t0 = gtid(); t0 < total; t0 += 4 * st) {
+        typename Pair<TA>::V x[4];
+        double2 y[4], z[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const long long t = t0 + u * st;
+            if (t < total) {
+                int j, k, hh, cc;
+                const long long e = pair_base(L, t, CH, j, k, hh, cc);
+                x[u] = *reinterpret_cast<const typename Pair<TA>::V *>(a + e);
+                y[u] = *reinterpret_cast<const double2 *>(b + e);
+                z[u] = *reinterpret_cast<const double2 *>(c + e);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            if (t0 + u * st < total) {
+                s = __dadd_rn(s, __dmul_rn((double)x[u].x, y[u].x));
+                s = __dadd_rn(s, __dmul_rn((double)x[u].y, y[u].y));
+                t2 = __dadd_rn(t2, __dmul_rn((double)x[u].x, z[u].x));
+                t2 = __dadd_rn(t2, __dmul_rn((double)x[u].y, z[u].y));
+            }
+        }
+    }
+    s = block_reduce<1>(s, sh);
+    t2 = block_reduce<1>(t2, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = s;
+        part[gridDim.x + blockIdx.x] = t2;
+    }
+}
+// the same for any nx, one cell per thread
+template <typename TA>
+__global__ void __launch_bounds__(256) k_dot_flex_part(Lay L, const TA *__restrict__ a, const double *__restrict__ b,
+                                                        const double *__restrict__ c, double *__restrict__ part) {
+    pdl_entry();
+    __shared__ double sh[256];
+    double s = 0.0, t2 = 0.0;
+    FOR_ROWS(L.ny * L.nz) {
+        const int j = row % L.ny, k = row / L.ny;
+        FOR_CHUNKS(L.nx) {
+            const long long id = L.idx(x_of(L, ch), j, k);
+            s = __dadd_rn(s, __dmul_rn((double)a[id], b[id]));
+            t2 = __dadd_rn(t2, __dmul_rn((double)a[id], c[id]));
+        }
+    }
+    s = block_reduce<1>(s, sh);
+    t2 = block_reduce<1>(t2, sh);
+    if (block_leader()) {
+        part[block_id()] = s;
+        part[gridDim.x * gridDim.y + block_id()] = t2;
+    }
 }
 
 // k_cg_xr_fused two positions at a time (same per-point arithmetic)
@@ -1817,6 +1940,22 @@ cudaError_t launch_cg_rho(const Lay &L, const TZ *zz, const double *res, double 
     return cudaSuccess;
 }
 
+// flexible CG scalars: rho = zz.res and beta = -zz.Ap_old / pap_old
+template <typename TZ>
+cudaError_t launch_fcg_rho(const Lay &L, const TZ *zz, const double *res, const double *Ap, double *part, CgScal *sc,
+                           cudaStream_t s) {
+    if (use_staged(L)) {  // nx a multiple of 8: two positions per thread
+        const unsigned nb2 = pair_grid(L);
+        BB_CHECK_LAUNCH((launch_k(k_dot2_flex_part<TZ>, dim3(nb2), dim3(256), 0, s, L, zz, res, Ap, part)));
+        BB_CHECK_LAUNCH((launch_k(k_fcg_scal, dim3(1), dim3(256), 0, s, (const double *)part, (int)nb2, sc)));
+        return cudaSuccess;
+    }
+    const Geo g = geo_red(L);
+    BB_CHECK_LAUNCH((launch_k(k_dot_flex_part<TZ>, g.grid, g.block, 0, s, L, zz, res, Ap, part)));
+    BB_CHECK_LAUNCH((launch_k(k_fcg_scal, dim3(1), dim3(256), 0, s, (const double *)part, (int)(g.grid.x * g.grid.y), sc)));
+    return cudaSuccess;
+}
+
 template <typename TZ>
 cudaError_t launch_cg_pap_fused(const Lay &L, const NbrOff &nb, int npt, const double *opr, const TZ *zz,
                                 const double *pp_old, double *pp_new, double *Ap, double *part, CgScal *sc,
@@ -1873,6 +2012,15 @@ cudaError_t launch_cg_xr_fused(const Lay &L, double *sol, const double *pp, doub
     const Geo g = geo_red(L);
     BB_CHECK_LAUNCH((launch_k(k_cg_xr_fused<TV>, g.grid, g.block, 0, s, L, sol, pp, res, Ap, sc, f32, vzero, part)));
     BB_CHECK_LAUNCH((launch_k(k_final<0>, dim3(1), dim3(256), 0, s, (const double *)part, (int)(g.grid.x * g.grid.y), out)));
+    return cudaSuccess;
+}
+
+cudaError_t launch_fcg_z(const Lay &L, const double *z1, const float *e, const double *res, const double *Ap,
+                         double *zz, double *part, CgScal *sc, cudaStream_t s) {
+    const Geo g = geo_rows(L.nx, (long long)L.ny * L.nz, kRedBlocks / 2);  // 2 partials per block
+    const int nb = (int)(g.grid.x * g.grid.y);
+    BB_CHECK_LAUNCH((launch_k(k_fcg_z, g.grid, g.block, 0, s, L, z1, e, res, Ap, zz, part)));
+    BB_CHECK_LAUNCH((launch_k(k_fcg_scal, dim3(1), dim3(256), 0, s, (const double *)part, nb, sc)));
     return cudaSuccess;
 }
 
@@ -2087,6 +2235,8 @@ template cudaError_t launch_vtail<float>(const TailArgs<float> &, int, size_t, c
     template cudaError_t launch_dot<T>(const Lay &, const T *, const T *, double *, double *, cudaStream_t);        \
     template cudaError_t launch_from_caller<T>(const Lay &, const double *, int, T *, cudaStream_t);                 \
     template cudaError_t launch_cg_rho<T>(const Lay &, const T *, const double *, double *, CgScal *, cudaStream_t); \
+    template cudaError_t launch_fcg_rho<T>(const Lay &, const T *, const double *, const double *, double *, CgScal *, \
+                                           cudaStream_t);                                                            \
     template cudaError_t launch_cg_pap_fused<T>(const Lay &, const NbrOff &, int, const double *, const T *,         \
                                                 const double *, double *, double *, double *, CgScal *,             \
                                                 cudaStream_t);                                                       \

@@ -407,6 +407,128 @@ class LearnedGuess:
         return loss
 
 
+class LearnedStage:
+    """A trained UNet as the first stage of the pcg_bbox preconditioner
+    (``BBMG.set_precond_stage``): z1 = kappa max|r| net(r / max|r|, rho / ratio),
+    an approximation of A^-1 r that the FP32 V-cycle then corrects (the solver
+    forms r - A z1 in FP64 and applies the V-cycle to it).  The network is the
+    guess's architecture with the residual (and the density, for two-phase
+    flow) as inputs; it is trained on (residual, error) pairs of the plain
+    solver's own iterations (``stage_samples``).  ``coarse``: the network runs
+    on the grid twice as coarse, as the guess does."""
+
+    def __init__(self, net: UNet, kappa=1.0, use_rho=True, ratio=1000.0, coarse=False):
+        self.net, self.kappa, self.use_rho, self.ratio, self.coarse = net, float(kappa), use_rho, ratio, coarse
+        if net.nf != (2 if use_rho else 1):
+            raise ValueError("network input count does not match use_rho")
+        self.rho = None
+        self.calls = 0
+
+    def set_density(self, rho):
+        """The density field of the operator being solved (FP64, the solve's shape)."""
+        self.rho = rho
+
+    def _fields(self, r, rho, rmax):
+        f, s = [r], [1.0 / rmax if rmax > 0 else 0.0]
+        if self.use_rho:
+            f.append(rho)
+            s.append(1.0 / self.ratio)
+        return f, s
+
+    def _buffers(self, shape, train):
+        nz, ny, nx = shape
+        k = 2 if self.coarse else 1
+        return self.net.buffers((1, nz // k, ny // k, nx // k), train)
+
+    def __call__(self, r, z, stream):
+        """The stage: z = kappa max|r| net(r) on the solver's stream."""
+        torch = self.net.torch
+        with torch.cuda.stream(torch.cuda.ExternalStream(stream)):
+            net = self.net
+            rmax = float(r.abs().max())
+            b = self._buffers(r.shape, False)
+            f, s = self._fields(r, self.rho, rmax)
+            net.embed(b, f, s, pool=2 if self.coarse else 1)
+            net.forward(b)
+            n, d, h, w = b["shape"][0]
+            _check(net.lib.nn_apply(None, net._ptr(b["out"]), self.kappa * rmax, n, d, h, w,
+                                    2 if self.coarse else 1, net._ptr(z), net.stream), "apply")
+        self.calls += 1
+
+    def train_step(self, rec, lr):
+        """One Adam step on a (residual "r", error "e", density "rho") sample."""
+        net = self.net
+        r = rec["r"]
+        rmax = float(r.abs().max())
+        b = self._buffers(r.shape, True)
+        f, s = self._fields(r, rec.get("rho"), rmax)
+        net.embed(b, f, s, pool=2 if self.coarse else 1)
+        net.forward(b)
+        loss = net.loss_grad(b, rec["target"], 1.0 / (self.kappa * rmax))
+        net.grads.zero_()
+        net.backward(b)
+        net.adam(lr)
+        return loss
+
+
+def apply_opr7(opr, x):
+    """A x for a 7-point operator opr[k, j, i, st] (NGA2's stencil order) on a
+    periodic (or wall-coefficient-zero) field x[k, j, i] (torch or numpy)."""
+    roll = x.roll if hasattr(x, "roll") else (lambda sh, ax: np.roll(x, sh, ax))
+    return (opr[..., 0] * x + opr[..., 1] * roll(-1, 2) + opr[..., 2] * roll(1, 2)
+            + opr[..., 3] * roll(-1, 1) + opr[..., 4] * roll(1, 1)
+            + opr[..., 5] * roll(-1, 0) + opr[..., 6] * roll(1, 0))
+
+
+def stage_samples(handle, rec, iters=(0, 1, 2)):
+    """(residual, error) pairs of the plain FP64 pcg_bbox on one sequence
+    record: from the zero guess (r = rhs, e = dp) and after k = 1, 2, ...
+    iterations (x_k from a solve stopped at maxit = k, r_k = rhs - A x_k,
+    e_k = dp - x_k with the mean removed: the periodic problem fixes the
+    solution up to a constant).  `handle` is a BBMG handle set up with rec's
+    operator."""
+    zeros = rec["rhs"].new_zeros
+    out = []
+    b, dp, opr = rec["rhs"], rec["dp"], rec["opr"]
+    for k in iters:
+        if k == 0:
+            r, e = b.clone(), dp - dp.mean()
+        else:
+            x = zeros(b.shape)
+            handle.set_convergence(k, 1e-30)
+            handle.solve(b, x, allow=(0, 1))
+            r = b - apply_opr7(opr, x)
+            e = dp - x
+            e = e - e.mean()
+        out.append({"r": r.contiguous(), "e": e.contiguous(), "rho": rec.get("rho"), "k": k})
+    return out
+
+
+def fit_stage_kappa(samples):
+    """Median of max|e| / max|r| over the samples."""
+    return float(np.median([float(s["e"].abs().max()) / float(s["r"].abs().max()) for s in samples]))
+
+
+def train_stage(stage: LearnedStage, samples, steps, lr=2e-3, lr_final=2e-4, seed=0):
+    """Adam on randomly drawn (residual, error) samples, cosine learning-rate
+    decay; returns the per-step losses (normalised MSE)."""
+    torch = stage.net.torch
+    rng = np.random.default_rng(seed)
+    for smp in samples:
+        if "target" not in smp:
+            t = smp["e"]
+            if stage.coarse:
+                t = torch.nn.functional.avg_pool3d(t[None, None], 2)[0, 0]
+            smp["target"] = t.contiguous()
+    losses = []
+    for t in range(steps):
+        lr_t = lr_final + 0.5 * (lr - lr_final) * (1.0 + math.cos(math.pi * t / max(1, steps)))
+        smp = samples[int(rng.integers(len(samples)))]
+        nvox = smp["r"].numel() // (8 if stage.coarse else 1)
+        losses.append(float(stage.train_step(smp, lr_t)) / nvox)
+    return losses
+
+
 def fit_kappa(records):
     """Median of max|dp - p_prev| / max|rhs| over the training records."""
     r = [float((rec["dp"] - rec["p_prev"]).abs().max()) / float(rec["rhs"].abs().max()) for rec in records]
