@@ -105,12 +105,13 @@ __global__ void k_prolong_sweep1(Lay L, const double *__restrict__ opr, double *
         any_cell(L, t, i, j, k);
         long long id = L.idx(i, j, k);
         int n1 = pmod(L.xper, i, L.nx), n2 = pmod(L.yper, j, L.ny), n3 = pmod(L.zper, k, L.nz);
-        double c[8];
-#pragma unroll
-        for (int s = 0; s < 8; s++) c[s] = 0.0;
+        // c2f(0,0,0) and the one line weight (slot sx); every other weight is zero.
+        // Scalars rather than an array indexed at run time, so nothing goes to local memory.
+        double c0 = 0.0, cx = 0.0;
+        int sx = -1;
         int sum = n1 + n2 + n3;
         if (sum == 0) {
-            c[0] = 1.0;
+            c0 = 1.0;
         } else if (sum == 1) {
             double m = 0.0, z = 0.0, p = 0.0;  // opr1d(-1), opr1d(0), opr1d(+1)
 #pragma unroll 1
@@ -129,11 +130,12 @@ __global__ void k_prolong_sweep1(Lay L, const double *__restrict__ opr, double *
                 }
             }
             z = sgn_clamp(z);
-            c[0] = -m / z;
-            c[n1 ? q8(1, 0, 0) : (n2 ? q8(0, 1, 0) : q8(0, 0, 1))] = -p / z;
+            c0 = -m / z;
+            cx = -p / z;
+            sx = n1 ? q8(1, 0, 0) : (n2 ? q8(0, 1, 0) : q8(0, 0, 1));
         }
 #pragma unroll
-        for (int s = 0; s < 8; s++) c2f[s * L.plane + id] = c[s];
+        for (int s = 0; s < 8; s++) c2f[s * L.plane + id] = s == 0 ? c0 : (s == sx ? cx : 0.0);
     }
 }
 
@@ -151,36 +153,41 @@ __device__ __forceinline__ void face_weights(const Lay &L, const double *__restr
     const int na[3] = {L.nx, L.ny, L.nz};
     if (ia[PA] == -1 || ia[PA] == na[PA] || ia[PB] == -1 || ia[PB] == na[PB]) return;
     const long long id = L.idx(i, j, k);
-    double o2[9];  // opr2d(a,b) at (a+1) + 3(b+1)
+    // opr2d(a,b) at (a+1) + 3(b+1).  The loops are unrolled so every index
+    // into o2 and c is a compile-time constant: both stay in registers.
+    double o2[9];
 #pragma unroll
     for (int e = 0; e < 9; e++) o2[e] = 0.0;
-#pragma unroll 1
+#pragma unroll
     for (int q = 0; q < 27; q++) {
         if (!((mask >> q) & 1u)) continue;  // an all-zero plane adds only zeros
-        int l[3] = {q % 3 - 1, (q / 3) % 3 - 1, q / 9 - 1};
-        int la = l[PA], lb = l[PB];
+        const int l[3] = {q % 3 - 1, (q / 3) % 3 - 1, q / 9 - 1};
+        const int la = l[PA], lb = l[PB];
         int lr[3] = {l[0], l[1], l[2]};
         lr[AXN] = 0;
-        double a = opr[q * L.plane + id];
-        int e = __dmul_rn(ratio, fabs(opr[q27(lr[0], lr[1], lr[2]) * L.plane + id])) >= fabs(a) ? (la + 1) + 3 * (lb + 1) : 4;
-        o2[e] = __dadd_rn(o2[e], a);
+        const double a = opr[q * L.plane + id];
+        const int e1 = (la + 1) + 3 * (lb + 1);
+        if (__dmul_rn(ratio, fabs(opr[q27(lr[0], lr[1], lr[2]) * L.plane + id])) >= fabs(a))
+            o2[e1] = __dadd_rn(o2[e1], a);
+        else
+            o2[4] = __dadd_rn(o2[4], a);
     }
     const double o00 = sgn_clamp(o2[4]);
     double c[8];
 #pragma unroll
     for (int t = 0; t < 8; t++) c[t] = c2f[t * L.plane + id];
-#pragma unroll 1
+#pragma unroll
     for (int lb = -1; lb <= 1; lb++)
-#pragma unroll 1
+#pragma unroll
         for (int la = -1; la <= 1; la++) {
             if (la == 0 && lb == 0) continue;
             int off[3] = {0, 0, 0};
             off[PA] = la; off[PB] = lb;
             const long long nid = L.idx(i + off[0], j + off[1], k + off[2]);
             const double w = o2[(la + 1) + 3 * (lb + 1)] / o00;
-#pragma unroll 1
+#pragma unroll
             for (int qb = 0; qb <= 1 - abs(lb); qb++)
-#pragma unroll 1
+#pragma unroll
                 for (int qa = 0; qa <= 1 - abs(la); qa++) {
                     int s3[3] = {0, 0, 0}, p3[3] = {0, 0, 0};
                     s3[PA] = (la + 1) / 2 + qa; s3[PB] = (lb + 1) / 2 + qb;
@@ -220,15 +227,20 @@ __global__ void k_prolong_sweep3(Lay L, const double *__restrict__ opr, double *
         double c[8];
 #pragma unroll
         for (int s = 0; s < 8; s++) c[s] = c2f[s * L.plane + id];
-#pragma unroll 1
+        // unrolled: every index into c is a compile-time constant (registers)
+#pragma unroll 27
         for (int q = 0; q < 27; q++) {
             if (q == kCentre27 || !((mask >> q) & 1u)) continue;  // an all-zero plane subtracts only zeros
-            int li = q % 3 - 1, lj = (q / 3) % 3 - 1, lk = q / 9 - 1;
+            const int li = q % 3 - 1, lj = (q / 3) % 3 - 1, lk = q / 9 - 1;
+            const int ni = li ? 1 : 2, nj = lj ? 1 : 2, nk = lk ? 1 : 2;  // prolongation weights per direction
             long long nid = L.idx(i + li, j + lj, k + lk);
             double w = opr[q * L.plane + id] / d;
-            for (int pk = 0; pk <= 1 - abs(lk); pk++)
-                for (int pj = 0; pj <= 1 - abs(lj); pj++)
-                    for (int pi = 0; pi <= 1 - abs(li); pi++) {
+#pragma unroll 2
+            for (int pk = 0; pk < nk; pk++)
+#pragma unroll 2
+                for (int pj = 0; pj < nj; pj++)
+#pragma unroll 2
+                    for (int pi = 0; pi < ni; pi++) {
                         int so = q8((li + 1) / 2 + pi, (lj + 1) / 2 + pj, (lk + 1) / 2 + pk);
                         c[so] = __dsub_rn(c[so], __dmul_rn(w, c2f[q8(pi, pj, pk) * L.plane + nid]));
                     }
@@ -263,54 +275,69 @@ __global__ void k_restriction_weights(Lay F, Lay C, const double *__restrict__ c
 }
 
 // ---------------------------------------------------------------------------
-// Galerkin operator, part 1: oprc2f = A P on the fine interior
-// (bbmg_class.f90:1245-1271).
+// Galerkin operator, part 1: oprc2f = A P at one fine interior cell
+// (bbmg_class.f90:1245-1271), the 27 sums in the reference's order.  The
+// accumulators are indexed at run time, so they live in shared memory (slot q
+// at acc[q * AS]: with AS the block's thread count a warp's accesses fall in
+// distinct banks), not in a per-thread local array that spills to L2.
+__device__ __forceinline__ void ap_cell(const Lay &F, const double *__restrict__ opr, const double *__restrict__ c2f,
+                                        unsigned mask, int fi, int fj, int fk, double *acc, int AS) {
+    const long long id = F.idx(fi, fj, fk);
+    const int px0 = pmod(F.xper, fi, F.nx), py0 = pmod(F.yper, fj, F.ny), pz0 = pmod(F.zper, fk, F.nz);
+#pragma unroll
+    for (int q = 0; q < 27; q++) acc[q * AS] = 0.0;
+#pragma unroll 1
+    for (int q = 0; q < 27; q++) {
+        if (!((mask >> q) & 1u)) continue;  // an all-zero plane adds only zeros
+        int li = q % 3 - 1, lj = (q / 3) % 3 - 1, lk = q / 9 - 1;
+        int pxl = pmod(F.xper, fi + li, F.nx), pyl = pmod(F.yper, fj + lj, F.ny), pzl = pmod(F.zper, fk + lk, F.nz);
+        double o = opr[q * F.plane + id];
+        long long nid = F.idx(fi + li, fj + lj, fk + lk);
+        for (int pk = 0; pk <= pzl; pk++)
+            for (int pj = 0; pj <= pyl; pj++)
+                for (int pi = 0; pi <= pxl; pi++) {
+                    int si = pi + (1 - px0) * min(li, 0) + (1 - pxl) * max(li, 0);
+                    int sj = pj + (1 - py0) * min(lj, 0) + (1 - pyl) * max(lj, 0);
+                    int sk = pk + (1 - pz0) * min(lk, 0) + (1 - pzl) * max(lk, 0);
+                    int so = q27(si, sj, sk);
+                    acc[so * AS] = __dadd_rn(acc[so * AS], __dmul_rn(o, c2f[q8(pi, pj, pk) * F.plane + nid]));
+                }
+    }
+}
+
+// oprc2f = A P on the whole fine interior.
 __global__ void k_rap_ap(Lay F, const double *__restrict__ opr, const double *__restrict__ c2f,
                          double *__restrict__ oprc2f, unsigned mask) {
+    extern __shared__ double rap_sm[];
+    double *acc = rap_sm + threadIdx.x;
+    const int AS = blockDim.x;
     long long total = (long long)F.nx * F.ny * F.nz;
     for (long long t = gtid(); t < total; t += gstride()) {
         int fi, fj, fk;
         interior_cell(F, t, fi, fj, fk);
-        long long id = F.idx(fi, fj, fk);
-        int px0 = pmod(F.xper, fi, F.nx), py0 = pmod(F.yper, fj, F.ny), pz0 = pmod(F.zper, fk, F.nz);
-        double acc[27];
+        ap_cell(F, opr, c2f, mask, fi, fj, fk, acc, AS);
+        const long long id = F.idx(fi, fj, fk);
 #pragma unroll
-        for (int q = 0; q < 27; q++) acc[q] = 0.0;
-#pragma unroll 1
-        for (int q = 0; q < 27; q++) {
-            if (!((mask >> q) & 1u)) continue;  // an all-zero plane adds only zeros
-            int li = q % 3 - 1, lj = (q / 3) % 3 - 1, lk = q / 9 - 1;
-            int pxl = pmod(F.xper, fi + li, F.nx), pyl = pmod(F.yper, fj + lj, F.ny), pzl = pmod(F.zper, fk + lk, F.nz);
-            double o = opr[q * F.plane + id];
-            long long nid = F.idx(fi + li, fj + lj, fk + lk);
-            for (int pk = 0; pk <= pzl; pk++)
-                for (int pj = 0; pj <= pyl; pj++)
-                    for (int pi = 0; pi <= pxl; pi++) {
-                        int si = pi + (1 - px0) * min(li, 0) + (1 - pxl) * max(li, 0);
-                        int sj = pj + (1 - py0) * min(lj, 0) + (1 - pyl) * max(lj, 0);
-                        int sk = pk + (1 - pz0) * min(lk, 0) + (1 - pzl) * max(lk, 0);
-                        int so = q27(si, sj, sk);
-                        acc[so] = __dadd_rn(acc[so], __dmul_rn(o, c2f[q8(pi, pj, pk) * F.plane + nid]));
-                    }
-        }
-#pragma unroll
-        for (int q = 0; q < 27; q++) oprc2f[q * F.plane + id] = acc[q];
+        for (int q = 0; q < 27; q++) oprc2f[q * F.plane + id] = acc[q * AS];
     }
 }
 
 // Galerkin operator, part 2: A_c = R (A P) on the coarse interior
-// (bbmg_class.f90:1274-1300).  opr_c is zero beforehand.
+// (bbmg_class.f90:1274-1300), accumulators in shared memory as in k_rap_ap.
+// opr_c is zero beforehand.
 __global__ void k_rap_rap(Lay F, Lay C, const double *__restrict__ f2c, const double *__restrict__ oprc2f,
                           double *__restrict__ oprc) {
+    extern __shared__ double rap_sm[];
+    double *acc = rap_sm + threadIdx.x;
+    const int AS = blockDim.x;
     long long total = (long long)C.nx * C.ny * C.nz;
     for (long long t = gtid(); t < total; t += gstride()) {
         int ci, cj, ck;
         interior_cell(C, t, ci, cj, ck);
         int fi = 2 * ci, fj = 2 * cj, fk = 2 * ck;
         long long cid = C.idx(ci, cj, ck);
-        double acc[27];
 #pragma unroll
-        for (int q = 0; q < 27; q++) acc[q] = 0.0;
+        for (int q = 0; q < 27; q++) acc[q * AS] = 0.0;
         int rk0 = -pmod(F.zper, fk - 1, F.nz), rk1 = pmod(F.zper, fk + 1, F.nz);
         int rj0 = -pmod(F.yper, fj - 1, F.ny), rj1 = pmod(F.yper, fj + 1, F.ny);
         int ri0 = -pmod(F.xper, fi - 1, F.nx), ri1 = pmod(F.xper, fi + 1, F.nx);
@@ -330,11 +357,11 @@ __global__ void k_rap_rap(Lay F, Lay C, const double *__restrict__ f2c, const do
                             for (int li = li0; li <= 1; li++) {
                                 // (r-1)/2 truncates toward zero, as Fortran's integer division
                                 int so = q27((ri - 1) / 2 + li, (rj - 1) / 2 + lj, (rk - 1) / 2 + lk);
-                                acc[so] = __dadd_rn(acc[so], __dmul_rn(w, oprc2f[q27(li, lj, lk) * F.plane + nid]));
+                                acc[so * AS] = __dadd_rn(acc[so * AS], __dmul_rn(w, oprc2f[q27(li, lj, lk) * F.plane + nid]));
                             }
                 }
 #pragma unroll
-        for (int q = 0; q < 27; q++) oprc[q * C.plane + cid] = acc[q];
+        for (int q = 0; q < 27; q++) oprc[q * C.plane + cid] = acc[q * AS];
     }
 }
 
@@ -521,16 +548,18 @@ cudaError_t setup_operator(const Lay &F, const Lay &C, const double *oprF, const
     cudaError_t e;
     // the products are written on every interior cell; the overlap is zero
     // (non-periodic) or the periodic image
+    constexpr int nt = 128;
+    constexpr size_t smem = 27 * nt * sizeof(double);  // 27 accumulators per thread
     k_zero_shell<<<grid_for(shell_cells(F), 256), 256, 0, s>>>(F, oprc2f, 27);
     BB_LAUNCH_CHECK();
     long long nf = (long long)F.nx * F.ny * F.nz;
-    k_rap_ap<<<grid_for(nf, 128), 128, 0, s>>>(F, oprF, c2f, oprc2f, mask);
+    k_rap_ap<<<grid_for(nf, nt), nt, smem, s>>>(F, oprF, c2f, oprc2f, mask);
     BB_LAUNCH_CHECK();
     if ((e = wrap_planes(F, oprc2f, 27, s)) != cudaSuccess) return e;
     k_zero_shell<<<grid_for(shell_cells(C), 256), 256, 0, s>>>(C, oprC, 27);
     BB_LAUNCH_CHECK();
     long long nc = (long long)C.nx * C.ny * C.nz;
-    k_rap_rap<<<grid_for(nc, 128), 128, 0, s>>>(F, C, f2c, oprc2f, oprC);
+    k_rap_rap<<<grid_for(nc, nt), nt, smem, s>>>(F, C, f2c, oprc2f, oprC);
     BB_LAUNCH_CHECK();
     return wrap_planes(C, oprC, 27, s);
 }

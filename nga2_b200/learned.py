@@ -535,21 +535,33 @@ def fit_kappa(records):
     return float(np.median(r))
 
 
-def train(guess: LearnedGuess, records, steps, lr=2e-3, lr_final=2e-4, seed=0, log=None):
+def _with_target(rec, coarse):
+    """The record with the network's target: the change from the warm start, on its grid."""
+    if "target" not in rec:
+        torch = __import__("torch")
+        t = rec["dp"] - rec["p_prev"]
+        if coarse:
+            t = torch.nn.functional.avg_pool3d(t[None, None], 2)[0, 0]
+        rec["target"] = t.contiguous()
+    return rec
+
+
+def train(guess: LearnedGuess, records, steps, lr=2e-3, lr_final=2e-4, seed=0, log=None, fetch=None):
     """Adam on randomly drawn training records with a cosine learning-rate
-    decay; returns the per-step losses (normalised MSE)."""
-    torch = guess.net.torch
+    decay; returns the per-step losses (normalised MSE).  ``fetch`` (optional)
+    turns a stored record into the FP64 record a step trains on (for training
+    sets kept in a compact form); without it the targets are cached on the
+    records."""
     rng = np.random.default_rng(seed)
-    for rec in records:  # the network's target: the change from the warm start, on its grid
-        if "target" not in rec:
-            t = rec["dp"] - rec["p_prev"]
-            if guess.coarse:
-                t = torch.nn.functional.avg_pool3d(t[None, None], 2)[0, 0]
-            rec["target"] = t.contiguous()
+    if fetch is None:
+        for rec in records:
+            _with_target(rec, guess.coarse)
     losses = []
     for t in range(steps):
         lr_t = lr_final + 0.5 * (lr - lr_final) * (1.0 + math.cos(math.pi * t / max(1, steps)))
         rec = records[int(rng.integers(len(records)))]
+        if fetch is not None:
+            rec = _with_target(fetch(rec), guess.coarse)
         nvox = rec["rhs"].numel() // (8 if guess.coarse else 1)
         losses.append(float(guess.train_step(rec, lr_t)) / nvox)
         if log and (t % 50 == 0 or t == steps - 1):

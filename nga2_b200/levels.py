@@ -6,7 +6,9 @@ V-cycle from level n down, the fused coarse tail included) and of the single
 passes (a Gauss-Seidel sweep, residual, restriction, prolongation) on the
 finest levels, then one full solve.  ``cycle(n) - cycle(n+1)`` is the cost of
 level n within a V-cycle.  With ``--cycle N`` only cycle(N) runs, ``--reps``
-times, which is the small case to put under a profiler.
+times, which is the small case to put under a profiler.  With ``--setup`` it
+times the setup (the whole Galerkin hierarchy) from a device-resident
+operator instead, the call the two-phase solvers make on every density change.
 """
 from __future__ import annotations
 
@@ -24,6 +26,7 @@ def main(argv=None):
     ap.add_argument("--precision", choices=("mixed", "fp64"), default="mixed")
     ap.add_argument("--cycle", type=int, default=0, help="run only cycle(N)")
     ap.add_argument("--reps", type=int, default=20)
+    ap.add_argument("--setup", action="store_true", help="time bbmg_setup from a device operator")
     a = ap.parse_args(argv)
     n = a.n
     if a.problem == "periodic":
@@ -34,6 +37,18 @@ def main(argv=None):
     pf = 1 if prec == B.MIXED else 0
     g = B.BBMG(n, n, n, pb.xper, pb.yper, pb.zper, method=B.PCG_BBOX, precision=prec)
     g.setup(pb.stc, pb.opr)
+    if a.setup:
+        import torch
+        dopr = torch.from_numpy(pb.opr).cuda()
+        ms = []
+        for _ in range(a.reps):
+            g.setup(pb.stc, dopr)
+            ms.append(g.info["setup_ms"])
+        ms.sort()
+        print(json.dumps({"n": n, "precision": a.precision, "setup_ms_median": ms[len(ms) // 2],
+                          "setup_ms_min": ms[0]}))
+        g.close()
+        return
     if a.cycle:
         print(json.dumps({"n": n, "cycle": a.cycle, "ms": g.profile("cycle", a.cycle, 0, pf, a.reps)}))
         g.close()
