@@ -1,13 +1,15 @@
 // unet.cu -- kernels of the learned initial guess (a small 3-D U-Net).
 //
 // No counterpart in the reference (NGA2 starts each pressure solve from the
-// previous pressure).  The 3x3x3 convolutions are implicit GEMMs on the
-// tensor cores: M = voxels, N = output channels, K = 27 taps x input
-// channels, BF16 operands, FP32 accumulation (mma.sync m16n8k16).  A warp owns
-// 16 consecutive voxels and all output channels; its A fragments are the
-// tap-shifted input rows (periodic wrap), its B fragments the packed weights.
-// The weight gradient is a reduction over voxels done on the CUDA cores with
-// shared-memory staging; everything else is elementwise.
+// previous pressure).  The 3x3x3 convolutions (forward and data gradient) are
+// implicit GEMMs on the tensor cores: M = voxels, N = output channels, K = 27
+// taps x input channels, BF16 operands, FP32 accumulation.  Grids of whole
+// 128-voxel tiles run on tcgen05 (k_conv3_tcg: TMEM accumulator, cp.async
+// stage ring, one thread issuing the MMAs); other sizes on mma.sync m16n8k16
+// (k_conv3: a warp owns 16 consecutive voxels and all output channels, its A
+// fragments the tap-shifted input rows with periodic wrap, its B fragments the
+// packed weights).  The weight gradient is a reduction over voxels done on the
+// CUDA cores with shared-memory staging; everything else is elementwise.
 #include <cuda_bf16.h>
 #include <cstdint>
 #include <cstdlib>
@@ -115,24 +117,27 @@ __global__ void __launch_bounds__(128) k_conv3(Act x, const bf16 *__restrict__ w
 }
 
 // ---------------------------------------------------------------------------
-// The same convolution on the fifth-generation tensor cores (tcgen05), for
-// grids whose rows hold a multiple of 128 voxels.  One CTA computes a tile of
-// 128 consecutive voxels of one (n, d, h) row against all output channels:
-//   * the 9 input rows (d+dz, h+dy) of the tile with their x-halo (130 voxels,
-//     periodic wrap) are staged once in shared memory in the K-major canonical
-//     layout of the MMA (no swizzle): for each group of 8 channels, the 130
-//     voxels' 16-byte chunks one after another.  A tap (dz, dy, dx) is then
-//     just a descriptor whose start address is shifted by dx chunks;
-//   * the packed weights [tap][cout][cin] are staged as [tap][K-chunk][group of
-//     8 channels][cout][16 bytes];
-//   * one thread issues 27 x cin/16 tcgen05.mma (M = 128, N = cout, K = 16,
-//     BF16 x BF16 -> FP32) into a TMEM accumulator of cout columns, then
-//     tcgen05.commit arrives on an mbarrier;
-//   * the four warps read their 32 TMEM lanes (= 32 voxels) with tcgen05.ld,
-//     add the bias, apply the ReLU and store BF16 rows.
-// The mbarrier wait is bounded: a wait that runs out raises *err, the CTA still
-// frees its TMEM and returns.
+// The same convolution on the fifth-generation tensor cores (tcgen05): an
+// implicit GEMM with M = 128 consecutive voxels per CTA (one or more (h, w)
+// rows, or part of one), N = all output channels, K = 27 taps x cin.
+//   * K is walked in units of 16 channels (of one tap, or of one input row
+//     for three taps, below); a few units form a pipeline stage.  A stage holds the A tile (the 128 voxels' tap-shifted
+//     input channels, periodic wrap: thread m copies voxel m's two 16-byte
+//     chunks per step) and the B tile (the packed weights [tap][cout][cin] of
+//     those steps), both in the K-major no-swizzle canonical layout of the
+//     MMA: per 8-channel group, rows of 16 bytes one after another (A:
+//     [step][group][voxel][16 B], B: [step][group][cout][16 B]).
+//   * kTgS stages form a ring filled with cp.async kTgS-1 stages ahead; one
+//     thread issues the tcgen05.mma (M = 128, N = cout, K = 16, BF16 x BF16 ->
+//     FP32 in TMEM) of a stage and commits them to that stage's mbarrier; a
+//     stage is refilled once its mbarrier shows the MMAs reading it are done.
+//   * after the last stage the four warps read their 32 TMEM lanes (= 32
+//     voxels) with tcgen05.ld, add the bias, apply the ReLU, store BF16.
+// Every mbarrier wait is bounded: a wait that runs out raises *err (read by
+// nn_tc_error), and the CTA then drains its copies, frees its TMEM and
+// returns without writing.
 constexpr unsigned kTcSpinLimit = 1u << 22;
+constexpr int kTgS = 4;   // pipeline stages
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -155,88 +160,180 @@ __host__ __device__ constexpr uint32_t umma_idesc_bf16(int n) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
 }
 
-template <int N>
-__global__ void __launch_bounds__(128, 1) k_conv3_tc(Act x, const bf16 *__restrict__ wt, const float *__restrict__ bias,
-                                                     Act y, int relu, int *err) {
+// bounded wait for the completion of phase `parity` of an mbarrier
+__device__ __forceinline__ bool mbar_wait(const uint64_t *mb, unsigned parity) {
+    for (unsigned spins = 0; spins < kTcSpinLimit; spins++) {
+        unsigned done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done) : "r"(smem_u32(mb)), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// Two tilings.  ROW (rows of a multiple of 128 voxels): a tile is 128
+// consecutive voxels of one (n, d, h) row, and a K unit is one (dz, dy) input
+// row with its x-halo (130 voxels) for 16 channels: it is staged once and
+// serves the three dx taps through descriptors shifted by one 16-byte row
+// (three MMAs per unit).  Otherwise a tile is 128 consecutive voxels of the
+// grid (several rows when w < 128) and a K unit is one tap's 16 channels of
+// the 128 voxels (one MMA).
+template <int N, bool ROW>
+struct TgCfg {
+    static constexpr int kCols = N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));  // TMEM columns
+    static constexpr int VOX = ROW ? 130 : 128;         // A rows staged per unit
+    static constexpr int TAPS = ROW ? 3 : 1;            // MMAs (taps) per unit
+    static constexpr int KU = ROW ? 2 : 4;              // units per stage
+    static constexpr int A_UNIT = 2 * VOX * 16;         // bytes: [group][voxel][16 B]
+    static constexpr int B_UNIT = TAPS * 2 * N * 16;    // bytes: [tap][group][cout][16 B]
+    static constexpr int A_BYTES = KU * A_UNIT;
+    static constexpr int B_BYTES = KU * B_UNIT;
+    static constexpr size_t SMEM = 128 + (size_t)kTgS * (A_BYTES + B_BYTES);
+};
+
+template <int N, bool ROW>
+__global__ void __launch_bounds__(128) k_conv3_tcg(Act x, const bf16 *__restrict__ wt, const float *__restrict__ bias,
+                                                    Act y, int relu, int *err) {
+    using Cfg = TgCfg<N, ROW>;
     extern __shared__ __align__(128) unsigned char smtc[];
-    constexpr int kCols = N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));  // TMEM columns (power of 2)
     unsigned *tmem_slot = reinterpret_cast<unsigned *>(smtc);
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(smtc + 8);
-    const int cin = x.c, kg = cin >> 3, kc = cin >> 4;
-    unsigned char *A = smtc + 128;                               // [9][kg][130][16 B]
-    unsigned char *B = A + (size_t)9 * kg * 130 * 16;          // [27][kc][2][N][16 B]
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int tiles_per_row = x.w >> 7;
-    const int tile = blockIdx.x;
-    const int w0 = (tile % tiles_per_row) << 7;
-    int rowid = tile / tiles_per_row;  // (n, d, h) row
-    const int h = rowid % x.h;
-    rowid /= x.h;
-    const int d = rowid % x.d, n = rowid / x.d;
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(smtc + 16);  // kTgS barriers
+    unsigned char *A = smtc + 128;
+    unsigned char *B = A + (size_t)kTgS * Cfg::A_BYTES;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int cin = x.c, kpt = cin >> 4;                 // 16-channel blocks
+    const int nu = (ROW ? 9 : 27) * kpt;                 // K units
+    const int nK = (nu + Cfg::KU - 1) / Cfg::KU;         // stages
+    int v0;              // first voxel of the tile
+    int vn[3], vd[3], vh[3], vw[3];
+    const int ag = tid & 1;  // A copies: chunk e = (voxel e/2, group e%2), e = tid + 128 r
+    if constexpr (ROW) {
+        const int tiles_per_row = x.w >> 7;
+        const int w0 = (blockIdx.x % tiles_per_row) << 7;
+        int rowid = blockIdx.x / tiles_per_row;
+        const int h = rowid % x.h;
+        rowid /= x.h;
+        const int d = rowid % x.d, n = rowid / x.d;
+        v0 = vox(x, n, d, h, w0);
+#pragma unroll
+        for (int u = 0; u < 3; u++) {  // halo voxel (tid>>1) + 64u of the row, x-wrapped
+            vn[u] = n; vd[u] = d; vh[u] = h;
+            vw[u] = wrapi(w0 - 1 + (tid >> 1) + 64 * u, x.w);
+        }
+    } else {
+        v0 = blockIdx.x * 128;
+#pragma unroll
+        for (int u = 0; u < 2; u++) decode(x, v0 + (tid >> 1) + 64 * u, vn[u], vd[u], vh[u], vw[u]);
+    }
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(kCols));
+                     "r"(Cfg::kCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
-    if (tid == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)));
-    // stage the weights: chunk (tap, c, g, o) <- wt[tap][o][16c + 8g .. +8]
-    const int nw = 27 * kc * 2 * N;
-    for (int e = tid; e < nw; e += 128) {
-        const int o = e % N, r = e / N, g = r & 1, c = (r >> 1) % kc, tap = (r >> 1) / kc;
-        cpa16(B + (size_t)e * 16, wt + ((size_t)tap * N + o) * cin + c * 16 + g * 8);
+    if (tid == 0)
+        for (int s = 0; s < kTgS; s++) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar + s)));
+
+    // stage `chunk` (units chunk*KU ..) into ring slot `s`
+    auto load = [&](int chunk, int s) {
+        unsigned char *As = A + (size_t)s * Cfg::A_BYTES, *Bs = B + (size_t)s * Cfg::B_BYTES;
+#pragma unroll
+        for (int j = 0; j < Cfg::KU; j++) {
+            const int un = chunk * Cfg::KU + j;
+            if (un >= nu) break;
+            int dz, dy, dx0, cb;  // the unit's row (and tap) and channel block
+            if constexpr (ROW) {
+                const int rr = un / kpt;
+                cb = un - rr * kpt;
+                dz = rr / 3 - 1; dy = rr % 3 - 1; dx0 = 0;
+            } else {
+                const int tap = un / kpt;
+                cb = un - tap * kpt;
+                dz = tap / 9 - 1; dy = (tap / 3) % 3 - 1; dx0 = tap % 3 - 1;
+            }
+#pragma unroll
+            for (int u = 0; u < (ROW ? 3 : 2); u++) {
+                const int vv = (tid >> 1) + 64 * u;  // A row of this copy
+                if (ROW && vv >= Cfg::VOX) break;
+                const bf16 *src = x.p +
+                                  (long long)vox(x, vn[u], wrapi(vd[u] + dz, x.d), wrapi(vh[u] + dy, x.h),
+                                                 ROW ? vw[u] : wrapi(vw[u] + dx0, x.w)) * x.ld + cb * 16 + ag * 8;
+                cpa16(As + (size_t)j * Cfg::A_UNIT + ((size_t)ag * Cfg::VOX + vv) * 16, src);
+            }
+            for (int e = tid; e < Cfg::TAPS * 2 * N; e += 128) {
+                const int t3 = e / (2 * N), r2 = e - t3 * 2 * N, g = r2 / N, o = r2 - g * N;
+                const int tap = ROW ? (dz + 1) * 9 + (dy + 1) * 3 + t3 : (dz + 1) * 9 + (dy + 1) * 3 + dx0 + 1;
+                cpa16(Bs + (size_t)j * Cfg::B_UNIT + ((size_t)(t3 * 2 + g) * N + o) * 16,
+                      wt + ((long long)tap * N + o) * cin + cb * 16 + g * 8);
+            }
+        }
+    };
+    auto commit_group = []() { asm volatile("cp.async.commit_group;" ::: "memory"); };
+
+#pragma unroll 1
+    for (int p = 0; p < kTgS - 1; p++) {
+        if (p < nK) load(p, p);
+        commit_group();
     }
-    // stage the 9 input rows with their x-halo
-    const int na = 9 * kg * 130;
-    for (int e = tid; e < na; e += 128) {
-        const int vv = e % 130, r = e / 130, g = r % kg, rr = r / kg;
-        const int dz = rr / 3 - 1, dy = rr % 3 - 1;
-        const int dd = wrapi(d + dz, x.d), hh = wrapi(h + dy, x.h), ww = wrapi(w0 - 1 + vv, x.w);
-        cpa16(A + (size_t)e * 16, x.p + (size_t)vox(x, n, dd, hh, ww) * x.ld + g * 8);
-    }
-    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
+    __syncthreads();  // barrier inits and the TMEM address are visible
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const unsigned tmem = *reinterpret_cast<volatile unsigned *>(tmem_slot);
-
-    if (tid == 0) {
-        const unsigned abase = smem_u32(A), bbase = smem_u32(B);
-        const uint32_t idesc = umma_idesc_bf16(N);
-        int first = 1;
-        for (int rr = 0; rr < 9; rr++)
-            for (int dx = 0; dx < 3; dx++)
-                for (int c = 0; c < kc; c++) {
-                    const int tap = rr * 3 + dx;
-                    const uint64_t ad = umma_desc(abase + ((rr * kg + 2 * c) * 130 + dx) * 16, 130 * 16, 128);
-                    const uint64_t bd = umma_desc(bbase + ((tap * kc + c) * 2) * N * 16, N * 16, 128);
+    const uint32_t idesc = umma_idesc_bf16(N);
+    bool ok = true;
+#pragma unroll 1
+    for (int k = 0; k < nK; k++) {
+        const int s = k % kTgS;
+        asm volatile("cp.async.wait_group %0;" ::"n"(kTgS - 2) : "memory");  // stage k has landed
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");          // visible to the tensor core
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const unsigned as = smem_u32(A + (size_t)s * Cfg::A_BYTES), bs = smem_u32(B + (size_t)s * Cfg::B_BYTES);
+#pragma unroll 1
+            for (int j = 0; j < Cfg::KU; j++) {
+                const int un = k * Cfg::KU + j;
+                if (un >= nu) break;
+#pragma unroll
+                for (int t3 = 0; t3 < Cfg::TAPS; t3++) {
+                    // ROW: tap dx = t3 - 1 reads the halo row shifted by t3 voxels
+                    const uint64_t ad = umma_desc(as + j * Cfg::A_UNIT + t3 * 16, Cfg::VOX * 16, 128);
+                    const uint64_t bd = umma_desc(bs + j * Cfg::B_UNIT + t3 * 2 * N * 16, N * 16, 128);
                     asm volatile(
                         "{\n\t.reg .pred p;\n\t"
                         "setp.ne.b32 p, %4, 0;\n\t"
                         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n"
-                        ::"r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(first ? 0 : 1), "r"(0));
-                    first = 0;
+                        ::"r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"((un > 0 || t3 > 0) ? 1 : 0), "r"(0));
                 }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mbar))
-                     : "memory");
-    }
-    // wait for the accumulator (bounded)
-    unsigned done = 0, spins = 0;
-    while (!done) {
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done) : "r"(smem_u32(mbar)) : "memory");
-        if (!done && ++spins > kTcSpinLimit) {
-            if (lane == 0) atomicExch(err, 1);
-            break;
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         ::"r"(smem_u32(mbar + s)) : "memory");
         }
+        const int nk = k + kTgS - 1;  // the stage to fill next, in the slot stage k-1 used
+        if (nk < nK) {
+            if (k >= 1) {
+                const bool done = mbar_wait(mbar + nk % kTgS, ((k - 1) / kTgS) & 1);
+                if (__syncthreads_or(!done)) {
+                    ok = false;
+                    break;
+                }
+            }
+            load(nk, nk % kTgS);
+        }
+        commit_group();
     }
+    bool done = false;
+    if (ok) done = mbar_wait(mbar + (nK - 1) % kTgS, ((nK - 1) / kTgS) & 1);
+    if (__syncthreads_or(!done)) {
+        done = false;
+        if (tid == 0) atomicExch(err, 1);
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (done) {
-        const int m = warp * 32 + lane;  // TMEM lane = tile row = voxel
-        const long long v = (long long)vox(x, n, d, h, w0 + m);
+        const long long v = v0 + tid;  // TMEM lane = tile row = voxel
 #pragma unroll
         for (int c0 = 0; c0 < N; c0 += 16) {
             unsigned r[16];
@@ -262,7 +359,7 @@ __global__ void __launch_bounds__(128, 1) k_conv3_tc(Act x, const bf16 *__restri
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::kCols));
 }
 
 int *tc_err_flag() {
@@ -271,40 +368,50 @@ int *tc_err_flag() {
     return flag;
 }
 
+// the tcgen05 path: whole 128-voxel tiles, 16-byte aligned channel rows, and
+// an output width the kernel is instantiated for
 bool tc_eligible(const Act &x, const Act &y) {
     static const bool off = getenv("BBMG_NO_TCGEN05") != nullptr;
-    if (off || x.w % 128 || x.c % 16 || (y.c != 16 && y.c != 32 && y.c != 48 && y.c != 64)) return false;
-    if (x.ld % 8 || y.ld % 8 || (reinterpret_cast<uintptr_t>(x.p) & 15) || (reinterpret_cast<uintptr_t>(y.p) & 15))
-        return false;
-    const size_t smem = 128 + (size_t)9 * (x.c / 8) * 130 * 16 + (size_t)27 * x.c * y.c * 2;
-    return smem <= 200 * 1024;
+    if (off || x.nvox % 128 || x.c % 16) return false;
+    if (y.c != 16 && y.c != 32 && y.c != 48 && y.c != 64 && y.c != 96 && y.c != 128 && y.c != 192) return false;
+    return !(x.ld % 8 || y.ld % 8 || (reinterpret_cast<uintptr_t>(x.p) & 15) || (reinterpret_cast<uintptr_t>(y.p) & 15));
 }
 
-template <int N>
-int launch_conv_tc(const Act &x, const bf16 *wt, const float *bias, const Act &y, int relu, cudaStream_t s) {
-    const size_t smem = 128 + (size_t)9 * (x.c / 8) * 130 * 16 + (size_t)27 * x.c * N * 2;
+template <int N, bool ROW>
+int launch_conv_tc_t(const Act &x, const bf16 *wt, const float *bias, const Act &y, int relu, cudaStream_t s) {
+    using Cfg = TgCfg<N, ROW>;
     static bool attr = false;
     if (!attr) {
-        if (cudaFuncSetAttribute(k_conv3_tc<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess)
+        if (cudaFuncSetAttribute(k_conv3_tcg<N, ROW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM) !=
+            cudaSuccess)
             return BBMG_CUDA;
         attr = true;
     }
     int *err = tc_err_flag();
     if (!err) return BBMG_NO_MEMORY;
-    const int tiles = (x.nvox >> 7);
-    k_conv3_tc<N><<<tiles, 128, smem, s>>>(x, wt, bias, y, relu, err);
+    k_conv3_tcg<N, ROW><<<x.nvox / 128, 128, Cfg::SMEM, s>>>(x, wt, bias, y, relu, err);
     return done(cudaGetLastError());
+}
+
+template <int N>
+int launch_conv_tc(const Act &x, const bf16 *wt, const float *bias, const Act &y, int relu, cudaStream_t s) {
+    static const bool no_rows = getenv("BBMG_NO_TC_ROWS") != nullptr;
+    return (x.w % 128 == 0 && !no_rows) ? launch_conv_tc_t<N, true>(x, wt, bias, y, relu, s)
+                                        : launch_conv_tc_t<N, false>(x, wt, bias, y, relu, s);
 }
 
 int launch_conv(const Act &x, const bf16 *wt, const float *bias, const Act &y, int relu, cudaStream_t s) {
     const int blocks = (x.nvox + 63) / 64;
-    // rows of a multiple of 128 voxels: the tcgen05 kernel
+    // whole 128-voxel tiles: the tcgen05 kernel
     if (tc_eligible(x, y)) {
         switch (y.c) {
         case 16: return launch_conv_tc<16>(x, wt, bias, y, relu, s);
         case 32: return launch_conv_tc<32>(x, wt, bias, y, relu, s);
         case 48: return launch_conv_tc<48>(x, wt, bias, y, relu, s);
         case 64: return launch_conv_tc<64>(x, wt, bias, y, relu, s);
+        case 96: return launch_conv_tc<96>(x, wt, bias, y, relu, s);
+        case 128: return launch_conv_tc<128>(x, wt, bias, y, relu, s);
+        case 192: return launch_conv_tc<192>(x, wt, bias, y, relu, s);
         }
     }
     // output widths of the U-Net: 16/32/64/128 forward; the data gradients
@@ -437,6 +544,18 @@ __global__ void k_up2(Act x, Act y) {
         int nn, d, h, w;
         decode(y, v, nn, d, h, w);
         y.p[(long long)v * y.ld + c] = x.p[(long long)vox(x, nn, d >> 1, h >> 1, w >> 1) * x.ld + c];
+    }
+}
+// the same, 8 channels (16 bytes) per thread, for 16-byte aligned views
+__global__ void k_up2_v8(Act x, Act y) {
+    const int g8 = y.c >> 3;
+    const long long n = (long long)y.nvox * g8;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const int v = (int)(e / g8), c = 8 * (int)(e - (long long)v * g8);
+        int nn, d, h, w;
+        decode(y, v, nn, d, h, w);
+        *reinterpret_cast<uint4 *>(y.p + (long long)v * y.ld + c) =
+            *reinterpret_cast<const uint4 *>(x.p + (long long)vox(x, nn, d >> 1, h >> 1, w >> 1) * x.ld + c);
     }
 }
 // dx (half the size of dy) = sum of the 8 children of dy
@@ -658,8 +777,13 @@ int nn_pool2_bwd(const nn_act *dy, const nn_act *dx, int accumulate, void *strea
 }
 int nn_up2(const nn_act *x, const nn_act *y, void *stream) {
     if (bad_act(x) || bad_act(y) || !halves(y, x)) return BBMG_BAD_ARGS;
-    const Act b = act_of(y);
-    k_up2<<<grid_elems((long long)b.nvox * b.c), 256, 0, (cudaStream_t)stream>>>(act_of(x), b);
+    const Act a = act_of(x), b = act_of(y);
+    const bool v8 = b.c % 8 == 0 && a.ld % 8 == 0 && b.ld % 8 == 0 && !(reinterpret_cast<uintptr_t>(a.p) & 15) &&
+                    !(reinterpret_cast<uintptr_t>(b.p) & 15);
+    if (v8)
+        k_up2_v8<<<grid_elems((long long)b.nvox * (b.c >> 3)), 256, 0, (cudaStream_t)stream>>>(a, b);
+    else
+        k_up2<<<grid_elems((long long)b.nvox * b.c), 256, 0, (cudaStream_t)stream>>>(a, b);
     return done(cudaGetLastError());
 }
 int nn_up2_bwd(const nn_act *dy, const nn_act *dx, void *stream) {

@@ -395,13 +395,17 @@ def test_learned_guess_on_turbulence_sequence():
     assert np.mean(its1) <= np.mean(its0), (its0, its1)
 
 
-@pytest.mark.parametrize("cin,cout,relu,dgrad", [(16, 16, 1, False), (48, 16, 0, False), (16, 32, 1, False),
-                                                 (16, 64, 0, False), (16, 48, 0, True)])
-def test_tcgen05_convolution(L, cin, cout, relu, dgrad):
-    """Rows of 128 voxels take the tcgen05 path (TMEM accumulator): forward and
-    data-gradient convolutions against the oracle, and no completion timeout."""
+@pytest.mark.parametrize("cin,cout,relu,dgrad,shape", [
+    (16, 16, 1, False, (1, 3, 2, 128)), (48, 16, 0, False, (1, 3, 2, 128)), (16, 32, 1, False, (1, 3, 2, 128)),
+    (16, 64, 0, False, (1, 3, 2, 128)), (16, 48, 0, True, (1, 3, 2, 128)),
+    # tiles spanning several rows (w = 32, 16), half a row (w = 256), the U-Net's widest layers
+    (96, 32, 1, False, (1, 4, 4, 32)), (192, 64, 0, False, (2, 2, 4, 16)), (64, 128, 1, False, (1, 2, 2, 256)),
+    (128, 128, 0, False, (1, 4, 4, 8)), (32, 96, 0, True, (1, 4, 4, 32)), (64, 192, 0, True, (1, 4, 8, 8))])
+def test_tcgen05_convolution(L, cin, cout, relu, dgrad, shape):
+    """Grids of whole 128-voxel tiles take the tcgen05 path (TMEM accumulator,
+    staged K ring): forward and data-gradient convolutions against the oracle,
+    and no completion timeout."""
     rng = np.random.default_rng(100 + cin + cout)
-    shape = (1, 3, 2, 128)
     n, d, h, w = shape
     if dgrad:   # dy has cin channels, dx the forward's input channels (cout here)
         dy = bf(rng.standard_normal((n, cin, d, h, w)))
