@@ -305,7 +305,10 @@ def test_learned_guess_saves_iterations():
     """Train on the first steps of a drop sequence the plain GPU multigrid
     generates, then solve the following steps from the network's guess and
     from zero (NGA2's choice) to the same max|b - A x| <= 1e-10 max|b|; the
-    plain warm start (the previous solve's solution) is measured beside it."""
+    plain warm start (the previous solve's solution) is measured beside it.
+    The network predicts the change from the warm start, so its guess must be
+    at least about as close to the solution as the warm start (within 5 %),
+    and it must not need more iterations than the warm start."""
     torch.manual_seed(0)
     n = 32
     seq = SQ.DropSequence(n, seed=11, ndrops=10, rmin=3.0 / n, rmax=6.0 / n, device="cuda")
@@ -319,7 +322,7 @@ def test_learned_guess_saves_iterations():
     assert np.mean(losses[-50:]) < 0.5 * np.mean(losses[:20])
     h = solve.handle
     h.set_residual_norm(B.NORM_RHS)
-    its0, its1, itsw = [], [], []
+    its0, its1, itsw, errw, errl = [], [], [], [], []
     for rec in test_recs:
         h.setup(SQ_STC(), rec["opr"].contiguous())
         b = rec["rhs"].contiguous()
@@ -330,6 +333,9 @@ def test_learned_guess_saves_iterations():
         x1 = torch.empty_like(b)
         guess.guess(rec, x1)
         torch.cuda.synchronize()
+        dp = rec["dp"] - rec["dp"].mean()
+        errw.append(float((rec["p_prev"] - rec["p_prev"].mean() - dp).norm() / dp.norm()))
+        errl.append(float((x1 - x1.mean() - dp).norm() / dp.norm()))
         _, it1, rerr1, st1 = h.solve(b, x1)
         assert st0 == 0 and st1 == 0 and stw == 0
         # all stop at the same absolute residual: check it in FP64 here
@@ -340,8 +346,10 @@ def test_learned_guess_saves_iterations():
         its0.append(it0)
         its1.append(it1)
         itsw.append(itw)
-    print("iterations zero / warm / learned:", its0, itsw, its1)
+    print("iterations zero / warm / learned:", its0, itsw, its1, "errors warm / learned:", errw, errl)
     assert np.mean(its1) < np.mean(its0), (its0, its1)
+    assert np.mean(its1) <= np.mean(itsw), (itsw, its1)
+    assert np.mean(errl) <= 1.05 * np.mean(errw), (errw, errl)
 
 
 def SQ_STC():
