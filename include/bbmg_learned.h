@@ -46,7 +46,9 @@ int nn_tc_error(void);
 int nn_conv3_dgrad(const nn_act *dy, const void *wd, const nn_act *dx, void *stream);
 
 /* dw[tap][cin][cout] += sum_v x(v + tap) dy(v) and db[cout] += sum_v dy(v)
- * (FP32 accumulation; dw/db are accumulated into, zero them first). */
+ * (FP32 accumulation; dw/db are accumulated into, zero them first).  On the
+ * tensor cores (mma.sync, BF16 products) when cin % 16 == 0, cout % 8 == 0 and
+ * the channel rows are 16-byte aligned; on the CUDA cores otherwise. */
 int nn_conv3_wgrad(const nn_act *x, const nn_act *dy, float *dw, float *db, void *stream);
 
 /* FP32 master weights [27][cin][cout] -> BF16 forward ([27][cout][cin]) and

@@ -8,8 +8,9 @@
 // stage ring, one thread issuing the MMAs); other sizes on mma.sync m16n8k16
 // (k_conv3: a warp owns 16 consecutive voxels and all output channels, its A
 // fragments the tap-shifted input rows with periodic wrap, its B fragments the
-// packed weights).  The weight gradient is a reduction over voxels done on the
-// CUDA cores with shared-memory staging; everything else is elementwise.
+// packed weights).  The weight gradient, a contraction over voxels, runs on
+// mma.sync with ldmatrix.trans fragments (k_wgrad_mma); everything else is
+// elementwise.
 #include <cuda_bf16.h>
 #include <cstdint>
 #include <cstdlib>
@@ -490,6 +491,106 @@ __global__ void __launch_bounds__(256) k_wgrad(Act x, Act gy, float *__restrict_
     if (db && tap == 13 && blockIdx.z == 0 && threadIdx.x < cout) atomicAdd(&db[threadIdx.x], accb);
 }
 
+// Weight gradient on the tensor cores: for one tap, dW[ci][co] = sum over
+// voxels v of x(v + tap, ci) dy(v, co) is a GEMM with M = ci, N = co and the
+// voxels as K (mma.sync m16n8k16, BF16 products, FP32 accumulation).  A CTA
+// takes one tap, a chunk of voxels and a group of up to kWgTiles output tiles
+// (16 ci x 8 co); per stage it copies kst voxels' channels (a multiple of 128:
+// tap-shifted x with periodic wrap, and dy) as rows of 16-byte chunks into
+// shared memory, its 8 warps take 16 of the voxels at a time as K steps, and
+// ldmatrix.trans turns
+// the channels-last rows into the A (ci x voxel) and B (voxel x co)
+// fragments.  The warps' partial sums meet in shared memory and go to dw with
+// one atomicAdd per output and CTA; the bias gradient (tap 13, tile group 0)
+// is the column sum of dy.  Rows are padded by 16 bytes, so the eight rows an
+// ldmatrix reads fall in distinct banks.
+constexpr int kWgTiles = 8;   // output tiles (16 x 8) per CTA
+
+__device__ __forceinline__ void ldsm_x4_t(unsigned &r0, unsigned &r1, unsigned &r2, unsigned &r3, const void *p) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3) : "r"(smem_u32(p)));
+}
+__device__ __forceinline__ void ldsm_x2_t(unsigned &r0, unsigned &r1, const void *p) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0,%1}, [%2];" : "=r"(r0), "=r"(r1) : "r"(smem_u32(p)));
+}
+
+__global__ void __launch_bounds__(256) k_wgrad_mma(Act x, Act gy, float *__restrict__ dw, float *__restrict__ db,
+                                                    int vchunk, int kst) {
+    extern __shared__ __align__(16) unsigned char smw[];
+    const int cin = x.c, cout = gy.c, tap = blockIdx.y;
+    const int xs = cin * 2 + 16, gs = cout * 2 + 16;  // padded row strides (bytes)
+    unsigned char *SX = smw;                                     // [kst][xs]
+    unsigned char *SG = SX + (size_t)kst * xs;                   // [kst][gs]
+    float *red = reinterpret_cast<float *>(SG + (size_t)kst * gs);  // [kWgTiles][128]
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t4 = lane & 3;
+    const int nt = cout >> 3, ntiles = (cin >> 4) * nt;
+    const int tile0 = blockIdx.z * kWgTiles, ntl = min(kWgTiles, ntiles - tile0);
+    const int dz = tap / 9 - 1, dyy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+    const int vbeg = blockIdx.x * vchunk, vend = min(vbeg + vchunk, gy.nvox);
+    const bool bias = db && tap == 13 && blockIdx.z == 0;
+    float acc[kWgTiles][4];
+#pragma unroll
+    for (int q = 0; q < kWgTiles; q++) acc[q][0] = acc[q][1] = acc[q][2] = acc[q][3] = 0.f;
+    float accb = 0.f;
+    for (int e = tid; e < kWgTiles * 128; e += 256) red[e] = 0.f;
+    const int cx = cin >> 3, cg = cout >> 3;  // 16-byte chunks per voxel
+    for (int vb = vbeg; vb < vend; vb += kst) {
+        __syncthreads();  // the previous stage is consumed
+        for (int kb = 0; kb < kst; kb += 128) {
+            const int k = kb + (tid & 127), half = tid >> 7, v = vb + k;  // two threads per voxel
+            const bool in = v < vend;
+            long long src = 0;
+            if (in) {
+                int n, d, h, w;
+                decode(gy, v, n, d, h, w);
+                src = (long long)vox(x, n, wrapi(d + dz, x.d), wrapi(h + dyy, x.h), wrapi(w + dx, x.w)) * x.ld;
+            }
+            const uint4 zero = make_uint4(0, 0, 0, 0);
+            for (int c = half; c < cx; c += 2)
+                *reinterpret_cast<uint4 *>(SX + (size_t)k * xs + c * 16) =
+                    in ? *reinterpret_cast<const uint4 *>(x.p + src + c * 8) : zero;
+            for (int c = half; c < cg; c += 2)
+                *reinterpret_cast<uint4 *>(SG + (size_t)k * gs + c * 16) =
+                    in ? *reinterpret_cast<const uint4 *>(gy.p + (long long)v * gy.ld + c * 8) : zero;
+        }
+        __syncthreads();
+        for (int k0 = warp * 16; k0 < kst; k0 += 128) {  // this warp's K steps: voxels k0 .. k0+15
+#pragma unroll
+            for (int q = 0; q < kWgTiles; q++) {
+                if (q >= ntl) break;
+                const int tile = tile0 + q, mb = (tile / nt) * 16, nb = (tile % nt) * 8;
+                unsigned a0, a1, a2, a3, b0, b1;
+                const int mi = lane >> 3, r = lane & 7;
+                ldsm_x4_t(a0, a1, a2, a3, SX + (size_t)(k0 + r + (mi >= 2 ? 8 : 0)) * xs + (mb + (mi & 1) * 8) * 2);
+                ldsm_x2_t(b0, b1, SG + (size_t)(k0 + r + ((lane >> 3) & 1) * 8) * gs + nb * 2);
+                mma16816(acc[q], a0, a1, a2, a3, b0, b1);
+            }
+        }
+        if (bias && tid < cout) {
+            for (int k = 0; k < kst; k++)
+                accb += __bfloat162float(reinterpret_cast<const bf16 *>(SG + (size_t)k * gs)[tid]);
+        }
+    }
+    // the 8 warps' partial tiles -> shared memory -> dw
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < kWgTiles; q++) {
+        if (q >= ntl) break;
+        // D fragment: rows g / g+8, columns 2 t4, 2 t4 + 1 of the 16 x 8 tile
+        atomicAdd(&red[q * 128 + g * 8 + 2 * t4], acc[q][0]);
+        atomicAdd(&red[q * 128 + g * 8 + 2 * t4 + 1], acc[q][1]);
+        atomicAdd(&red[q * 128 + (g + 8) * 8 + 2 * t4], acc[q][2]);
+        atomicAdd(&red[q * 128 + (g + 8) * 8 + 2 * t4 + 1], acc[q][3]);
+    }
+    __syncthreads();
+    for (int e = tid; e < ntl * 128; e += 256) {
+        const int q = e >> 7, m = (e >> 3) & 15, nn = e & 7;
+        const int tile = tile0 + q, ci = (tile / nt) * 16 + m, co = (tile % nt) * 8 + nn;
+        atomicAdd(&dw[((long long)tap * cin + ci) * cout + co], red[e]);
+    }
+    if (bias && tid < cout) atomicAdd(&db[tid], accb);
+}
+
 // ---------------------------------------------------------------------------
 __global__ void k_pack(const float *__restrict__ w, int cin, int cout, bf16 *__restrict__ wt, bf16 *__restrict__ wd) {
     const long long n = 27LL * cin * cout;
@@ -725,6 +826,30 @@ int nn_conv3_wgrad(const nn_act *x, const nn_act *dy, float *dw, float *db, void
         dy->c > 256)
         return BBMG_BAD_ARGS;
     const Act ax = act_of(x), ag = act_of(dy);
+    static const bool no_mma = getenv("BBMG_NO_WGRAD_MMA") != nullptr;
+    // tensor cores: channel counts in whole tiles and 16-byte aligned channel rows
+    if (!no_mma && ax.c % 16 == 0 && ag.c % 8 == 0 && ax.ld % 8 == 0 && ag.ld % 8 == 0 &&
+        !(reinterpret_cast<uintptr_t>(ax.p) & 15) && !(reinterpret_cast<uintptr_t>(ag.p) & 15)) {
+        const int ntiles = (ax.c / 16) * (ag.c / 8), groups = (ntiles + kWgTiles - 1) / kWgTiles;
+        // voxels per stage: 128 x (1..4), up to ~64 KB of staged rows
+        const size_t row = (size_t)(ax.c * 2 + 16 + ag.c * 2 + 16);
+        int kst = 128;
+        while (kst < 512 && (size_t)(2 * kst) * row <= 64 * 1024) kst *= 2;
+        const size_t smem = (size_t)kst * row + sizeof(float) * kWgTiles * 128;
+        static int attr_set = 0;
+        if (smem > 48 * 1024 && !attr_set) {
+            if (cudaFuncSetAttribute(k_wgrad_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess)
+                return BBMG_CUDA;
+            attr_set = 1;
+        }
+        // about eight CTAs per SM in all: voxel chunks of whole stages
+        int nchunk = (148 * 8 + 27 * groups - 1) / (27 * groups);
+        int vchunk = (ag.nvox + nchunk - 1) / nchunk;
+        vchunk = (vchunk + kst - 1) / kst * kst;
+        nchunk = (ag.nvox + vchunk - 1) / vchunk;
+        k_wgrad_mma<<<dim3(nchunk, 27, groups), 256, smem, (cudaStream_t)stream>>>(ax, ag, dw, db, vchunk, kst);
+        return done(cudaGetLastError());
+    }
     const int chunks = 148 * 4 / 27 + 1;
     int vchunk = (ag.nvox + chunks - 1) / chunks;
     vchunk = (vchunk + kWgVB - 1) / kWgVB * kWgVB;
