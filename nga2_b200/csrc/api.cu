@@ -111,7 +111,6 @@ struct bbmg_handle {
     // staging for caller arrays
     double *d_opr_in = nullptr;
     size_t d_opr_in_n = 0;
-    int *d_stc = nullptr;
     double *d_io = nullptr;  // one caller-shaped vector
     size_t io_n = 0;
     bool setup_done = false;
@@ -418,7 +417,7 @@ int bbmg_destroy(bbmg_handle *h) {
     dfree(h->sol); dfree(h->pp); dfree(h->pp2); dfree(h->Ap); dfree(h->x2); dfree(h->b1); dfree(h->sc); dfree(h->part);
     dfree(h->z1); dfree(h->zz);
     dfree(h->dscal);
-    dfree(h->d_opr_in); dfree(h->d_stc); dfree(h->d_io);
+    dfree(h->d_opr_in); dfree(h->d_io);
     if (h->h_scal) cudaFreeHost(h->h_scal);
     h->copier.release();
     if (h->ev0) cudaEventDestroy(h->ev0);
@@ -659,11 +658,6 @@ int bbmg_setup(bbmg_handle *h, int nst, const int *stc, const double *opr) {
         CU(h, h->copier.h2d(h->d_opr_in, opr, sizeof(double) * ncaller * nst, s));
         src = h->d_opr_in;
     }
-    if (!h->d_stc) {
-        int st = dalloc(h, &h->d_stc, 81);
-        if (st) return st;
-    }
-    CU(h, cudaMemcpyAsync(h->d_stc, stc, sizeof(int) * 3 * nst, cudaMemcpyHostToDevice, s));
     // ils scatter + identity overlap + periodic copy (ils_class.f90:247-256, bbmg_class.f90:937-950).
     // Only the planes the stencil touches (and the centre, which carries the
     // overlap's identity) are written; the other planes of the 27-point
@@ -675,15 +669,35 @@ int bbmg_setup(bbmg_handle *h, int nst, const int *stc, const double *opr) {
         CU(h, cudaMemsetAsync(l1.opr27, 0, sizeof(double) * 27 * (size_t)L1.plane, s));
         h->l1_planes = smask;
     }
-    CU(h, setup_scatter(L1, src, nst, g, h->d_stc, l1.opr27, smask, s));
+    CU(h, setup_scatter(L1, src, nst, g, stc, l1.opr27, smask, s));
     CU(h, wrap_planes_mask(L1, l1.opr27, smask, s));
-    // hierarchy (bbmg_class.f90:952-959)
+    const bool mixed = h->prm.precision == BBMG_PREC_MIXED;
+    // the mixed V-cycle's FP32 operators of the coarse levels (27 planes) are
+    // written by the Galerkin product itself
+    if (mixed) {
+        for (int n = 2; n <= h->nlvl; n++) {
+            Level &l = h->lv[n];
+            if (l.oprS32 && l.n32 == 27) continue;
+            if (l.oprS32) {
+                dfree(l.oprS32);
+                h->bytes -= (long long)((size_t)l.n32 * l.L.plane * sizeof(float));
+                l.oprS32 = nullptr;
+                drop_graphs(h);
+            }
+            int st = dalloc(h, &l.oprS32, (size_t)27 * l.L.plane);
+            if (st) return st;
+            l.n32 = 27;
+        }
+    }
+    // hierarchy (bbmg_class.f90:952-959); in mixed precision the FP32 copies
+    // of the prolongation weights and coarse operators come out of the same
+    // kernels
     for (int n = 2; n <= h->nlvl; n++) {
         Level &F = h->lv[n - 1], &C = h->lv[n];
         const unsigned fmask = n == 2 ? smask : 0x7FFFFFFu;
-        CU(h, setup_prolongation(F.L, F.opr27, F.c2f, fmask, s));
+        CU(h, setup_prolongation(F.L, F.opr27, F.c2f, fmask, s, mixed ? F.c2f32 : nullptr));
         CU(h, setup_restriction(F.L, C.L, F.c2f, C.f2c, s));
-        CU(h, setup_operator(F.L, C.L, F.opr27, F.c2f, C.f2c, F.oprc2f, C.opr27, fmask, s));
+        CU(h, setup_operator(F.L, C.L, F.opr27, F.c2f, C.f2c, F.oprc2f, C.opr27, fmask, s, mixed ? C.oprS32 : nullptr));
     }
     // dense coarsest problem (bbmg_class.f90:961, 1307-1385)
     CU(h, setup_direct(h->lv[h->nlvl].L, h->lv[h->nlvl].opr27, h->OP, h->LU, h->piv, h->pinned, h->d_info, s));
@@ -701,7 +715,6 @@ int bbmg_setup(bbmg_handle *h, int nst, const int *stc, const double *opr) {
     const int npt1 = seven ? (sym ? 4 : 7) : 27;
     if (npt1 != h->npt1) drop_graphs(h);
     h->npt1 = npt1;
-    const bool mixed = h->prm.precision == BBMG_PREC_MIXED;
     for (int n = 1; n <= h->nlvl; n++) {
         Level &l = h->lv[n];
         size_t P = (size_t)l.L.plane;
@@ -725,12 +738,6 @@ int bbmg_setup(bbmg_handle *h, int nst, const int *stc, const double *opr) {
                 if (st) return st;
                 l.nS = npt;
             }
-            static const int sym4[4] = {13, 14, 16, 22};
-            for (int q = 0; q < npt; q++) {
-                int slot = npt == 4 ? sym4[q] : k7to27(q);
-                CU(h, cudaMemcpyAsync(l.oprS + q * P, l.opr27 + (size_t)slot * P, sizeof(double) * P,
-                                      cudaMemcpyDeviceToDevice, s));
-            }
         }
         if (l.npt != npt) { l.npt = npt; drop_graphs(h); }
         if (mixed) {
@@ -745,8 +752,15 @@ int bbmg_setup(bbmg_handle *h, int nst, const int *stc, const double *opr) {
                 if (st) return st;
                 l.n32 = npt;
             }
-            CU(h, launch_to_f32(l.oprS, l.oprS32, (long long)npt * P, s));
-            if (n < h->nlvl) CU(h, launch_to_f32(l.c2f, l.c2f32, 8LL * P, s));
+            // levels >= 2 and every c2f32 were written during the hierarchy
+            if (n == 1 && npt == 27) CU(h, launch_to_f32(l.oprS, l.oprS32, 27LL * P, s));
+        }
+        if (npt < 27) {
+            // the level-1 4- or 7-plane storage (and its FP32 copy) in one pass
+            static const int sym4[4] = {13, 14, 16, 22};
+            int slots[7];
+            for (int q = 0; q < npt; q++) slots[q] = npt == 4 ? sym4[q] : k7to27(q);
+            CU(h, setup_solve_planes(l.L, l.opr27, npt, slots, l.oprS, mixed ? l.oprS32 : nullptr, s));
         }
     }
     CU(h, cudaMemcpyAsync(h->h_scal + kScalInfo, h->d_info, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -1010,8 +1024,14 @@ long long bbmg_debug_get(bbmg_handle *h, int n, int which, int prec, double *out
     const Lay &L = h->lv[n].L;
     long long cells = (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
     if (!out) return cells * nc;
-    if (cudaSetDevice(h->device) != cudaSuccess || cudaStreamSynchronize(h->stream) != cudaSuccess)
-        return -fail(h, BBMG_CUDA, "sync");
+    if (cudaSetDevice(h->device) != cudaSuccess) return -fail(h, BBMG_CUDA, "device");
+    // the setup does not fill the overlap of these two (nothing reads it there)
+    if (h->setup_done && which == BBMG_ARR_F2C && n > 1 && fill_overlap_f2c(L, (double *)p, h->stream) != cudaSuccess)
+        return -fail(h, BBMG_CUDA, "overlap");
+    if (h->setup_done && which == BBMG_ARR_OPRC2F && n < h->nlvl &&
+        fill_overlap_oprc2f(L, (double *)p, h->stream) != cudaSuccess)
+        return -fail(h, BBMG_CUDA, "overlap");
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return -fail(h, BBMG_CUDA, "sync");
     size_t es = is32 ? 4 : 8;
     std::vector<char> buf((size_t)nc * L.plane * es);
     if (cudaMemcpy(buf.data(), p, buf.size(), cudaMemcpyDeviceToHost) != cudaSuccess) return -fail(h, BBMG_CUDA, "copy");

@@ -14,14 +14,28 @@ namespace bbmg {
 // Level-1 operator: ils scatter of the caller's nst-point stencil into the
 // 27-point layout (ils_class.f90:247-256), identity in the overlap
 // (bbmg_class.f90:937-949).  src is (nst, nx+2g, ny+2g, nz+2g) Fortran order.
-__global__ void k_scatter_operator(Lay L, const double *__restrict__ src, int nst, int g,
-                                   const int *__restrict__ stc, double *__restrict__ opr, unsigned wmask) {
-    // slot of every caller stencil entry; each slot's value is the sum of its
-    // entries in stencil order, built one slot at a time so the sums stay in
-    // registers
+// caller stencil entries of each q27 slot
+struct ScatterMap {
+    signed char slot[27];  // q27 slot of caller entry st
+    signed char one[27];   // DIRECT form: the caller entry of slot q, -1 if none
+};
+
+// Each slot's value is the sum of the caller's entries that map to it, in
+// stencil order, built one slot at a time so the sums stay in registers.
+// DIRECT: every slot has at most one entry (the usual stencil), so slot q is
+// 0 + src[one[q]] and the loads do not depend on a search.
+template <bool DIRECT>
+__global__ void __launch_bounds__(128, 8) k_scatter_operator(Lay L, const double *__restrict__ src, int nst, int g,
+                                                             ScatterMap map, double *__restrict__ opr,
+                                                             unsigned wmask) {
     __shared__ int qst[27];
-    for (int st = threadIdx.x; st < nst; st += blockDim.x) qst[st] = q27(stc[3 * st], stc[3 * st + 1], stc[3 * st + 2]);
-    __syncthreads();
+    if (!DIRECT) {
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int st = 0; st < 27; st++) qst[st] = map.slot[st];
+        }
+        __syncthreads();
+    }
     long long total = (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
     const long long sx = nst, sy = sx * (L.nx + 2 * g), sz = sy * (L.ny + 2 * g);
     for (long long t = gtid(); t < total; t += gstride()) {
@@ -35,9 +49,13 @@ __global__ void k_scatter_operator(Lay L, const double *__restrict__ src, int ns
             if (!((wmask >> q) & 1u)) continue;
             double o = 0.0;
             if (interior) {
+                if (DIRECT) {
+                    if (map.one[q] >= 0) o = __dadd_rn(o, s[map.one[q]]);
+                } else {
 #pragma unroll 1
-                for (int st = 0; st < nst; st++)
-                    if (qst[st] == q) o = __dadd_rn(o, s[st]);
+                    for (int st = 0; st < nst; st++)
+                        if (qst[st] == q) o = __dadd_rn(o, s[st]);
+                }
             } else if (q == kCentre27) {
                 o = 1.0;
             }
@@ -63,8 +81,16 @@ __global__ void k_wrap(Lay L, double *__restrict__ a, unsigned mask) {
         int si = wrap(L.xper, i, L.nx), sj = wrap(L.yper, j, L.ny), sk = wrap(L.zper, k, L.nz);
         if (si == i && sj == j && sk == k) continue;
         long long d = L.idx(i, j, k), s = L.idx(si, sj, sk);
+        // all loads before the stores: the image is interior and the
+        // destination is not, but the compiler cannot know, and a load after
+        // each store would wait out the previous store's latency
+        double v[27];
+#pragma unroll
         for (int q = 0; q < 27; q++)
-            if ((mask >> q) & 1u) a[q * L.plane + d] = a[q * L.plane + s];
+            if ((mask >> q) & 1u) v[q] = a[q * L.plane + s];
+#pragma unroll
+        for (int q = 0; q < 27; q++)
+            if ((mask >> q) & 1u) a[q * L.plane + d] = v[q];
     }
 }
 __global__ void k_wrap_f(Lay L, float *__restrict__ a, int nplanes) {
@@ -75,9 +101,69 @@ __global__ void k_wrap_f(Lay L, float *__restrict__ a, int nplanes) {
         int si = wrap(L.xper, i, L.nx), sj = wrap(L.yper, j, L.ny), sk = wrap(L.zper, k, L.nz);
         if (si == i && sj == j && sk == k) continue;
         long long d = L.idx(i, j, k), s = L.idx(si, sj, sk);
-        for (int q = 0; q < nplanes; q++) a[q * L.plane + d] = a[q * L.plane + s];
+        float v[27];  // loads first, as in k_wrap
+#pragma unroll
+        for (int q = 0; q < 27; q++)
+            if (q < nplanes) v[q] = a[q * L.plane + s];
+#pragma unroll
+        for (int q = 0; q < 27; q++)
+            if (q < nplanes) a[q * L.plane + d] = v[q];
     }
 }
+// The overlap shell after a kernel that wrote the interior: a shell cell that
+// lies outside in a non-periodic direction is zero, any other takes its
+// periodic image (an interior cell).  The same values as k_zero_shell
+// followed by k_wrap of every plane, in one pass; a32, if given, receives the
+// FP32 copy of what is written.
+__global__ void k_fill_shell(Lay L, double *__restrict__ a, int nplanes, float *__restrict__ a32) {
+    const long long total = shell_cells(L);
+    for (long long t = gtid(); t < total; t += gstride()) {
+        int i, j, k;
+        shell_cell(L, t, i, j, k);
+        const bool out = (!L.xper && (i < 0 || i >= L.nx)) || (!L.yper && (j < 0 || j >= L.ny)) ||
+                         (!L.zper && (k < 0 || k >= L.nz));
+        const long long d = L.idx(i, j, k);
+        if (out) {
+            for (int q = 0; q < nplanes; q++) a[q * L.plane + d] = 0.0;
+            if (a32)
+                for (int q = 0; q < nplanes; q++) a32[q * L.plane + d] = 0.0f;
+            continue;
+        }
+        const long long s = L.idx(wrap(L.xper, i, L.nx), wrap(L.yper, j, L.ny), wrap(L.zper, k, L.nz));
+        double v[27];  // all loads before the stores, as in k_wrap
+#pragma unroll
+        for (int q = 0; q < 27; q++)
+            if (q < nplanes) v[q] = a[q * L.plane + s];
+#pragma unroll
+        for (int q = 0; q < 27; q++)
+            if (q < nplanes) a[q * L.plane + d] = v[q];
+        if (a32) {
+#pragma unroll
+            for (int q = 0; q < 27; q++)
+                if (q < nplanes) a32[q * L.plane + d] = (float)v[q];
+        }
+    }
+}
+
+// Solve-phase planes of a level that keeps fewer than 27 (the level-1 4- or
+// 7-point storage): plane q of oprS is plane slot[q] of the 27-plane opr;
+// oprS32, if given, receives the FP32 copy.  Every element of the arrays
+// (guards and padding included), as a plane-by-plane copy.
+struct PlaneSlots {
+    int n;
+    int slot[7];
+};
+__global__ void k_solve_planes(long long P, const double *__restrict__ opr, PlaneSlots ps, double *__restrict__ oprS,
+                               float *__restrict__ oprS32) {
+    for (long long t = gtid(); t < P; t += gstride()) {
+        for (int q = 0; q < ps.n; q++) {
+            const double v = opr[(long long)ps.slot[q] * P + t];
+            oprS[q * P + t] = v;
+            if (oprS32) oprS32[q * P + t] = (float)v;
+        }
+    }
+}
+
 // zero every plane of the overlap shell (the interior is written by the caller's kernel)
 __global__ void k_zero_shell(Lay L, double *__restrict__ a, int nplanes) {
     const long long total = shell_cells(L);
@@ -96,8 +182,12 @@ __device__ __forceinline__ double sgn_clamp(double a) {
 
 // ---------------------------------------------------------------------------
 // Prolongation, sweep 1: identity and 1-D lines with Shapira lumping
-// (bbmg_class.f90:978-1051).  Every cell including the overlap.
-__global__ void k_prolong_sweep1(Lay L, const double *__restrict__ opr, double *__restrict__ c2f, unsigned mask) {
+// (bbmg_class.f90:978-1051).  Every cell including the overlap.  With
+// `skip_later` (even levels) the face and cube cells that sweeps 2 and 3
+// write in full (every index >= 0) are left to them; c2f32, if given,
+// receives the FP32 copy of what is written.
+__global__ void k_prolong_sweep1(Lay L, const double *__restrict__ opr, double *__restrict__ c2f, unsigned mask,
+                                 bool skip_later, float *__restrict__ c2f32) {
     const double ratio = 10.0;
     long long total = (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
     for (long long t = gtid(); t < total; t += gstride()) {
@@ -105,6 +195,7 @@ __global__ void k_prolong_sweep1(Lay L, const double *__restrict__ opr, double *
         any_cell(L, t, i, j, k);
         long long id = L.idx(i, j, k);
         int n1 = pmod(L.xper, i, L.nx), n2 = pmod(L.yper, j, L.ny), n3 = pmod(L.zper, k, L.nz);
+        if (skip_later && n1 + n2 + n3 >= 2 && i >= 0 && j >= 0 && k >= 0) continue;
         // c2f(0,0,0) and the one line weight (slot sx); every other weight is zero.
         // Scalars rather than an array indexed at run time, so nothing goes to local memory.
         double c0 = 0.0, cx = 0.0;
@@ -114,7 +205,8 @@ __global__ void k_prolong_sweep1(Lay L, const double *__restrict__ opr, double *
             c0 = 1.0;
         } else if (sum == 1) {
             double m = 0.0, z = 0.0, p = 0.0;  // opr1d(-1), opr1d(0), opr1d(+1)
-#pragma unroll 1
+            // unrolled: the loads of all planes can be in flight together
+#pragma unroll
             for (int q = 0; q < 27; q++) {
                 if (!((mask >> q) & 1u)) continue;  // an all-zero plane adds only zeros
                 int li = q % 3 - 1, lj = (q / 3) % 3 - 1, lk = q / 9 - 1;
@@ -136,6 +228,10 @@ __global__ void k_prolong_sweep1(Lay L, const double *__restrict__ opr, double *
         }
 #pragma unroll
         for (int s = 0; s < 8; s++) c2f[s * L.plane + id] = s == 0 ? c0 : (s == sx ? cx : 0.0);
+        if (c2f32) {
+#pragma unroll
+            for (int s = 0; s < 8; s++) c2f32[s * L.plane + id] = (float)(s == 0 ? c0 : (s == sx ? cx : 0.0));
+        }
     }
 }
 
@@ -143,9 +239,12 @@ __global__ void k_prolong_sweep1(Lay L, const double *__restrict__ opr, double *
 // line weights of the in-plane neighbours written by sweep 1.  AXN is the
 // plane normal (0: yz-plane, 1: zx-plane, 2: xy-plane); PA is the in-plane
 // axis of the reference's inner loop, PB that of its outer loop.
+// zinit: the cell's weights start from the zeros sweep 1 would have written
+// (it skipped the cell); c2f32, if given, receives the FP32 copy.
 template <int AXN>
 __device__ __forceinline__ void face_weights(const Lay &L, const double *__restrict__ opr, double *__restrict__ c2f,
-                                             int i, int j, int k, unsigned mask) {
+                                             int i, int j, int k, unsigned mask, bool zinit = false,
+                                             float *__restrict__ c2f32 = nullptr) {
     constexpr int PA = AXN == 0 ? 1 : 0;
     constexpr int PB = AXN == 2 ? 1 : 2;
     const double ratio = 10.0;
@@ -175,7 +274,7 @@ __device__ __forceinline__ void face_weights(const Lay &L, const double *__restr
     const double o00 = sgn_clamp(o2[4]);
     double c[8];
 #pragma unroll
-    for (int t = 0; t < 8; t++) c[t] = c2f[t * L.plane + id];
+    for (int t = 0; t < 8; t++) c[t] = zinit ? 0.0 : c2f[t * L.plane + id];
 #pragma unroll
     for (int lb = -1; lb <= 1; lb++)
 #pragma unroll
@@ -199,6 +298,10 @@ __device__ __forceinline__ void face_weights(const Lay &L, const double *__restr
         }
 #pragma unroll
     for (int t = 0; t < 8; t++) c2f[t * L.plane + id] = c[t];
+    if (c2f32) {
+#pragma unroll
+        for (int t = 0; t < 8; t++) c2f32[t * L.plane + id] = (float)c[t];
+    }
 }
 
 __global__ void k_prolong_sweep2(Lay L, const double *__restrict__ opr, double *__restrict__ c2f, unsigned mask) {
@@ -215,18 +318,14 @@ __global__ void k_prolong_sweep2(Lay L, const double *__restrict__ opr, double *
 }
 
 // Prolongation, sweep 3: cube centres, interior only (bbmg_class.f90:1161-1194).
-__global__ void k_prolong_sweep3(Lay L, const double *__restrict__ opr, double *__restrict__ c2f, unsigned mask) {
-    long long total = (long long)L.nx * L.ny * L.nz;
-    for (long long t = gtid(); t < total; t += gstride()) {
-        int i, j, k;
-        interior_cell(L, t, i, j, k);
-        int n1 = pmod(L.xper, i, L.nx), n2 = pmod(L.yper, j, L.ny), n3 = pmod(L.zper, k, L.nz);
-        if (n1 + n2 + n3 != 3) continue;
+__device__ __forceinline__ void cube_weights(const Lay &L, const double *__restrict__ opr, double *__restrict__ c2f,
+                                             int i, int j, int k, unsigned mask, bool zinit = false,
+                                             float *__restrict__ c2f32 = nullptr) {
         long long id = L.idx(i, j, k);
         double d = sgn_clamp(opr[kCentre27 * L.plane + id]);
         double c[8];
 #pragma unroll
-        for (int s = 0; s < 8; s++) c[s] = c2f[s * L.plane + id];
+        for (int s = 0; s < 8; s++) c[s] = zinit ? 0.0 : c2f[s * L.plane + id];
         // unrolled: every index into c is a compile-time constant (registers)
 #pragma unroll 27
         for (int q = 0; q < 27; q++) {
@@ -247,6 +346,231 @@ __global__ void k_prolong_sweep3(Lay L, const double *__restrict__ opr, double *
         }
 #pragma unroll
         for (int s = 0; s < 8; s++) c2f[s * L.plane + id] = c[s];
+        if (c2f32) {
+#pragma unroll
+            for (int s = 0; s < 8; s++) c2f32[s * L.plane + id] = (float)c[s];
+        }
+}
+
+__global__ void k_prolong_sweep3(Lay L, const double *__restrict__ opr, double *__restrict__ c2f, unsigned mask) {
+    long long total = (long long)L.nx * L.ny * L.nz;
+    for (long long t = gtid(); t < total; t += gstride()) {
+        int i, j, k;
+        interior_cell(L, t, i, j, k);
+        int n1 = pmod(L.xper, i, L.nx), n2 = pmod(L.yper, j, L.ny), n3 = pmod(L.zper, k, L.nz);
+        if (n1 + n2 + n3 != 3) continue;
+        cube_weights(L, opr, c2f, i, j, k, mask);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Even levels (nx, ny, nz all even).  There pmod(i) is the parity of i for
+// every i in [-1, n], periodic or not, so a cell's parity class (i, j, k mod
+// 2) fixes which prolongation sweep writes it and, in the Galerkin products,
+// every loop bound and accumulator slot.  The kernels below enumerate only
+// the cells a sweep updates, and give each parity class its own unrolled code
+// with the accumulators in registers; every sum keeps the reference's order,
+// so the results are the same bits as the generic kernels above (which serve
+// the odd-sized levels).
+
+// Sweep 2, face cells only: the normal index even in [0, n] (the overlap n
+// included), the two in-plane indices odd and interior -- the cells of
+// k_prolong_sweep2 that face_weights does not skip.
+__global__ void k_prolong_sweep2_even(Lay L, const double *__restrict__ opr, double *__restrict__ c2f,
+                                      unsigned mask, float *__restrict__ c2f32) {
+    const long long hx = L.nx / 2, hy = L.ny / 2, hz = L.nz / 2;
+    const long long n0 = (hx + 1) * hy * hz, n1 = hx * (hy + 1) * hz, n2 = hx * hy * (hz + 1);
+    for (long long t = gtid(); t < n0 + n1 + n2; t += gstride()) {
+        if (t < n0) {
+            const long long u = t / (hx + 1);
+            face_weights<0>(L, opr, c2f, (int)(2 * (t % (hx + 1))), (int)(2 * (u % hy) + 1), (int)(2 * (u / hy) + 1),
+                            mask, true, c2f32);
+        } else if (t < n0 + n1) {
+            const long long v = t - n0, u = v / hx;
+            face_weights<1>(L, opr, c2f, (int)(2 * (v % hx) + 1), (int)(2 * (u % (hy + 1))), (int)(2 * (u / (hy + 1)) + 1),
+                            mask, true, c2f32);
+        } else {
+            const long long v = t - n0 - n1, u = v / hx;
+            face_weights<2>(L, opr, c2f, (int)(2 * (v % hx) + 1), (int)(2 * (u % hy) + 1), (int)(2 * (u / hy)), mask,
+                            true, c2f32);
+        }
+    }
+}
+
+// Sweep 3, the interior cells with three odd indices only.
+__global__ void k_prolong_sweep3_even(Lay L, const double *__restrict__ opr, double *__restrict__ c2f,
+                                      unsigned mask, float *__restrict__ c2f32) {
+    const long long hx = L.nx / 2, hy = L.ny / 2, hz = L.nz / 2;
+    for (long long t = gtid(); t < hx * hy * hz; t += gstride()) {
+        const long long u = t / hx;
+        cube_weights(L, opr, c2f, (int)(2 * (t % hx) + 1), (int)(2 * (u % hy) + 1), (int)(2 * (u / hy) + 1), mask, true,
+                     c2f32);
+    }
+}
+
+// A P at one fine cell of parity class (PX, PY, PZ), ap_cell's loops with
+// compile-time bounds (the parity of a neighbour at offset l is that of the
+// cell plus |l|).  SEVEN: the operator has only the centre and the six face
+// planes.  Slots with s = -1 in a direction of odd parity are never reached
+// and never read by R (A P); they are not written (the array is zeroed when
+// allocated and stays zero there).
+template <int PX, int PY, int PZ, bool SEVEN>
+__device__ __forceinline__ void ap_fast(const Lay &F, const double *__restrict__ opr, const double *__restrict__ c2f,
+                                        double *__restrict__ oprc2f, unsigned mask, int fi, int fj, int fk) {
+    const long long id = F.idx(fi, fj, fk);
+    double acc[27];
+#pragma unroll
+    for (int q = 0; q < 27; q++) acc[q] = 0.0;
+#pragma unroll
+    for (int q = 0; q < 27; q++) {
+        const int li = q % 3 - 1, lj = (q / 3) % 3 - 1, lk = q / 9 - 1;
+        if (SEVEN && (li != 0) + (lj != 0) + (lk != 0) > 1) continue;
+        if (!((mask >> q) & 1u)) continue;  // an all-zero plane adds only zeros
+        const int pxl = (PX + (li & 1)) & 1, pyl = (PY + (lj & 1)) & 1, pzl = (PZ + (lk & 1)) & 1;
+        const double o = opr[q * F.plane + id];
+        const long long nid = F.idx(fi + li, fj + lj, fk + lk);
+#pragma unroll 2
+        for (int pk = 0; pk <= pzl; pk++)
+#pragma unroll 2
+            for (int pj = 0; pj <= pyl; pj++)
+#pragma unroll 2
+                for (int pi = 0; pi <= pxl; pi++) {
+                    const int si = pi + (1 - PX) * min(li, 0) + (1 - pxl) * max(li, 0);
+                    const int sj = pj + (1 - PY) * min(lj, 0) + (1 - pyl) * max(lj, 0);
+                    const int sk = pk + (1 - PZ) * min(lk, 0) + (1 - pzl) * max(lk, 0);
+                    const int so = q27(si, sj, sk);
+                    acc[so] = __dadd_rn(acc[so], __dmul_rn(o, c2f[q8(pi, pj, pk) * F.plane + nid]));
+                }
+    }
+#pragma unroll
+    for (int q = 0; q < 27; q++) {
+        const int sx = q % 3 - 1, sy = (q / 3) % 3 - 1, sz = q / 9 - 1;
+        if ((PX && sx < 0) || (PY && sy < 0) || (PZ && sz < 0)) continue;
+        oprc2f[q * F.plane + id] = acc[q];
+    }
+}
+
+template <bool SEVEN>
+__global__ void __launch_bounds__(128) k_rap_ap_even(Lay F, const double *__restrict__ opr,
+                                                     const double *__restrict__ c2f, double *__restrict__ oprc2f,
+                                                     unsigned mask) {
+    long long total = (long long)F.nx * F.ny * F.nz;
+    for (long long t = gtid(); t < total; t += gstride()) {
+        int fi, fj, fk;
+        interior_cell(F, t, fi, fj, fk);
+        switch ((fi & 1) | ((fj & 1) << 1) | ((fk & 1) << 2)) {
+            case 0: ap_fast<0, 0, 0, SEVEN>(F, opr, c2f, oprc2f, mask, fi, fj, fk); break;
+            case 1: ap_fast<1, 0, 0, SEVEN>(F, opr, c2f, oprc2f, mask, fi, fj, fk); break;
+            case 2: ap_fast<0, 1, 0, SEVEN>(F, opr, c2f, oprc2f, mask, fi, fj, fk); break;
+            case 3: ap_fast<1, 1, 0, SEVEN>(F, opr, c2f, oprc2f, mask, fi, fj, fk); break;
+            case 4: ap_fast<0, 0, 1, SEVEN>(F, opr, c2f, oprc2f, mask, fi, fj, fk); break;
+            case 5: ap_fast<1, 0, 1, SEVEN>(F, opr, c2f, oprc2f, mask, fi, fj, fk); break;
+            case 6: ap_fast<0, 1, 1, SEVEN>(F, opr, c2f, oprc2f, mask, fi, fj, fk); break;
+            default: ap_fast<1, 1, 1, SEVEN>(F, opr, c2f, oprc2f, mask, fi, fj, fk); break;
+        }
+    }
+}
+
+// R (A P) at one coarse cell, the 9 output slots with z offset SK.  The fine
+// centre 2c is even, so the fine offsets r run over -1..1 and the A P slots l
+// from -1 + |r| to 1 in every direction; for given r and SK the z slot of A P
+// is lk = SK - (rk - 1) / 2.  Each output slot's contributions come in the
+// reference's (rk, rj, ri) order, a subsequence of k_rap_rap's loop.  A fine
+// cell in the overlap is read at its periodic image (the value the overlap
+// copy would hold there; in a non-periodic direction the overlap of A P is
+// never written and stays zero), so A P's overlap is not filled during the
+// setup.
+template <int SK>
+__device__ __forceinline__ void rap_fast(const Lay &F, const Lay &C, const double *__restrict__ f2c,
+                                         const double *__restrict__ oprc2f, double *__restrict__ oprc,
+                                         float *__restrict__ oprc32, int ci, int cj, int ck) {
+    const int fi = 2 * ci, fj = 2 * cj, fk = 2 * ck;
+    const long long cid = C.idx(ci, cj, ck);
+    double acc[9];
+#pragma unroll
+    for (int q = 0; q < 9; q++) acc[q] = 0.0;
+#pragma unroll
+    for (int rk = -1; rk <= 1; rk++) {
+        const int lk = SK - (rk - 1) / 2;  // (r-1)/2 truncates toward zero, as Fortran's integer division
+        if (lk < -1 + (rk & 1) || lk > 1) continue;
+#pragma unroll
+        for (int rj = -1; rj <= 1; rj++)
+#pragma unroll
+            for (int ri = -1; ri <= 1; ri++) {
+                const double w = f2c[q27(ri, rj, rk) * C.plane + cid];
+                const long long nid = F.idx(wrap(F.xper, fi + ri, F.nx), wrap(F.yper, fj + rj, F.ny),
+                                            wrap(F.zper, fk + rk, F.nz));
+#pragma unroll
+                for (int lj = -1; lj <= 1; lj++) {
+                    if (lj < -1 + (rj & 1)) continue;
+#pragma unroll
+                    for (int li = -1; li <= 1; li++) {
+                        if (li < -1 + (ri & 1)) continue;
+                        const int so = ((ri - 1) / 2 + li + 1) + 3 * ((rj - 1) / 2 + lj + 1);
+                        acc[so] = __dadd_rn(acc[so], __dmul_rn(w, oprc2f[q27(li, lj, lk) * F.plane + nid]));
+                    }
+                }
+            }
+    }
+#pragma unroll
+    for (int q = 0; q < 9; q++) oprc[(q + 9 * (SK + 1)) * C.plane + cid] = acc[q];
+    if (oprc32) {
+#pragma unroll
+        for (int q = 0; q < 9; q++) oprc32[(q + 9 * (SK + 1)) * C.plane + cid] = (float)acc[q];
+    }
+}
+
+// One warp per 32 consecutive coarse cells and one z slot: warp w takes the
+// slot SK = w % 3 - 1 of the cells 32 (w / 3) .. + 31.  oprc32, if given,
+// receives the FP32 copy.
+__global__ void __launch_bounds__(128) k_rap_rap_even(Lay F, Lay C, const double *__restrict__ f2c,
+                                                      const double *__restrict__ oprc2f, double *__restrict__ oprc,
+                                                      float *__restrict__ oprc32) {
+    const long long total = (long long)C.nx * C.ny * C.nz;
+    const long long nw = 3 * ((total + 31) / 32);
+    const int lane = threadIdx.x & 31;
+    for (long long w = gtid() >> 5; w < nw; w += gstride() >> 5) {
+        const long long t = (w / 3) * 32 + lane;
+        if (t >= total) continue;
+        int ci, cj, ck;
+        interior_cell(C, t, ci, cj, ck);
+        switch ((int)(w % 3)) {
+            case 0: rap_fast<-1>(F, C, f2c, oprc2f, oprc, oprc32, ci, cj, ck); break;
+            case 1: rap_fast<0>(F, C, f2c, oprc2f, oprc, oprc32, ci, cj, ck); break;
+            default: rap_fast<1>(F, C, f2c, oprc2f, oprc, oprc32, ci, cj, ck); break;
+        }
+    }
+}
+
+static bool even_level(const Lay &L) { return !(L.nx & 1) && !(L.ny & 1) && !(L.nz & 1); }
+
+// BBMG_GENERIC_SETUP=1 keeps the generic kernels on every level (for timing)
+static bool fast_setup() {
+    static int f = -1;
+    if (f < 0) {
+        const char *e = getenv("BBMG_GENERIC_SETUP");
+        f = (e && atoi(e)) ? 0 : 1;
+    }
+    return f == 1;
+}
+
+// Restriction weights of a coarse cell on an even fine level: every offset
+// r runs over -1..1 (unrolled), so all 27 weights are written.
+__global__ void k_restriction_weights_even(Lay F, Lay C, const double *__restrict__ c2f, double *__restrict__ f2c) {
+    const long long total = (long long)C.nx * C.ny * C.nz;
+    for (long long t = gtid(); t < total; t += gstride()) {
+        int ci, cj, ck;
+        interior_cell(C, t, ci, cj, ck);
+        const int fi = 2 * ci, fj = 2 * cj, fk = 2 * ck;
+        const long long cid = C.idx(ci, cj, ck);
+#pragma unroll
+        for (int rk = -1; rk <= 1; rk++)
+#pragma unroll
+            for (int rj = -1; rj <= 1; rj++)
+#pragma unroll
+                for (int ri = -1; ri <= 1; ri++)
+                    f2c[q27(ri, rj, rk) * C.plane + cid] =
+                        c2f[q8((1 - ri) / 2, (1 - rj) / 2, (1 - rk) / 2) * F.plane + F.idx(fi + ri, fj + rj, fk + rk)];
     }
 }
 
@@ -401,11 +725,10 @@ __global__ void k_dense_operator(Lay L, const double *__restrict__ opr, double *
 // Pivot: the first row holding the largest magnitude.  Then marks the
 // unknowns whose pivot is below 1000*n*eps*max|pivot| (a singular coarsest
 // matrix); the solve sets those to zero.
-__global__ void k_lu(double *__restrict__ A, int n, int *__restrict__ piv, int *__restrict__ pinned,
-                     int *__restrict__ info_out) {
-    __shared__ double sval[1024];
-    __shared__ int sidx[1024];
-    __shared__ int s_info;
+// The factorisation of k_lu on A (global or shared memory), one block; sval
+// and sidx hold blockDim.x entries.
+__device__ __forceinline__ void lu_block(double *A, int n, int *__restrict__ piv, int *__restrict__ pinned,
+                                         int *__restrict__ info_out, double *sval, int *sidx, int &s_info) {
     const int tid = threadIdx.x, nt = blockDim.x;
     if (tid == 0) s_info = 0;
     __syncthreads();
@@ -471,6 +794,32 @@ __global__ void k_lu(double *__restrict__ A, int n, int *__restrict__ piv, int *
     if (tid == 0) *info_out = s_info;
 }
 
+__global__ void k_lu(double *__restrict__ A, int n, int *__restrict__ piv, int *__restrict__ pinned,
+                     int *__restrict__ info_out) {
+    __shared__ double sval[1024];
+    __shared__ int sidx[1024];
+    __shared__ int s_info;
+    lu_block(A, n, piv, pinned, info_out, sval, sidx, s_info);
+}
+
+// The same factorisation with the matrix held in shared memory (n*n*8 bytes
+// plus blockDim.x * 12): the per-column barriers then wait on shared-memory
+// traffic instead of global-memory round trips.
+__global__ void k_lu_smem(double *__restrict__ A, int n, int *__restrict__ piv, int *__restrict__ pinned,
+                          int *__restrict__ info_out) {
+    extern __shared__ __align__(16) unsigned char lu_sm[];
+    double *M = reinterpret_cast<double *>(lu_sm);
+    double *sval = M + (size_t)n * n;
+    int *sidx = reinterpret_cast<int *>(sval + blockDim.x);
+    __shared__ int s_info;
+    const long long nn = (long long)n * n;
+    for (long long e = threadIdx.x; e < nn; e += blockDim.x) M[e] = A[e];
+    __syncthreads();
+    lu_block(M, n, piv, pinned, info_out, sval, sidx, s_info);
+    __syncthreads();
+    for (long long e = threadIdx.x; e < nn; e += blockDim.x) A[e] = M[e];
+}
+
 // ---------------------------------------------------------------------------
 // Exact symmetry of a 7-point level-1 operator: west(c) == east(c - x) etc.
 // for every interior cell whose neighbour is interior or a periodic image
@@ -498,8 +847,23 @@ __global__ void k_check_sym7(Lay L, const double *__restrict__ opr, int *flag) {
 
 cudaError_t setup_scatter(const Lay &L, const double *src, int nst, int g, const int *stc, double *opr, unsigned wmask,
                           cudaStream_t s) {
+    ScatterMap map;
+    int cnt[27] = {0};
+    for (int q = 0; q < 27; q++) map.one[q] = -1;
+    for (int st = 0; st < 27; st++) map.slot[st] = -1;
+    for (int st = 0; st < nst; st++) {
+        const int q = q27h(stc[3 * st], stc[3 * st + 1], stc[3 * st + 2]);
+        map.slot[st] = (signed char)q;
+        map.one[q] = (signed char)st;
+        cnt[q]++;
+    }
+    bool direct = true;
+    for (int q = 0; q < 27; q++) direct = direct && cnt[q] <= 1;
     long long n = (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
-    k_scatter_operator<<<grid_for(n, 128), 128, 0, s>>>(L, src, nst, g, stc, opr, wmask);
+    if (direct)
+        k_scatter_operator<true><<<grid_for(n, 128), 128, 0, s>>>(L, src, nst, g, map, opr, wmask);
+    else
+        k_scatter_operator<false><<<grid_for(n, 128), 128, 0, s>>>(L, src, nst, g, map, opr, wmask);
     BB_LAUNCH_CHECK();
     return cudaSuccess;
 }
@@ -522,46 +886,106 @@ cudaError_t wrap_planes(const Lay &L, float *a, int nplanes, cudaStream_t s) {
     return cudaSuccess;
 }
 
-cudaError_t setup_prolongation(const Lay &L, const double *opr, double *c2f, unsigned mask, cudaStream_t s) {
+cudaError_t setup_prolongation(const Lay &L, const double *opr, double *c2f, unsigned mask, cudaStream_t s,
+                               float *c2f32) {
     long long na = (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
     long long ni = (long long)L.nx * L.ny * L.nz;
-    k_prolong_sweep1<<<grid_for(na, 128), 128, 0, s>>>(L, opr, c2f, mask);
+    cudaError_t e;
+    if (even_level(L) && fast_setup()) {
+        k_prolong_sweep1<<<grid_for(na, 128), 128, 0, s>>>(L, opr, c2f, mask, true, c2f32);
+        BB_LAUNCH_CHECK();
+        const long long hx = L.nx / 2, hy = L.ny / 2, hz = L.nz / 2;
+        const long long nf = (hx + 1) * hy * hz + hx * (hy + 1) * hz + hx * hy * (hz + 1);
+        k_prolong_sweep2_even<<<grid_for(nf, 128), 128, 0, s>>>(L, opr, c2f, mask, c2f32);
+        BB_LAUNCH_CHECK();
+        k_prolong_sweep3_even<<<grid_for(hx * hy * hz, 128), 128, 0, s>>>(L, opr, c2f, mask, c2f32);
+        BB_LAUNCH_CHECK();
+        if ((e = wrap_planes(L, c2f, 8, s)) != cudaSuccess) return e;
+        return c2f32 ? wrap_planes(L, c2f32, 8, s) : cudaSuccess;
+    }
+    k_prolong_sweep1<<<grid_for(na, 128), 128, 0, s>>>(L, opr, c2f, mask, false, nullptr);
     BB_LAUNCH_CHECK();
     k_prolong_sweep2<<<grid_for(na, 128), 128, 0, s>>>(L, opr, c2f, mask);
     BB_LAUNCH_CHECK();
     k_prolong_sweep3<<<grid_for(ni, 128), 128, 0, s>>>(L, opr, c2f, mask);
     BB_LAUNCH_CHECK();
-    return wrap_planes(L, c2f, 8, s);
+    if ((e = wrap_planes(L, c2f, 8, s)) != cudaSuccess) return e;
+    return c2f32 ? launch_to_f32(c2f, c2f32, 8LL * L.plane, s) : cudaSuccess;
 }
 
+// The overlap of f2c is read by nothing in the setup or the solve (the
+// Galerkin product reads the weights of interior coarse cells only); it is
+// filled when the array is read out (fill_overlap_f2c).
 cudaError_t setup_restriction(const Lay &F, const Lay &C, const double *c2f, double *f2c, cudaStream_t s) {
+    long long n = (long long)C.nx * C.ny * C.nz;
+    if (even_level(F) && fast_setup()) {
+        // every interior weight is written; the overlap is zero since the
+        // allocation or its periodic image (written at read-out)
+        k_restriction_weights_even<<<grid_for(n, 128), 128, 0, s>>>(F, C, c2f, f2c);
+        BB_LAUNCH_CHECK();
+        return cudaSuccess;
+    }
     cudaError_t e = cudaMemsetAsync(f2c, 0, sizeof(double) * 27 * C.plane, s);
     if (e != cudaSuccess) return e;
-    long long n = (long long)C.nx * C.ny * C.nz;
     k_restriction_weights<<<grid_for(n, 128), 128, 0, s>>>(F, C, c2f, f2c);
     BB_LAUNCH_CHECK();
-    return wrap_planes(C, f2c, 27, s);
+    return cudaSuccess;
+}
+
+cudaError_t fill_overlap_f2c(const Lay &C, double *f2c, cudaStream_t s) { return wrap_planes(C, f2c, 27, s); }
+
+cudaError_t fill_overlap_oprc2f(const Lay &F, double *oprc2f, cudaStream_t s) {
+    k_fill_shell<<<grid_for(shell_cells(F), 256), 256, 0, s>>>(F, oprc2f, 27, nullptr);
+    BB_LAUNCH_CHECK();
+    return cudaSuccess;
 }
 
 cudaError_t setup_operator(const Lay &F, const Lay &C, const double *oprF, const double *c2f, const double *f2c,
-                           double *oprc2f, double *oprC, unsigned mask, cudaStream_t s) {
-    cudaError_t e;
+                           double *oprc2f, double *oprC, unsigned mask, cudaStream_t s, float *oprC32) {
     // the products are written on every interior cell; the overlap is zero
     // (non-periodic) or the periodic image
     constexpr int nt = 128;
     constexpr size_t smem = 27 * nt * sizeof(double);  // 27 accumulators per thread
-    k_zero_shell<<<grid_for(shell_cells(F), 256), 256, 0, s>>>(F, oprc2f, 27);
-    BB_LAUNCH_CHECK();
     long long nf = (long long)F.nx * F.ny * F.nz;
-    k_rap_ap<<<grid_for(nf, nt), nt, smem, s>>>(F, oprF, c2f, oprc2f, mask);
+    const bool fast = even_level(F) && fast_setup();
+    // the centre and the six face planes only
+    const unsigned seven = (1u << q27h(0, 0, 0)) | (1u << q27h(-1, 0, 0)) | (1u << q27h(1, 0, 0)) |
+                           (1u << q27h(0, -1, 0)) | (1u << q27h(0, 1, 0)) | (1u << q27h(0, 0, -1)) |
+                           (1u << q27h(0, 0, 1));
+    if (fast && !(mask & ~seven))
+        k_rap_ap_even<true><<<grid_for(nf, nt), nt, 0, s>>>(F, oprF, c2f, oprc2f, mask);
+    else if (fast)
+        k_rap_ap_even<false><<<grid_for(nf, nt), nt, 0, s>>>(F, oprF, c2f, oprc2f, mask);
+    else
+        k_rap_ap<<<grid_for(nf, nt), nt, smem, s>>>(F, oprF, c2f, oprc2f, mask);
     BB_LAUNCH_CHECK();
-    if ((e = wrap_planes(F, oprc2f, 27, s)) != cudaSuccess) return e;
-    k_zero_shell<<<grid_for(shell_cells(C), 256), 256, 0, s>>>(C, oprC, 27);
-    BB_LAUNCH_CHECK();
+    if (!fast) {  // k_rap_rap reads A P in the overlap
+        k_fill_shell<<<grid_for(shell_cells(F), 256), 256, 0, s>>>(F, oprc2f, 27, nullptr);
+        BB_LAUNCH_CHECK();
+    }
     long long nc = (long long)C.nx * C.ny * C.nz;
+    if (fast) {
+        k_rap_rap_even<<<grid_for(3 * ((nc + 31) / 32) * 32, nt), nt, 0, s>>>(F, C, f2c, oprc2f, oprC, oprC32);
+        BB_LAUNCH_CHECK();
+        k_fill_shell<<<grid_for(shell_cells(C), 256), 256, 0, s>>>(C, oprC, 27, oprC32);
+        BB_LAUNCH_CHECK();
+        return cudaSuccess;
+    }
     k_rap_rap<<<grid_for(nc, nt), nt, smem, s>>>(F, C, f2c, oprc2f, oprC);
     BB_LAUNCH_CHECK();
-    return wrap_planes(C, oprC, 27, s);
+    k_fill_shell<<<grid_for(shell_cells(C), 256), 256, 0, s>>>(C, oprC, 27, nullptr);
+    BB_LAUNCH_CHECK();
+    return oprC32 ? launch_to_f32(oprC, oprC32, 27LL * C.plane, s) : cudaSuccess;
+}
+
+cudaError_t setup_solve_planes(const Lay &L, const double *opr, int npt, const int *slots, double *oprS,
+                               float *oprS32, cudaStream_t s) {
+    PlaneSlots ps{};
+    ps.n = npt;
+    for (int q = 0; q < npt; q++) ps.slot[q] = slots[q];
+    k_solve_planes<<<grid_for(L.plane, 256), 256, 0, s>>>(L.plane, opr, ps, oprS, oprS32);
+    BB_LAUNCH_CHECK();
+    return cudaSuccess;
 }
 
 cudaError_t check_symmetric7(const Lay &L, const double *opr, int *flag, cudaStream_t s) {
@@ -583,7 +1007,19 @@ cudaError_t setup_direct(const Lay &L, const double *opr, double *OP, double *LU
     BB_LAUNCH_CHECK();
     cudaError_t e = cudaMemcpyAsync(LU, OP, sizeof(double) * (size_t)np * np, cudaMemcpyDeviceToDevice, s);
     if (e != cudaSuccess) return e;
-    k_lu<<<1, 1024, 0, s>>>(LU, np, piv, pinned, info);
+    constexpr int kLuThreads = 256;
+    const size_t lu_smem = (size_t)np * np * sizeof(double) + kLuThreads * (sizeof(double) + sizeof(int));
+    if (lu_smem <= 200 * 1024) {
+        static bool attr = false;
+        if (!attr) {
+            e = cudaFuncSetAttribute(k_lu_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            if (e != cudaSuccess) return e;
+            attr = true;
+        }
+        k_lu_smem<<<1, kLuThreads, lu_smem, s>>>(LU, np, piv, pinned, info);
+    } else {
+        k_lu<<<1, 1024, 0, s>>>(LU, np, piv, pinned, info);
+    }
     BB_LAUNCH_CHECK();
     return cudaSuccess;
 }

@@ -9,16 +9,28 @@ namespace bbmg {
 // setup.cu (FP64)
 // `wmask`/`mask`: 27-bit sets of operator planes (q27 slots); the scatter
 // writes only the planes in wmask (the others hold zeros already), the
-// prolongation and A*P skip planes outside mask (known to be all zero)
+// prolongation and A*P skip planes outside mask (known to be all zero);
+// the scatter's stc is the caller's stencil in host memory
 cudaError_t setup_scatter(const Lay &L, const double *src, int nst, int g, const int *stc, double *opr, unsigned wmask,
                           cudaStream_t s);
 cudaError_t wrap_planes(const Lay &L, double *a, int nplanes, cudaStream_t s);
 cudaError_t wrap_planes_mask(const Lay &L, double *a, unsigned mask, cudaStream_t s);
 cudaError_t wrap_planes(const Lay &L, float *a, int nplanes, cudaStream_t s);
-cudaError_t setup_prolongation(const Lay &L, const double *opr, double *c2f, unsigned mask, cudaStream_t s);
+// c2f32 / oprC32, if given, receive the FP32 copies of the prolongation
+// weights and of the coarse operator (the mixed-precision V-cycle's arrays)
+cudaError_t setup_prolongation(const Lay &L, const double *opr, double *c2f, unsigned mask, cudaStream_t s,
+                               float *c2f32 = nullptr);
 cudaError_t setup_restriction(const Lay &F, const Lay &C, const double *c2f, double *f2c, cudaStream_t s);
 cudaError_t setup_operator(const Lay &F, const Lay &C, const double *oprF, const double *c2f, const double *f2c,
-                           double *oprc2f, double *oprC, unsigned mask, cudaStream_t s);
+                           double *oprc2f, double *oprC, unsigned mask, cudaStream_t s, float *oprC32 = nullptr);
+// the overlap of f2c and of A P (oprc2f) as the reference holds it (zero in
+// non-periodic directions, the periodic image otherwise); the setup leaves it
+// unfilled where nothing reads it, so it is filled before a read-out
+cudaError_t fill_overlap_f2c(const Lay &C, double *f2c, cudaStream_t s);
+cudaError_t fill_overlap_oprc2f(const Lay &F, double *oprc2f, cudaStream_t s);
+// plane q of oprS (and of oprS32, if given) = plane slots[q] of the 27-plane opr, npt <= 7
+cudaError_t setup_solve_planes(const Lay &L, const double *opr, int npt, const int *slots, double *oprS,
+                               float *oprS32, cudaStream_t s);
 cudaError_t check_symmetric7(const Lay &L, const double *opr, int *flag, cudaStream_t s);
 cudaError_t setup_direct(const Lay &L, const double *opr, double *OP, double *LU, int *piv, int *pinned, int *info,
                          cudaStream_t s);

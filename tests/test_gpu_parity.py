@@ -328,6 +328,31 @@ def test_setup_reuse_across_stencils_bitexact():
                 assert np.array_equal(g.get(n, w), o.get(n, w)), (n, w)
 
 
+def test_setup_repeated_stencil_entries_bitexact():
+    """A caller stencil that names a slot more than once (the ils scatter adds
+    the entries of one slot in stencil order, ils_class.f90:247-256): the
+    general form of the scatter; every setup array equals the oracle's."""
+    dims, per = (16, 12, 10), (True, False, True)
+    stc7, opr7 = P.random_operator(*dims, per, seed=21)
+    rng = np.random.default_rng(5)
+    # the centre split in two entries, the east coupling in two, in that order
+    a = rng.uniform(0.2, 0.8, size=opr7.shape[:-1])
+    stc = np.concatenate([stc7, stc7[[0, 1]]]).astype(np.int32)
+    opr = np.concatenate([opr7, np.zeros(opr7.shape[:-1] + (2,))], axis=-1)
+    opr[..., 7] = (1.0 - a) * opr7[..., 0]
+    opr[..., 0] = a * opr7[..., 0]
+    opr[..., 8] = 0.5 * opr7[..., 1]
+    opr[..., 1] = opr7[..., 1] - opr[..., 8]
+    g = BBMG(*dims, *per, method=BBOX)
+    g.setup(stc, opr)
+    o = OracleBBMG(*dims, *per, method=BBOX)
+    o.setup(stc, opr)
+    for n in range(1, o.nlvl + 1):
+        names = ["opr"] + (["c2f", "oprc2f"] if n < o.nlvl else []) + (["f2c"] if n > 1 else [])
+        for w in names:
+            assert np.array_equal(g.get(n, w), o.get(n, w)), (n, w)
+
+
 def test_pageable_host_arrays_match_device():
     """Arrays larger than one 32 MB staging chunk: the operator, rhs and
     solution given as pageable numpy arrays (copied through the pinned staging
