@@ -667,6 +667,9 @@ int bbmg_setup(bbmg_handle *h, int nst, const int *stc, const double *opr) {
     for (int st = 0; st < nst; st++) smask |= 1u << q27(stc[3 * st], stc[3 * st + 1], stc[3 * st + 2]);
     if (smask != h->l1_planes) {
         CU(h, cudaMemsetAsync(l1.opr27, 0, sizeof(double) * 27 * (size_t)L1.plane, s));
+        // A*P of a 7-point level 1 writes only the slots such an operator
+        // reaches; the others must read zero after a 27-point setup
+        if (h->nlvl > 1) CU(h, cudaMemsetAsync(l1.oprc2f, 0, sizeof(double) * 27 * (size_t)L1.plane, s));
         h->l1_planes = smask;
     }
     CU(h, setup_scatter(L1, src, nst, g, stc, l1.opr27, smask, s));

@@ -182,12 +182,8 @@ __device__ __forceinline__ double sgn_clamp(double a) {
 
 // ---------------------------------------------------------------------------
 // Prolongation, sweep 1: identity and 1-D lines with Shapira lumping
-// (bbmg_class.f90:978-1051).  Every cell including the overlap.  With
-// `skip_later` (even levels) the face and cube cells that sweeps 2 and 3
-// write in full (every index >= 0) are left to them; c2f32, if given,
-// receives the FP32 copy of what is written.
-__global__ void k_prolong_sweep1(Lay L, const double *__restrict__ opr, double *__restrict__ c2f, unsigned mask,
-                                 bool skip_later, float *__restrict__ c2f32) {
+// (bbmg_class.f90:978-1051).  Every cell including the overlap.
+__global__ void k_prolong_sweep1(Lay L, const double *__restrict__ opr, double *__restrict__ c2f, unsigned mask) {
     const double ratio = 10.0;
     long long total = (long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
     for (long long t = gtid(); t < total; t += gstride()) {
@@ -195,7 +191,6 @@ __global__ void k_prolong_sweep1(Lay L, const double *__restrict__ opr, double *
         any_cell(L, t, i, j, k);
         long long id = L.idx(i, j, k);
         int n1 = pmod(L.xper, i, L.nx), n2 = pmod(L.yper, j, L.ny), n3 = pmod(L.zper, k, L.nz);
-        if (skip_later && n1 + n2 + n3 >= 2 && i >= 0 && j >= 0 && k >= 0) continue;
         // c2f(0,0,0) and the one line weight (slot sx); every other weight is zero.
         // Scalars rather than an array indexed at run time, so nothing goes to local memory.
         double c0 = 0.0, cx = 0.0;
@@ -228,10 +223,6 @@ __global__ void k_prolong_sweep1(Lay L, const double *__restrict__ opr, double *
         }
 #pragma unroll
         for (int s = 0; s < 8; s++) c2f[s * L.plane + id] = s == 0 ? c0 : (s == sx ? cx : 0.0);
-        if (c2f32) {
-#pragma unroll
-            for (int s = 0; s < 8; s++) c2f32[s * L.plane + id] = (float)(s == 0 ? c0 : (s == sx ? cx : 0.0));
-        }
     }
 }
 
@@ -373,6 +364,67 @@ __global__ void k_prolong_sweep3(Lay L, const double *__restrict__ opr, double *
 // so the results are the same bits as the generic kernels above (which serve
 // the odd-sized levels).
 
+// Sweep 1 on an even level, where a cell's parity class never changes: only
+// the point cells (three even indices) and the line cells (one odd index),
+// one class per blockIdx.y (0 points, 1 + AX lines along AX), each writing
+// the planes that can be nonzero (0, and the line's plane sx); the other
+// planes of these cells hold the zeros of the allocation.  The face and cube
+// cells are left to sweeps 2 and 3 (or, with an index -1, hold zeros or their
+// periodic image, written by the overlap copy).  c2f32, if given, receives the
+// FP32 copy.  Each class enumerates (nx/2+1)(ny/2+1)(nz/2+1) cells: an odd
+// index runs over -1, 1, .., n-1, an even one over 0, 2, .., n.
+template <int AX>
+__device__ __forceinline__ void line_weights(const Lay &L, const double *__restrict__ opr, double *__restrict__ c2f,
+                                             float *__restrict__ c2f32, unsigned mask, long long id) {
+    const double ratio = 10.0;
+    double m = 0.0, z = 0.0, p = 0.0;  // opr1d(-1), opr1d(0), opr1d(+1)
+#pragma unroll
+    for (int q = 0; q < 27; q++) {
+        if (!((mask >> q) & 1u)) continue;  // an all-zero plane adds only zeros
+        const int li = q % 3 - 1, lj = (q / 3) % 3 - 1, lk = q / 9 - 1;
+        const int l = AX == 0 ? li : (AX == 1 ? lj : lk);
+        const int ax = AX == 0 ? q27(li, 0, 0) : (AX == 1 ? q27(0, lj, 0) : q27(0, 0, lk));
+        const double a = opr[q * L.plane + id];
+        if (__dmul_rn(ratio, fabs(opr[ax * L.plane + id])) >= fabs(a)) {
+            if (l < 0) m = __dadd_rn(m, a);
+            else if (l == 0) z = __dadd_rn(z, a);
+            else p = __dadd_rn(p, a);
+        } else {
+            z = __dadd_rn(z, a);
+        }
+    }
+    z = sgn_clamp(z);
+    const double c0 = -m / z, cx = -p / z;
+    constexpr int sx = AX == 0 ? 1 : (AX == 1 ? 2 : 4);
+    c2f[id] = c0;
+    c2f[sx * L.plane + id] = cx;
+    if (c2f32) {
+        c2f32[id] = (float)c0;
+        c2f32[sx * L.plane + id] = (float)cx;
+    }
+}
+
+__global__ void k_prolong_sweep1_even(Lay L, const double *__restrict__ opr, double *__restrict__ c2f,
+                                      unsigned mask, float *__restrict__ c2f32) {
+    const int cls = blockIdx.y;
+    const long long ax = L.nx / 2 + 1, ay = L.ny / 2 + 1, total = ax * ay * (L.nz / 2 + 1);
+    for (long long t = gtid(); t < total; t += gstride()) {
+        const long long u = t / ax;
+        const int a = (int)(t % ax), b = (int)(u % ay), c = (int)(u / ay);
+        const int i = 2 * a - (cls == 1), j = 2 * b - (cls == 2), k = 2 * c - (cls == 3);
+        const long long id = L.idx(i, j, k);
+        switch (cls) {
+            case 0:
+                c2f[id] = 1.0;
+                if (c2f32) c2f32[id] = 1.0f;
+                break;
+            case 1: line_weights<0>(L, opr, c2f, c2f32, mask, id); break;
+            case 2: line_weights<1>(L, opr, c2f, c2f32, mask, id); break;
+            default: line_weights<2>(L, opr, c2f, c2f32, mask, id); break;
+        }
+    }
+}
+
 // Sweep 2, face cells only: the normal index even in [0, n] (the overlap n
 // included), the two in-plane indices odd and interior -- the cells of
 // k_prolong_sweep2 that face_weights does not skip.
@@ -413,7 +465,10 @@ __global__ void k_prolong_sweep3_even(Lay L, const double *__restrict__ opr, dou
 // cell plus |l|).  SEVEN: the operator has only the centre and the six face
 // planes.  Slots with s = -1 in a direction of odd parity are never reached
 // and never read by R (A P); they are not written (the array is zeroed when
-// allocated and stays zero there).
+// allocated and stays zero there).  With SEVEN a slot is reached only if at
+// most one of its components is nonzero in a direction of even parity (one
+// face neighbour moves one index); the others hold zero (the array is zeroed
+// whenever the level-1 stencil changes) and are not written either.
 template <int PX, int PY, int PZ, bool SEVEN>
 __device__ __forceinline__ void ap_fast(const Lay &F, const double *__restrict__ opr, const double *__restrict__ c2f,
                                         double *__restrict__ oprc2f, unsigned mask, int fi, int fj, int fk) {
@@ -446,19 +501,26 @@ __device__ __forceinline__ void ap_fast(const Lay &F, const double *__restrict__
     for (int q = 0; q < 27; q++) {
         const int sx = q % 3 - 1, sy = (q / 3) % 3 - 1, sz = q / 9 - 1;
         if ((PX && sx < 0) || (PY && sy < 0) || (PZ && sz < 0)) continue;
+        if (SEVEN && (!PX && sx != 0) + (!PY && sy != 0) + (!PZ && sz != 0) > 1) continue;
         oprc2f[q * F.plane + id] = acc[q];
     }
 }
 
+// One parity class per blockIdx.y: the blocks of a class are dispatched
+// together, so an SM runs one class's code at a time (the eight unrolled
+// classes together overflow the instruction cache).  Within a class, t runs
+// over the cells i = 2a + PX, j = 2b + PY, k = 2c + PZ (a fastest).
 template <bool SEVEN>
 __global__ void __launch_bounds__(128) k_rap_ap_even(Lay F, const double *__restrict__ opr,
                                                      const double *__restrict__ c2f, double *__restrict__ oprc2f,
                                                      unsigned mask) {
-    long long total = (long long)F.nx * F.ny * F.nz;
+    const int cls = blockIdx.y;
+    const int px = cls & 1, py = (cls >> 1) & 1, pz = cls >> 2;
+    const long long hx = F.nx / 2, hy = F.ny / 2, total = hx * hy * (F.nz / 2);
     for (long long t = gtid(); t < total; t += gstride()) {
-        int fi, fj, fk;
-        interior_cell(F, t, fi, fj, fk);
-        switch ((fi & 1) | ((fj & 1) << 1) | ((fk & 1) << 2)) {
+        const long long u = t / hx;
+        const int fi = (int)(2 * (t % hx)) + px, fj = (int)(2 * (u % hy)) + py, fk = (int)(2 * (u / hy)) + pz;
+        switch (cls) {
             case 0: ap_fast<0, 0, 0, SEVEN>(F, opr, c2f, oprc2f, mask, fi, fj, fk); break;
             case 1: ap_fast<1, 0, 0, SEVEN>(F, opr, c2f, oprc2f, mask, fi, fj, fk); break;
             case 2: ap_fast<0, 1, 0, SEVEN>(F, opr, c2f, oprc2f, mask, fi, fj, fk); break;
@@ -480,7 +542,7 @@ __global__ void __launch_bounds__(128) k_rap_ap_even(Lay F, const double *__rest
 // copy would hold there; in a non-periodic direction the overlap of A P is
 // never written and stays zero), so A P's overlap is not filled during the
 // setup.
-template <int SK>
+template <int SK, bool SEVEN>
 __device__ __forceinline__ void rap_fast(const Lay &F, const Lay &C, const double *__restrict__ f2c,
                                          const double *__restrict__ oprc2f, double *__restrict__ oprc,
                                          float *__restrict__ oprc32, int ci, int cj, int ck) {
@@ -506,6 +568,10 @@ __device__ __forceinline__ void rap_fast(const Lay &F, const Lay &C, const doubl
 #pragma unroll
                     for (int li = -1; li <= 1; li++) {
                         if (li < -1 + (ri & 1)) continue;
+                        // a 7-point fine operator leaves this slot of A P zero
+                        // (fine parity is even where r = 0): adding w * 0 to a
+                        // sum that starts at +0 changes no bit
+                        if (SEVEN && (ri == 0 && li != 0) + (rj == 0 && lj != 0) + (rk == 0 && lk != 0) > 1) continue;
                         const int so = ((ri - 1) / 2 + li + 1) + 3 * ((rj - 1) / 2 + lj + 1);
                         acc[so] = __dadd_rn(acc[so], __dmul_rn(w, oprc2f[q27(li, lj, lk) * F.plane + nid]));
                     }
@@ -522,7 +588,8 @@ __device__ __forceinline__ void rap_fast(const Lay &F, const Lay &C, const doubl
 
 // One warp per 32 consecutive coarse cells and one z slot: warp w takes the
 // slot SK = w % 3 - 1 of the cells 32 (w / 3) .. + 31.  oprc32, if given,
-// receives the FP32 copy.
+// receives the FP32 copy.  SEVEN: the fine operator is 7-point.
+template <bool SEVEN>
 __global__ void __launch_bounds__(128) k_rap_rap_even(Lay F, Lay C, const double *__restrict__ f2c,
                                                       const double *__restrict__ oprc2f, double *__restrict__ oprc,
                                                       float *__restrict__ oprc32) {
@@ -535,9 +602,9 @@ __global__ void __launch_bounds__(128) k_rap_rap_even(Lay F, Lay C, const double
         int ci, cj, ck;
         interior_cell(C, t, ci, cj, ck);
         switch ((int)(w % 3)) {
-            case 0: rap_fast<-1>(F, C, f2c, oprc2f, oprc, oprc32, ci, cj, ck); break;
-            case 1: rap_fast<0>(F, C, f2c, oprc2f, oprc, oprc32, ci, cj, ck); break;
-            default: rap_fast<1>(F, C, f2c, oprc2f, oprc, oprc32, ci, cj, ck); break;
+            case 0: rap_fast<-1, SEVEN>(F, C, f2c, oprc2f, oprc, oprc32, ci, cj, ck); break;
+            case 1: rap_fast<0, SEVEN>(F, C, f2c, oprc2f, oprc, oprc32, ci, cj, ck); break;
+            default: rap_fast<1, SEVEN>(F, C, f2c, oprc2f, oprc, oprc32, ci, cj, ck); break;
         }
     }
 }
@@ -740,16 +807,25 @@ __device__ __forceinline__ void lu_block(double *A, int n, int *__restrict__ piv
             double a = fabs(A[(long long)j * n + i]);
             if (a > best || (a == best && i < bi)) { best = a; bi = i; }
         }
-        sval[tid] = best; sidx[tid] = bi;
-        __syncthreads();
-        for (int s = nt / 2; s > 0; s >>= 1) {
-            if (tid < s) {
-                double a = sval[tid + s]; int ia = sidx[tid + s];
-                if (a > sval[tid] || (a == sval[tid] && ia < sidx[tid])) { sval[tid] = a; sidx[tid] = ia; }
-            }
-            __syncthreads();
+        // the largest value with the smallest index among equals: a total
+        // order, so any reduction order gives the same pivot.  Within each
+        // warp by shuffles, then over the warps' winners by every thread.
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double a = __shfl_down_sync(0xffffffffu, best, o);
+            const int ia = __shfl_down_sync(0xffffffffu, bi, o);
+            if (a > best || (a == best && ia < bi)) { best = a; bi = ia; }
         }
-        int p = sidx[0];
+        if ((tid & 31) == 0) { sval[tid >> 5] = best; sidx[tid >> 5] = bi; }
+        __syncthreads();
+        best = sval[0];
+        bi = sidx[0];
+        for (int w = 1; w < (nt + 31) / 32; w++) {
+            const double a = sval[w];
+            const int ia = sidx[w];
+            if (a > best || (a == best && ia < bi)) { best = a; bi = ia; }
+        }
+        int p = bi;
         if (p >= n) p = j;
         __syncthreads();
         double pv = A[(long long)j * n + p];
@@ -892,7 +968,8 @@ cudaError_t setup_prolongation(const Lay &L, const double *opr, double *c2f, uns
     long long ni = (long long)L.nx * L.ny * L.nz;
     cudaError_t e;
     if (even_level(L) && fast_setup()) {
-        k_prolong_sweep1<<<grid_for(na, 128), 128, 0, s>>>(L, opr, c2f, mask, true, c2f32);
+        const long long np = (long long)(L.nx / 2 + 1) * (L.ny / 2 + 1) * (L.nz / 2 + 1);
+        k_prolong_sweep1_even<<<dim3((unsigned)grid_for(np, 128, 148 * 8), 4), 128, 0, s>>>(L, opr, c2f, mask, c2f32);
         BB_LAUNCH_CHECK();
         const long long hx = L.nx / 2, hy = L.ny / 2, hz = L.nz / 2;
         const long long nf = (hx + 1) * hy * hz + hx * (hy + 1) * hz + hx * hy * (hz + 1);
@@ -903,7 +980,7 @@ cudaError_t setup_prolongation(const Lay &L, const double *opr, double *c2f, uns
         if ((e = wrap_planes(L, c2f, 8, s)) != cudaSuccess) return e;
         return c2f32 ? wrap_planes(L, c2f32, 8, s) : cudaSuccess;
     }
-    k_prolong_sweep1<<<grid_for(na, 128), 128, 0, s>>>(L, opr, c2f, mask, false, nullptr);
+    k_prolong_sweep1<<<grid_for(na, 128), 128, 0, s>>>(L, opr, c2f, mask);
     BB_LAUNCH_CHECK();
     k_prolong_sweep2<<<grid_for(na, 128), 128, 0, s>>>(L, opr, c2f, mask);
     BB_LAUNCH_CHECK();
@@ -952,10 +1029,12 @@ cudaError_t setup_operator(const Lay &F, const Lay &C, const double *oprF, const
     const unsigned seven = (1u << q27h(0, 0, 0)) | (1u << q27h(-1, 0, 0)) | (1u << q27h(1, 0, 0)) |
                            (1u << q27h(0, -1, 0)) | (1u << q27h(0, 1, 0)) | (1u << q27h(0, 0, -1)) |
                            (1u << q27h(0, 0, 1));
-    if (fast && !(mask & ~seven))
-        k_rap_ap_even<true><<<grid_for(nf, nt), nt, 0, s>>>(F, oprF, c2f, oprc2f, mask);
+    const bool fast7 = fast && !(mask & ~seven);
+    const dim3 gap((unsigned)grid_for(nf / 8, nt, 148 * 4), 8);  // one class per blockIdx.y
+    if (fast7)
+        k_rap_ap_even<true><<<gap, nt, 0, s>>>(F, oprF, c2f, oprc2f, mask);
     else if (fast)
-        k_rap_ap_even<false><<<grid_for(nf, nt), nt, 0, s>>>(F, oprF, c2f, oprc2f, mask);
+        k_rap_ap_even<false><<<gap, nt, 0, s>>>(F, oprF, c2f, oprc2f, mask);
     else
         k_rap_ap<<<grid_for(nf, nt), nt, smem, s>>>(F, oprF, c2f, oprc2f, mask);
     BB_LAUNCH_CHECK();
@@ -965,7 +1044,10 @@ cudaError_t setup_operator(const Lay &F, const Lay &C, const double *oprF, const
     }
     long long nc = (long long)C.nx * C.ny * C.nz;
     if (fast) {
-        k_rap_rap_even<<<grid_for(3 * ((nc + 31) / 32) * 32, nt), nt, 0, s>>>(F, C, f2c, oprc2f, oprC, oprC32);
+        if (fast7)
+            k_rap_rap_even<true><<<grid_for(3 * ((nc + 31) / 32) * 32, nt), nt, 0, s>>>(F, C, f2c, oprc2f, oprC, oprC32);
+        else
+            k_rap_rap_even<false><<<grid_for(3 * ((nc + 31) / 32) * 32, nt), nt, 0, s>>>(F, C, f2c, oprc2f, oprC, oprC32);
         BB_LAUNCH_CHECK();
         k_fill_shell<<<grid_for(shell_cells(C), 256), 256, 0, s>>>(C, oprC, 27, oprC32);
         BB_LAUNCH_CHECK();
