@@ -128,7 +128,8 @@ __global__ void __launch_bounds__(128) k_conv3(Act x, const bf16 *__restrict__ w
 //     those steps), both in the K-major no-swizzle canonical layout of the
 //     MMA: per 8-channel group, rows of 16 bytes one after another (A:
 //     [step][group][voxel][16 B], B: [step][group][cout][16 B]).
-//   * kTgS stages form a ring filled with cp.async kTgS-1 stages ahead; one
+//   * S stages (template parameter, 2 by default) form a ring filled with
+//     cp.async S-1 stages ahead; one
 //     thread issues the tcgen05.mma (M = 128, N = cout, K = 16, BF16 x BF16 ->
 //     FP32 in TMEM) of a stage and commits them to that stage's mbarrier; a
 //     stage is refilled once its mbarrier shows the MMAs reading it are done.
@@ -138,7 +139,7 @@ __global__ void __launch_bounds__(128) k_conv3(Act x, const bf16 *__restrict__ w
 // nn_tc_error), and the CTA then drains its copies, frees its TMEM and
 // returns without writing.
 constexpr unsigned kTcSpinLimit = 1u << 22;
-constexpr int kTgS = 4;   // pipeline stages
+constexpr int kTgS = 4;   // pipeline stages (the default of TgCfg; the launcher picks 2)
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -182,7 +183,7 @@ __device__ __forceinline__ bool mbar_wait(const uint64_t *mb, unsigned parity) {
 // (three MMAs per unit).  Otherwise a tile is 128 consecutive voxels of the
 // grid (several rows when w < 128) and a K unit is one tap's 16 channels of
 // the 128 voxels (one MMA).
-template <int N, bool ROW>
+template <int N, bool ROW, int S = kTgS>
 struct TgCfg {
     static constexpr int kCols = N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));  // TMEM columns
     static constexpr int VOX = ROW ? 130 : 128;         // A rows staged per unit
@@ -192,18 +193,18 @@ struct TgCfg {
     static constexpr int B_UNIT = TAPS * 2 * N * 16;    // bytes: [tap][group][cout][16 B]
     static constexpr int A_BYTES = KU * A_UNIT;
     static constexpr int B_BYTES = KU * B_UNIT;
-    static constexpr size_t SMEM = 128 + (size_t)kTgS * (A_BYTES + B_BYTES);
+    static constexpr size_t SMEM = 128 + (size_t)S * (A_BYTES + B_BYTES);
 };
 
-template <int N, bool ROW>
+template <int N, bool ROW, int S>
 __global__ void __launch_bounds__(128) k_conv3_tcg(Act x, const bf16 *__restrict__ wt, const float *__restrict__ bias,
                                                     Act y, int relu, int *err) {
-    using Cfg = TgCfg<N, ROW>;
+    using Cfg = TgCfg<N, ROW, S>;
     extern __shared__ __align__(128) unsigned char smtc[];
     unsigned *tmem_slot = reinterpret_cast<unsigned *>(smtc);
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(smtc + 16);  // kTgS barriers
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(smtc + 16);  // S barriers
     unsigned char *A = smtc + 128;
-    unsigned char *B = A + (size_t)kTgS * Cfg::A_BYTES;
+    unsigned char *B = A + (size_t)S * Cfg::A_BYTES;
     const int tid = threadIdx.x, warp = tid >> 5;
     const int cin = x.c, kpt = cin >> 4;                 // 16-channel blocks
     const int nu = (ROW ? 9 : 27) * kpt;                 // K units
@@ -236,7 +237,7 @@ __global__ void __launch_bounds__(128) k_conv3_tcg(Act x, const bf16 *__restrict
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0)
-        for (int s = 0; s < kTgS; s++) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar + s)));
+        for (int s = 0; s < S; s++) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar + s)));
 
     // stage `chunk` (units chunk*KU ..) into ring slot `s`
     auto load = [&](int chunk, int s) {
@@ -275,7 +276,7 @@ __global__ void __launch_bounds__(128) k_conv3_tcg(Act x, const bf16 *__restrict
     auto commit_group = []() { asm volatile("cp.async.commit_group;" ::: "memory"); };
 
 #pragma unroll 1
-    for (int p = 0; p < kTgS - 1; p++) {
+    for (int p = 0; p < S - 1; p++) {
         if (p < nK) load(p, p);
         commit_group();
     }
@@ -286,8 +287,8 @@ __global__ void __launch_bounds__(128) k_conv3_tcg(Act x, const bf16 *__restrict
     bool ok = true;
 #pragma unroll 1
     for (int k = 0; k < nK; k++) {
-        const int s = k % kTgS;
-        asm volatile("cp.async.wait_group %0;" ::"n"(kTgS - 2) : "memory");  // stage k has landed
+        const int s = k % S;
+        asm volatile("cp.async.wait_group %0;" ::"n"(S - 2) : "memory");  // stage k has landed
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");          // visible to the tensor core
         __syncthreads();
         if (tid == 0) {
@@ -312,21 +313,21 @@ __global__ void __launch_bounds__(128) k_conv3_tcg(Act x, const bf16 *__restrict
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                          ::"r"(smem_u32(mbar + s)) : "memory");
         }
-        const int nk = k + kTgS - 1;  // the stage to fill next, in the slot stage k-1 used
+        const int nk = k + S - 1;  // the stage to fill next, in the slot stage k-1 used
         if (nk < nK) {
             if (k >= 1) {
-                const bool done = mbar_wait(mbar + nk % kTgS, ((k - 1) / kTgS) & 1);
+                const bool done = mbar_wait(mbar + nk % S, ((k - 1) / S) & 1);
                 if (__syncthreads_or(!done)) {
                     ok = false;
                     break;
                 }
             }
-            load(nk, nk % kTgS);
+            load(nk, nk % S);
         }
         commit_group();
     }
     bool done = false;
-    if (ok) done = mbar_wait(mbar + (nK - 1) % kTgS, ((nK - 1) / kTgS) & 1);
+    if (ok) done = mbar_wait(mbar + (nK - 1) % S, ((nK - 1) / S) & 1);
     if (__syncthreads_or(!done)) {
         done = false;
         if (tid == 0) atomicExch(err, 1);
@@ -378,27 +379,43 @@ bool tc_eligible(const Act &x, const Act &y) {
     return !(x.ld % 8 || y.ld % 8 || (reinterpret_cast<uintptr_t>(x.p) & 15) || (reinterpret_cast<uintptr_t>(y.p) & 15));
 }
 
-template <int N, bool ROW>
+template <int N, bool ROW, int S>
 int launch_conv_tc_t(const Act &x, const bf16 *wt, const float *bias, const Act &y, int relu, cudaStream_t s) {
-    using Cfg = TgCfg<N, ROW>;
+    using Cfg = TgCfg<N, ROW, S>;
     static bool attr = false;
     if (!attr) {
-        if (cudaFuncSetAttribute(k_conv3_tcg<N, ROW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM) !=
+        if (cudaFuncSetAttribute(k_conv3_tcg<N, ROW, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM) !=
             cudaSuccess)
             return BBMG_CUDA;
         attr = true;
     }
     int *err = tc_err_flag();
     if (!err) return BBMG_NO_MEMORY;
-    k_conv3_tcg<N, ROW><<<x.nvox / 128, 128, Cfg::SMEM, s>>>(x, wt, bias, y, relu, err);
+    k_conv3_tcg<N, ROW, S><<<x.nvox / 128, 128, Cfg::SMEM, s>>>(x, wt, bias, y, relu, err);
     return done(cudaGetLastError());
+}
+
+// ring depth S (BBMG_TC_STAGES = 2, 3 or 4): with 2 stages a CTA needs half
+// the shared memory of 4 and about twice as many CTAs share an SM; measured
+// at 128^3 the forward pass took 3.66 ms with 2 stages, 3.72 with 3, 3.79
+// with 4
+template <int N, bool ROW>
+int launch_conv_tc_s(const Act &x, const bf16 *wt, const float *bias, const Act &y, int relu, cudaStream_t s) {
+    static int st = -1;
+    if (st < 0) {
+        const char *e = getenv("BBMG_TC_STAGES");
+        st = e ? atoi(e) : 2;
+    }
+    if (st == 2) return launch_conv_tc_t<N, ROW, 2>(x, wt, bias, y, relu, s);
+    if (st == 3) return launch_conv_tc_t<N, ROW, 3>(x, wt, bias, y, relu, s);
+    return launch_conv_tc_t<N, ROW, 4>(x, wt, bias, y, relu, s);
 }
 
 template <int N>
 int launch_conv_tc(const Act &x, const bf16 *wt, const float *bias, const Act &y, int relu, cudaStream_t s) {
     static const bool no_rows = getenv("BBMG_NO_TC_ROWS") != nullptr;
-    return (x.w % 128 == 0 && !no_rows) ? launch_conv_tc_t<N, true>(x, wt, bias, y, relu, s)
-                                        : launch_conv_tc_t<N, false>(x, wt, bias, y, relu, s);
+    return (x.w % 128 == 0 && !no_rows) ? launch_conv_tc_s<N, true>(x, wt, bias, y, relu, s)
+                                        : launch_conv_tc_s<N, false>(x, wt, bias, y, relu, s);
 }
 
 int launch_conv(const Act &x, const bf16 *wt, const float *bias, const Act &y, int relu, cudaStream_t s) {
