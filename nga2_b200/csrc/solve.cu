@@ -1285,12 +1285,11 @@ __global__ void __launch_bounds__(NT) k_cg_pap_march(Lay L, const double *__rest
                                                       double *__restrict__ pp_new, double *__restrict__ Ap,
                                                       const CgScal *__restrict__ sc, double *__restrict__ part,
                                                       int na, int kchunk) {
-    pdl_entry();
+    pdl_launch();
     __shared__ double red[NT];
     extern __shared__ __align__(16) unsigned char smraw[];
     using O = Ops<double, true>;
     constexpr int VW = 2;
-    const double beta = sc->beta;
     const int TH = na / VW, TY = blockDim.x / (2 * TH);
     const int seg = na + 8;  // position p of a half-row at index p + 4
     const int rowsO = 4 * TY + 1, rowsV = TY + 2;
@@ -1318,6 +1317,14 @@ __global__ void __launch_bounds__(NT) k_cg_pap_march(Lay L, const double *__rest
     const bool lo_edge = h == 0 && c == 0, hi_edge = h == 1 && c == TH - 1, edge = lo_edge || hi_edge;
     const int ovl = h == 0 ? -1 : na;
     auto goff = [&](int jr, int kr) { return L.G + L.row(jr, kr) * L.P + hb; };
+    if (valid && k0 < k1) {  // the first stages' operator rows into L2 while the predecessor finishes
+#pragma unroll
+        for (int kp = k0 - 1; kp <= k0 + 1; kp++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) pf_l2(opr + q * P + goff(j, kp) + pos);
+    }
+    pdl_wait();
+    const double beta = sc->beta;  // written by the predecessor: after the wait
     auto commit = []() { asm volatile("cp.async.commit_group;" ::: "memory"); };
     // zz and pp_old of plane kp on row jr into tile row rr of slot sl
     auto fill_v = [&](int sl, int rr, int jr, int kp) {
