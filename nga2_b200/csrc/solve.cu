@@ -804,25 +804,29 @@ __global__ void __launch_bounds__(256) k_prolong(Lay F, Lay C, const T *__restri
 template <typename T>
 __global__ void __launch_bounds__(128) k_restrict_staged(Lay F, Lay C, const T *__restrict__ c2f,
                                                           const T *__restrict__ rF, T *__restrict__ fC,
-                                                          T *__restrict__ vC, int na) {
+                                                          T *__restrict__ vC, int na, int np) {
     pdl_launch();
     extern __shared__ __align__(16) unsigned char smraw[];
     T *smf = reinterpret_cast<T *>(smraw);
     using O = Ops<T, ExactOf<T>::value>;
     constexpr int EPC = 16 / sizeof(T);  // elements per 16-byte copy
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int seg = na + 8;
+    // a job is one of the np equal parts of a coarse row (np = 2 halves the
+    // shared memory per warp, so twice the warps fit on an SM)
+    const int nh = na / np, seg = nh + 8;
     T *S = smf + (size_t)warp * 45 * seg;
     const long long P = F.plane;
-    const int nrows = C.ny * C.nz;
-    // the weight segments of coarse row `row` (written only by the setup)
+    const int nrows = C.ny * C.nz * np;
+    // the weight segments of job `row` (written only by the setup)
     auto copy_w = [&](int row) {
+        const int h0 = (row % np) * nh;
+        row /= np;
         const int fj = 2 * (row % C.ny), fk = 2 * (row / C.ny);
         for (int rk = -1; rk <= 1; rk++)
             for (int rj = -1; rj <= 1; rj++) {
                 const int b = 5 * ((rk + 1) * 3 + (rj + 1));
                 const int pj = (1 - rj) / 2, pk = (1 - rk) / 2;
-                const long long fr = F.G + F.row(fj + rj, fk + rk) * F.P - 4;
+                const long long fr = F.G + F.row(fj + rj, fk + rk) * F.P - 4 + h0;
                 for (int e = lane * EPC; e < seg; e += 32 * EPC) {
                     cp16(S + (b + 2) * seg + e, c2f + q8(0, pj, pk) * P + fr + F.B0 + e);  // ri = 0
                     cp16(S + (b + 3) * seg + e, c2f + q8(0, pj, pk) * P + fr + e);         // ri = +1
@@ -834,7 +838,8 @@ __global__ void __launch_bounds__(128) k_restrict_staged(Lay F, Lay C, const T *
     if (row < nrows) copy_w(row);  // before the wait for the predecessor
     pdl_wait();
     for (bool first = true; row < nrows; row += gridDim.x * 4, first = false) {
-        const int cj = row % C.ny, ck = row / C.ny;
+        const int h0 = (row % np) * nh, crow = row / np;
+        const int cj = crow % C.ny, ck = crow / C.ny;
         const int fj = 2 * cj, fk = 2 * ck;
         const int rk0 = -pmod(F.zper, fk - 1, F.nz), rk1 = pmod(F.zper, fk + 1, F.nz);
         const int rj0 = -pmod(F.yper, fj - 1, F.ny), rj1 = pmod(F.yper, fj + 1, F.ny);
@@ -843,7 +848,7 @@ __global__ void __launch_bounds__(128) k_restrict_staged(Lay F, Lay C, const T *
         for (int rk = -1; rk <= 1; rk++)
             for (int rj = -1; rj <= 1; rj++) {
                 const int b = 5 * ((rk + 1) * 3 + (rj + 1));
-                const long long fr = F.G + F.row(fj + rj, fk + rk) * F.P - 4;
+                const long long fr = F.G + F.row(fj + rj, fk + rk) * F.P - 4 + h0;
                 for (int e = lane * EPC; e < seg; e += 32 * EPC) {
                     cp16(S + (b + 0) * seg + e, rF + fr + e);         // r odd half
                     cp16(S + (b + 1) * seg + e, rF + fr + F.B0 + e);  // r even half
@@ -851,9 +856,9 @@ __global__ void __launch_bounds__(128) k_restrict_staged(Lay F, Lay C, const T *
             }
         asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
         __syncwarp();
-        for (int c0 = lane; c0 < C.nx; c0 += 32) {  // lane-strided coarse points
+        for (int c0 = lane; c0 < nh; c0 += 32) {  // lane-strided coarse points of the part
             {
-                const int ci = c0;
+                const int ci = h0 + c0;
                 const int fi = 2 * ci;
                 const int ri0 = -pmod(F.xper, fi - 1, F.nx), ri1 = pmod(F.xper, fi + 1, F.nx);
                 T sum = T(0);
@@ -866,8 +871,9 @@ __global__ void __launch_bounds__(128) k_restrict_staged(Lay F, Lay C, const T *
                             if (rk < rk0 || rk > rk1 || rj < rj0 || rj > rj1 || ri < ri0 || ri > ri1) continue;
                             const T *Sb = S + 5 * ((rk + 1) * 3 + (rj + 1)) * seg + 4;
                             // fi = 2ci: even position ci; fi+1: odd ci; fi-1: odd ci-1
-                            const T w = ri == 0 ? Sb[2 * seg + ci] : (ri > 0 ? Sb[3 * seg + ci] : Sb[4 * seg + ci - 1]);
-                            const T rv = ri == 0 ? Sb[seg + ci] : (ri > 0 ? Sb[ci] : Sb[ci - 1]);
+                            // (segment index relative to the part's start h0)
+                            const T w = ri == 0 ? Sb[2 * seg + c0] : (ri > 0 ? Sb[3 * seg + c0] : Sb[4 * seg + c0 - 1]);
+                            const T rv = ri == 0 ? Sb[seg + c0] : (ri > 0 ? Sb[c0] : Sb[c0 - 1]);
                             sum = O::mac(sum, w, rv);
                         }
                 const long long cid = C.idx(ci, cj, ck);
@@ -1968,7 +1974,9 @@ cudaError_t launch_residual(const Lay &L, const NbrOff &nb, int npt, const T *op
 template <typename T>
 cudaError_t launch_restrict(const Lay &F, const Lay &C, const T *c2f, const T *rF, T *fC, T *vC, cudaStream_t s) {
     const int na = F.nx >> 1;
-    const size_t smem = sizeof(T) * 45 * (size_t)(na + 8) * 4;
+    // coarse rows of 128 or more points in two parts (16-byte aligned starts)
+    const int np = (na >= 128 && na % 8 == 0) ? 2 : 1;
+    const size_t smem = sizeof(T) * 45 * (size_t)(na / np + 8) * 4;
     // FP64 segments fill up to 196 KB per block (one block per SM): slower than
     // the register kernel at 256^3, so the staged restriction is FP32 only
     if (sizeof(T) == 4 && use_staged(F) && C.nx == na && smem <= 200 * 1024) {
@@ -1979,10 +1987,10 @@ cudaError_t launch_restrict(const Lay &F, const Lay &C, const T *c2f, const T *r
             if (e != cudaSuccess) return e;
             attr = true;
         }
-        long long gx = ((long long)C.ny * C.nz + 3) / 4;
+        long long gx = ((long long)C.ny * C.nz * np + 3) / 4;
         if (gx > 148LL * 16) gx = 148LL * 16;
         BB_CHECK_LAUNCH((launch_k(k_restrict_staged<T>, dim3((unsigned)gx), dim3(128), smem, s, F, C, c2f, rF, fC, vC,
-                                  na)));
+                                  na, np)));
         return cudaSuccess;
     }
     const Geo g = geo_rows(C.nx, (long long)C.ny * C.nz);
