@@ -112,9 +112,9 @@ __global__ void k_wrap_f(Lay L, float *__restrict__ a, int nplanes) {
 }
 // The overlap shell after a kernel that wrote the interior: a shell cell that
 // lies outside in a non-periodic direction is zero, any other takes its
-// periodic image (an interior cell).  The same values as k_zero_shell
-// followed by k_wrap of every plane, in one pass; a32, if given, receives the
-// FP32 copy of what is written.
+// periodic image (an interior cell).  The same values as zeroing the shell
+// and then running k_wrap on every plane, in one pass; a32, if given,
+// receives the FP32 copy of what is written.
 __global__ void k_fill_shell(Lay L, double *__restrict__ a, int nplanes, float *__restrict__ a32) {
     const long long total = shell_cells(L);
     for (long long t = gtid(); t < total; t += gstride()) {
@@ -164,16 +164,6 @@ __global__ void k_solve_planes(long long P, const double *__restrict__ opr, Plan
     }
 }
 
-// zero every plane of the overlap shell (the interior is written by the caller's kernel)
-__global__ void k_zero_shell(Lay L, double *__restrict__ a, int nplanes) {
-    const long long total = shell_cells(L);
-    for (long long t = gtid(); t < total; t += gstride()) {
-        int i, j, k;
-        shell_cell(L, t, i, j, k);
-        const long long d = L.idx(i, j, k);
-        for (int q = 0; q < nplanes; q++) a[q * L.plane + d] = 0.0;
-    }
-}
 
 __device__ __forceinline__ double sgn_clamp(double a) {
     // sign(max(abs(a),epsilon(1.0_WP)),a)
@@ -1071,8 +1061,6 @@ cudaError_t setup_solve_planes(const Lay &L, const double *opr, int npt, const i
 }
 
 cudaError_t check_symmetric7(const Lay &L, const double *opr, int *flag, cudaStream_t s) {
-    long long n = (long long)L.nx * L.ny * L.nz;
-    (void)n;
     const int bx = L.nx >= 64 ? 64 : 32, by = 256 / bx;
     const int gx = (L.nx + bx - 1) / bx;
     long long gy = ((long long)L.ny * L.nz + by - 1) / by;
