@@ -160,7 +160,7 @@ int bbmg_set_residual_norm(bbmg_handle *h, int norm);
  * V-cycle alone.  If the residual falls by less than 10 % over three
  * iterations, the solve continues as the plain FP64 pcg_bbox from the current
  * iterate (bbmg_info.fallback_it), so plain multigrid stays the fallback and
- * the judge of convergence.  fn = NULL removes the stage.  The handle must be
+ * decides convergence.  fn = NULL removes the stage.  The handle must be
  * BBMG_METHOD_PCG_BBOX with BBMG_PREC_MIXED.  No counterpart in the
  * reference. */
 typedef int (*bbmg_stage_fn)(void *ctx, const double *r, double *z, void *stream);
