@@ -203,7 +203,11 @@ const char *bbmg_last_error(const bbmg_handle *h);
 #define BBMG_STEP_CYCLE        4  /* cycle(n)                              bbmg_class.f90:732-776 */
 #define BBMG_STEP_DIRECT       5  /* direct_solve()                        bbmg_class.f90:891-927 */
 
-/* prec selects the FP64 (0) or FP32 (1) copy of a level's data. */
+/* prec selects the FP64 (0) or FP32 (1) copy of a level's data.  The overlap
+ * of f2c and oprc2f is read by nothing in the setup or the solve; on levels
+ * with even sizes the setup leaves it unfilled, and bbmg_debug_get fills it
+ * (zero in non-periodic directions, the periodic image otherwise, as the
+ * reference holds it) on the handle's stream before the copy out. */
 long long bbmg_debug_get(bbmg_handle *h, int level, int which, int prec, double *out);
 long long bbmg_debug_put(bbmg_handle *h, int level, int which, int prec, const double *in);
 int bbmg_debug_step(bbmg_handle *h, int step, int level, int arg, int prec);
